@@ -1,0 +1,147 @@
+/* exafmm_b200: B200-native 3D Laplace FMM (free space and periodic), C ABI.
+ *
+ * Drop-in for the evaluation path of minimal ExaFMM's `3d/` and `3dp/`
+ * variants: the same bodies, adaptive octree, dual-tree interaction lists and
+ * P2P/P2M/M2M/M2L/L2L/L2P operators with complex spherical-harmonic expansions
+ * of order P, computed by hand-written sm_100a CUDA kernels on one GPU.
+ * Interface citations name the reference function each entry point replaces
+ * (paths relative to the reference project).
+ *
+ * Conventions
+ *  - Every function returns an int status: EXAFMM_OK (0) or a negative
+ *    EXAFMM_ERR_* code; exafmm_b200_last_error() gives the message.
+ *  - Bodies cross the boundary as the reference's Body record, 8 doubles per
+ *    body: X[3], q, p, F[3] (3d/exafmm.h:14-19).  Host or device pointers are
+ *    accepted where a `where` argument says so.
+ *  - A handle owns its device buffers and one CUDA stream; calls on a handle
+ *    must not overlap in time (the reference is not reentrant either:
+ *    3d/exafmm.h:40-45 keeps its state in globals).  Separate handles are
+ *    independent.
+ *  - Results are in tree order (the order buildTree leaves the bodies in,
+ *    3d/build_tree.h:88-96), and exafmm_b200_get_perm() maps tree positions
+ *    back to input positions.
+ */
+#ifndef EXAFMM_B200_H
+#define EXAFMM_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define EXAFMM_API __attribute__((visibility("default")))
+#else
+#define EXAFMM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  EXAFMM_OK = 0,
+  EXAFMM_ERR_ARG = -1,       /* invalid argument (N, P, ncrit, theta, pointer) */
+  EXAFMM_ERR_CUDA = -2,      /* a CUDA call failed */
+  EXAFMM_ERR_NOMEM = -3,     /* device allocation failed */
+  EXAFMM_ERR_STATE = -4,     /* call out of order (e.g. lists before tree) */
+  EXAFMM_ERR_DEPTH = -5,     /* tree deeper than EXAFMM_MAX_LEVEL (coincident bodies) */
+  EXAFMM_ERR_CAPACITY = -6,  /* a device buffer stayed too small after retries */
+  EXAFMM_ERR_TIMEOUT = -7,   /* a bounded device-side wait ran out */
+  EXAFMM_ERR_NOGPU = -8      /* no usable sm_100 device */
+};
+
+enum { EXAFMM_FP64 = 0, EXAFMM_MIXED = 1 };
+enum { EXAFMM_HOST = 0, EXAFMM_DEVICE = 1 };
+
+#define EXAFMM_MAX_P 32     /* largest expansion order accepted */
+#define EXAFMM_MAX_LEVEL 21 /* deepest octree level (3 bits per level in a 64-bit key) */
+
+/* Global configuration of the reference (3d/exafmm.h:40-45 P, ncrit, theta;
+ * 3dp/exafmm.h:45-47 images, cycle) plus the arithmetic form. */
+typedef struct exafmm_params {
+  int P;           /* expansion order (NTERM = P(P+1)/2 coefficients) */
+  int ncrit;       /* max bodies per leaf */
+  double theta;    /* multipole acceptance criterion */
+  int images;      /* 0: free space (3d); >0: periodic image levels (3dp) */
+  double cycle;    /* period of the periodic box (3dp) */
+  int precision;   /* EXAFMM_FP64 or EXAFMM_MIXED */
+  int device;      /* CUDA device ordinal */
+} exafmm_params;
+
+typedef struct exafmm_b200 exafmm_b200;
+
+/* Handle lifecycle.  exafmm_b200_create replaces the reference's global
+ * set-up (3d/fmm.cxx:12-15 parameter globals, 3d/kernel.h:118-120
+ * initKernel). */
+EXAFMM_API int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out);
+EXAFMM_API int exafmm_b200_destroy(exafmm_b200 *h);
+EXAFMM_API const char *exafmm_b200_last_error(const exafmm_b200 *h);
+EXAFMM_API int exafmm_b200_set_params(exafmm_b200 *h, const exafmm_params *params);
+
+/* Load N bodies (Body records, 8 doubles each; p and F are ignored).
+ * where = EXAFMM_HOST or EXAFMM_DEVICE.  The caller's copy is not modified. */
+EXAFMM_API int exafmm_b200_set_bodies(exafmm_b200 *h, const double *bodies8, int64_t n, int where);
+
+/* Phases of one evaluation, replacing the reference's buildTree
+ * (3d/build_tree.h:88-96), the list recording of the lazy traversal
+ * (3d/traverse_lazy.h:27-44 getList; 3dp/traverse_lazy.h:276-293 image loop),
+ * upwardPass (3d/traverse_eager.h:127-144), horizontalPass
+ * (3d/traverse_eager.h:147-172 M2L + P2P; 3dp/traverse_eager.h:95-110 with the
+ * periodic root, :46-93) and downwardPass (3d/traverse_eager.h:175-190). */
+EXAFMM_API int exafmm_b200_build_tree(exafmm_b200 *h);
+EXAFMM_API int exafmm_b200_build_lists(exafmm_b200 *h);
+EXAFMM_API int exafmm_b200_upward(exafmm_b200 *h);
+EXAFMM_API int exafmm_b200_horizontal(exafmm_b200 *h);
+EXAFMM_API int exafmm_b200_downward(exafmm_b200 *h);
+
+/* All phases: tree, lists, upward, horizontal, downward (3d/fmm.cxx:40-53). */
+EXAFMM_API int exafmm_b200_evaluate(exafmm_b200 *h);
+
+/* Results.  get_bodies writes N Body records in tree order (X,q as sorted,
+ * p,F = FMM result) to host or device memory.  get_perm writes, per tree
+ * position, the input index of that body. */
+EXAFMM_API int exafmm_b200_get_bodies(exafmm_b200 *h, double *bodies8, int where);
+EXAFMM_API int exafmm_b200_get_perm(exafmm_b200 *h, int64_t *perm, int where);
+
+/* Tree in the reference's cell order (3d/build_tree.h:117-131): per cell
+ * NCHILD, index of the first child (-1 for a leaf), index of the first body
+ * in tree order, NBODY, level, and centre+radius as 4 doubles.  Host arrays
+ * of exafmm_b200_num_cells() entries. */
+EXAFMM_API int64_t exafmm_b200_num_cells(exafmm_b200 *h);
+EXAFMM_API int exafmm_b200_get_tree(exafmm_b200 *h, int *nchild, int *child, int *body, int *nbody, int *level, double *xr);
+
+/* Interaction lists per target cell, reference cell indices, in the
+ * reference's recording order (3d/traverse_lazy.h:27-44): CSR offsets
+ * (num_cells+1), source cells, and the periodic index periodic1D(iX)
+ * (3dp/traverse_lazy.h:27-30; 13 = no shift).  Counts first, then arrays. */
+EXAFMM_API int exafmm_b200_count_lists(exafmm_b200 *h, int64_t *n_m2l, int64_t *n_p2p);
+EXAFMM_API int exafmm_b200_get_lists(exafmm_b200 *h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src,
+                          int *p2p_img);
+
+/* Multipole and local expansions (complex, re/im interleaved, NTERM per cell)
+ * in the reference's cell order.  Host arrays. */
+EXAFMM_API int exafmm_b200_get_expansions(exafmm_b200 *h, double *M, double *L);
+
+/* Direct summation of all current bodies onto nt targets (Body records in
+ * host or device memory; p and F accumulate), FP64: replaces direct()
+ * (3d/traverse_eager.h:193-202). */
+EXAFMM_API int exafmm_b200_direct(exafmm_b200 *h, double *targets8, int64_t nt, int where);
+
+/* Per-phase device times of the last evaluation in milliseconds, measured
+ * with CUDA events on the handle's stream: tree, lists, upward, m2l, p2p,
+ * downward, total (7 values). */
+EXAFMM_API int exafmm_b200_get_timings(exafmm_b200 *h, double *ms7);
+
+/* Library information: number of kernel launches issued by the last
+ * evaluate(), and the build's compute capability target (100 = sm_100a). */
+EXAFMM_API int64_t exafmm_b200_last_launches(exafmm_b200 *h);
+EXAFMM_API int exafmm_b200_arch(void);
+
+/* Diagnostic with no reference counterpart: FMA-pipe throughput of the
+ * handle's device in TFLOP/s (precision EXAFMM_FP64 or EXAFMM_MIXED = FP32),
+ * measured with a dependent-chain FMA kernel; the denominator of the FP64 and
+ * FP32 rooflines. */
+EXAFMM_API int exafmm_b200_fma_peak(exafmm_b200 *h, int precision, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,250 @@
+"""minimal_b200: B200-native 3D Laplace FMM (minimal ExaFMM `3d/`, `3dp/`).
+
+The product is the C-ABI library ``lib/libexafmm_b200.so`` (declared in
+``include/exafmm_b200.h``).  This module is a thin ctypes mirror of the
+reference's driver-level interface for Python callers (tests, bench.py):
+
+    fmm = FMM(P=10, ncrit=64, theta=0.4)   # globals of 3d/fmm.cxx:12-15
+    fmm.set_bodies(bodies)                  # Body records (N x 8) or x,y,z,q (N x 4)
+    fmm.evaluate()                          # buildTree .. downwardPass
+    out = fmm.bodies()                      # tree order, like the reference
+
+There is no CPU fallback: without the built library (or without an sm_100
+GPU) the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .bodies import drand48_bodies, plummer_bodies, uniform_bodies  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libexafmm_b200.so")
+
+FP64, MIXED = 0, 1
+HOST, DEVICE = 0, 1
+ERRORS = {
+    -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_STATE", -5: "ERR_DEPTH",
+    -6: "ERR_CAPACITY", -7: "ERR_TIMEOUT", -8: "ERR_NOGPU",
+}
+
+# Every entry point of include/exafmm_b200.h (checked by the tests).
+API = [
+    "exafmm_b200_create", "exafmm_b200_destroy", "exafmm_b200_last_error", "exafmm_b200_set_params",
+    "exafmm_b200_set_bodies", "exafmm_b200_build_tree", "exafmm_b200_build_lists", "exafmm_b200_upward",
+    "exafmm_b200_horizontal", "exafmm_b200_downward", "exafmm_b200_evaluate", "exafmm_b200_get_bodies",
+    "exafmm_b200_get_perm", "exafmm_b200_num_cells", "exafmm_b200_get_tree", "exafmm_b200_count_lists",
+    "exafmm_b200_get_lists", "exafmm_b200_get_expansions", "exafmm_b200_direct", "exafmm_b200_get_timings",
+    "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak",
+]
+
+PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
+
+
+class FMMError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("P", ctypes.c_int), ("ncrit", ctypes.c_int), ("theta", ctypes.c_double),
+                ("images", ctypes.c_int), ("cycle", ctypes.c_double), ("precision", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load (once) and type the C ABI.  Raises if the library was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run `python -m minimal_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, i, i64, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double
+    sig = {
+        "exafmm_b200_create": (i, [ctypes.POINTER(Params), ctypes.POINTER(vp)]),
+        "exafmm_b200_destroy": (i, [vp]),
+        "exafmm_b200_last_error": (ctypes.c_char_p, [vp]),
+        "exafmm_b200_set_params": (i, [vp, ctypes.POINTER(Params)]),
+        "exafmm_b200_set_bodies": (i, [vp, vp, i64, i]),
+        "exafmm_b200_build_tree": (i, [vp]),
+        "exafmm_b200_build_lists": (i, [vp]),
+        "exafmm_b200_upward": (i, [vp]),
+        "exafmm_b200_horizontal": (i, [vp]),
+        "exafmm_b200_downward": (i, [vp]),
+        "exafmm_b200_evaluate": (i, [vp]),
+        "exafmm_b200_get_bodies": (i, [vp, vp, i]),
+        "exafmm_b200_get_perm": (i, [vp, vp, i]),
+        "exafmm_b200_num_cells": (i64, [vp]),
+        "exafmm_b200_get_tree": (i, [vp, vp, vp, vp, vp, vp, vp]),
+        "exafmm_b200_count_lists": (i, [vp, vp, vp]),
+        "exafmm_b200_get_lists": (i, [vp] * 7),
+        "exafmm_b200_get_expansions": (i, [vp, vp, vp]),
+        "exafmm_b200_direct": (i, [vp, vp, i64, i]),
+        "exafmm_b200_get_timings": (i, [vp, vp]),
+        "exafmm_b200_last_launches": (i64, [vp]),
+        "exafmm_b200_arch": (i, []),
+        "exafmm_b200_fma_peak": (i, [vp, i, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def as_records(bodies):
+    """N x 4 (x,y,z,q) or N x 8 Body records -> contiguous N x 8 float64."""
+    b = np.asarray(bodies, dtype=np.float64)
+    if b.ndim != 2 or b.shape[1] not in (4, 8):
+        raise ValueError("bodies must be N x 4 (x,y,z,q) or N x 8 (X,q,p,F)")
+    if b.shape[1] == 4:
+        r = np.zeros((len(b), 8))
+        r[:, :4] = b
+        return r
+    return np.ascontiguousarray(b)
+
+
+class FMM:
+    """One FMM problem on one GPU (a handle of the C ABI)."""
+
+    def __init__(self, P=10, ncrit=64, theta=0.4, images=0, cycle=0.0, precision="fp64", device=0):
+        self.lib = load_library()
+        self.params = Params(P, ncrit, theta, images, cycle, MIXED if precision == "mixed" else FP64, device)
+        h = ctypes.c_void_p()
+        rc = self.lib.exafmm_b200_create(ctypes.byref(self.params), ctypes.byref(h))
+        if rc != 0:
+            raise FMMError(rc, self.lib.exafmm_b200_last_error(None).decode())
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.exafmm_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise FMMError(rc, self.lib.exafmm_b200_last_error(self.h).decode())
+
+    # ---- configuration and input
+    def set_params(self, **kw):
+        for k, v in kw.items():
+            if k == "precision":
+                v = MIXED if v == "mixed" else FP64
+            setattr(self.params, k, v)
+        self._check(self.lib.exafmm_b200_set_params(self.h, ctypes.byref(self.params)))
+
+    def set_bodies(self, bodies):
+        rec = as_records(bodies)
+        self.n = len(rec)
+        self._check(self.lib.exafmm_b200_set_bodies(self.h, _p(rec), self.n, HOST))
+
+    def set_bodies_device(self, ptr, n):
+        """Body records already in device memory (e.g. a torch tensor's data_ptr())."""
+        self.n = int(n)
+        self._check(self.lib.exafmm_b200_set_bodies(self.h, ctypes.c_void_p(ptr), self.n, DEVICE))
+
+    # ---- phases (3d/fmm.cxx:40-53)
+    def build_tree(self):
+        self._check(self.lib.exafmm_b200_build_tree(self.h))
+
+    def build_lists(self):
+        self._check(self.lib.exafmm_b200_build_lists(self.h))
+
+    def upward(self):
+        self._check(self.lib.exafmm_b200_upward(self.h))
+
+    def horizontal(self):
+        self._check(self.lib.exafmm_b200_horizontal(self.h))
+
+    def downward(self):
+        self._check(self.lib.exafmm_b200_downward(self.h))
+
+    def evaluate(self):
+        self._check(self.lib.exafmm_b200_evaluate(self.h))
+
+    # ---- results
+    def bodies(self):
+        out = np.zeros((self.n, 8))
+        self._check(self.lib.exafmm_b200_get_bodies(self.h, _p(out), HOST))
+        return out
+
+    def bodies_device(self, ptr):
+        self._check(self.lib.exafmm_b200_get_bodies(self.h, ctypes.c_void_p(ptr), DEVICE))
+
+    def perm(self):
+        out = np.zeros(self.n, np.int64)
+        self._check(self.lib.exafmm_b200_get_perm(self.h, _p(out), HOST))
+        return out
+
+    def num_cells(self):
+        return int(self.lib.exafmm_b200_num_cells(self.h))
+
+    def tree(self):
+        c = self.num_cells()
+        nchild, child, body, nbody, level = (np.zeros(c, np.int32) for _ in range(5))
+        xr = np.zeros((c, 4))
+        self._check(self.lib.exafmm_b200_get_tree(self.h, _p(nchild), _p(child), _p(body), _p(nbody), _p(level),
+                                                  _p(xr)))
+        return dict(nchild=nchild, child=child, body=body, nbody=nbody, level=level, xr=xr)
+
+    def lists(self):
+        a, b = np.zeros(1, np.int64), np.zeros(1, np.int64)
+        self._check(self.lib.exafmm_b200_count_lists(self.h, _p(a), _p(b)))
+        c = self.num_cells()
+        na, nb = int(a[0]), int(b[0])
+        mo, po = np.zeros(c + 1, np.int32), np.zeros(c + 1, np.int32)
+        ms, mi = np.zeros(max(na, 1), np.int32), np.zeros(max(na, 1), np.int32)
+        ps, pi = np.zeros(max(nb, 1), np.int32), np.zeros(max(nb, 1), np.int32)
+        self._check(self.lib.exafmm_b200_get_lists(self.h, _p(mo), _p(ms), _p(mi), _p(po), _p(ps), _p(pi)))
+        return dict(m2l_off=mo, m2l_src=ms[:na], m2l_img=mi[:na], p2p_off=po, p2p_src=ps[:nb], p2p_img=pi[:nb])
+
+    def expansions(self):
+        c, nt = self.num_cells(), self.params.P * (self.params.P + 1) // 2
+        M = np.zeros((c, nt, 2))
+        L = np.zeros((c, nt, 2))
+        self._check(self.lib.exafmm_b200_get_expansions(self.h, _p(M), _p(L)))
+        return M[..., 0] + 1j * M[..., 1], L[..., 0] + 1j * L[..., 1]
+
+    def direct(self, targets):
+        """FP64 direct sum of all loaded bodies onto targets (Body records; p, F accumulate)."""
+        t = as_records(targets).copy()
+        self._check(self.lib.exafmm_b200_direct(self.h, _p(t), len(t), HOST))
+        return t
+
+    def timings(self):
+        t = np.zeros(7)
+        self._check(self.lib.exafmm_b200_get_timings(self.h, _p(t)))
+        return dict(zip(PHASES, t.tolist()))
+
+    def last_launches(self):
+        return int(self.lib.exafmm_b200_last_launches(self.h))
+
+    def fma_peak(self, precision="fp64"):
+        t = np.zeros(1)
+        self._check(self.lib.exafmm_b200_fma_peak(self.h, FP64 if precision == "fp64" else MIXED, _p(t)))
+        return float(t[0])
+
+
+def rel_l2(a, b):
+    """Relative L2 error of a against b (the reference's verification metric, 3d/fmm.cxx:71-85)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))

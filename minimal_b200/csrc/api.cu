@@ -1,0 +1,422 @@
+// The C ABI (include/exafmm_b200.h): argument checking, phase ordering,
+// per-phase CUDA-event timing and the host<->device copies at the boundary.
+// Every entry point turns internal errors into a status code plus a message.
+#include <cstring>
+#include <new>
+
+#include "fmm.cuh"
+
+namespace fmm {
+double fma_peak_tflops(int precision);
+void m2l_set_attributes();
+void expansions_set_attributes();
+}  // namespace fmm
+
+using namespace fmm;
+
+struct exafmm_b200 {
+  Handle h;
+};
+
+namespace {
+
+thread_local std::string g_create_err;
+
+template <class F>
+int guarded(exafmm_b200 *H, F f) {
+  if (!H) return EXAFMM_ERR_ARG;
+  try {
+    f(H->h);
+    H->h.err.clear();
+    return EXAFMM_OK;
+  } catch (const Error &e) {
+    H->h.err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    H->h.err = "host allocation failed";
+    return EXAFMM_ERR_NOMEM;
+  }
+}
+
+void check_params(const exafmm_params &p) {
+  if (p.P < 1 || p.P > EXAFMM_MAX_P) throw Error{EXAFMM_ERR_ARG, "P must be in [1, 32]"};
+  if (p.ncrit < 1) throw Error{EXAFMM_ERR_ARG, "ncrit must be >= 1"};
+  if (!(p.theta > 0) || !(p.theta < 1e6)) throw Error{EXAFMM_ERR_ARG, "theta must be positive and finite"};
+  if (p.images < 0 || p.images > 12) throw Error{EXAFMM_ERR_ARG, "images must be in [0, 12]"};
+  if (p.images > 0 && !(p.cycle > 0)) throw Error{EXAFMM_ERR_ARG, "cycle must be positive when images > 0"};
+  if (p.precision != EXAFMM_FP64 && p.precision != EXAFMM_MIXED) throw Error{EXAFMM_ERR_ARG, "unknown precision"};
+}
+
+__global__ void k_pack_in(const double *rec, long n, double4 *in, int *bad) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double *r = rec + 8 * i;
+  const double4 v = make_double4(r[0], r[1], r[2], r[3]);
+  if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) *bad = 1;
+  in[i] = v;
+}
+
+__global__ void k_unpack_out(const double4 *src, const double4 *out, long n, double *rec) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 a = src[i], b = out[i];
+  double *r = rec + 8 * i;
+  r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
+  r[4] = b.x; r[5] = b.y; r[6] = b.z; r[7] = b.w;
+}
+
+__global__ void k_direct_prep(const double *rec, long n, double4 *xq, double4 *pf) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double *r = rec + 8 * i;
+  xq[i] = make_double4(r[0], r[1], r[2], r[3]);
+  pf[i] = make_double4(r[4], r[5], r[6], r[7]);
+}
+
+__global__ void k_direct_back(const double4 *pf, long n, double *rec) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double *r = rec + 8 * i;
+  r[4] = pf[i].x; r[5] = pf[i].y; r[6] = pf[i].z; r[7] = pf[i].w;
+}
+
+struct Timer {
+  Handle &h;
+  int ph;
+  Timer(Handle &h_, int p) : h(h_), ph(p) {
+    if (h.ev_ok) cudaEventRecord(h.ev[ph][0], h.stream);
+  }
+  ~Timer() {
+    if (h.ev_ok) cudaEventRecord(h.ev[ph][1], h.stream);
+  }
+};
+
+void need_tree(Handle &h) {
+  if (!h.have_tree) throw Error{EXAFMM_ERR_STATE, "build_tree() has not run on the current bodies"};
+}
+
+void do_tree(Handle &h) {
+  if (h.n <= 0) throw Error{EXAFMM_ERR_STATE, "no bodies loaded"};
+  Timer t(h, PH_TREE);
+  build_tree(h);
+  h.have_tree = true;
+  h.have_lists = h.have_up = h.have_horiz = h.have_down = false;
+}
+
+void do_lists(Handle &h) {
+  need_tree(h);
+  Timer t(h, PH_LISTS);
+  build_lists(h);
+  h.have_lists = true;
+}
+
+void do_up(Handle &h) {
+  need_tree(h);
+  Timer t(h, PH_UP);
+  upward_pass(h);
+  h.have_up = true;
+}
+
+void do_horiz(Handle &h) {
+  if (!h.have_up) throw Error{EXAFMM_ERR_STATE, "upward() must run before horizontal()"};
+  if (!h.have_lists) do_lists(h);
+  if (h.prm.images > 0) throw Error{EXAFMM_ERR_STATE, "periodic images are not available in this build"};
+  {
+    Timer t(h, PH_M2L);
+    m2l_pass(h);
+  }
+  {
+    Timer t(h, PH_P2P);
+    p2p_pass(h);
+  }
+  h.have_horiz = true;
+}
+
+void do_down(Handle &h) {
+  if (!h.have_horiz) throw Error{EXAFMM_ERR_STATE, "horizontal() must run before downward()"};
+  Timer t(h, PH_DOWN);
+  downward_pass(h);
+  h.have_down = true;
+}
+
+void sync(Handle &h) {
+  FMM_CUDA(cudaStreamSynchronize(h.stream));
+  if (h.ev_ok) {
+    for (int p = 0; p < PH_COUNT; p++) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, h.ev[p][0], h.ev[p][1]) == cudaSuccess) h.ms[p] = ms;
+      else { cudaGetLastError(); h.ms[p] = 0; }
+    }
+    float tot = 0;
+    if (cudaEventElapsedTime(&tot, h.ev[PH_TREE][0], h.ev[PH_DOWN][1]) == cudaSuccess) h.ms[PH_COUNT] = tot;
+    else cudaGetLastError();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int exafmm_b200_arch(void) { return 100; }
+
+int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
+  if (!params || !out) return EXAFMM_ERR_ARG;
+  *out = nullptr;
+  exafmm_b200 *H = new (std::nothrow) exafmm_b200();
+  if (!H) return EXAFMM_ERR_NOMEM;
+  try {
+    check_params(*params);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      throw Error{EXAFMM_ERR_NOGPU, "no CUDA device"};
+    }
+    if (params->device < 0 || params->device >= ndev) throw Error{EXAFMM_ERR_ARG, "device ordinal out of range"};
+    cudaDeviceProp prop;
+    FMM_CUDA(cudaGetDeviceProperties(&prop, params->device));
+    if (prop.major != 10) throw Error{EXAFMM_ERR_NOGPU, std::string("needs an sm_100 GPU, found ") + prop.name};
+    FMM_CUDA(cudaSetDevice(params->device));
+    Handle &h = H->h;
+    h.prm = *params;
+    h.nterm = nterm_of(params->P);
+    FMM_CUDA(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    h.ev_ok = true;
+    for (int p = 0; p < PH_COUNT + 1; p++)
+      for (int k = 0; k < 2; k++)
+        if (cudaEventCreate(&h.ev[p][k]) != cudaSuccess) h.ev_ok = false;
+    m2l_set_attributes();
+    expansions_set_attributes();
+    FMM_CUDA(cudaGetLastError());
+  } catch (const Error &e) {
+    g_create_err = e.msg;
+    delete H;
+    return e.code;
+  }
+  *out = H;
+  return EXAFMM_OK;
+}
+
+int exafmm_b200_destroy(exafmm_b200 *H) {
+  if (!H) return EXAFMM_ERR_ARG;
+  Handle &h = H->h;
+  cudaSetDevice(h.prm.device);
+  if (h.stream) cudaStreamSynchronize(h.stream);
+  Buf *bufs[] = {&h.in, &h.src, &h.out, &h.perm, &h.srcf, &h.keys[0], &h.keys[1], &h.vals[0], &h.vals[1],
+                 &h.lfirst, &h.chain, &h.prebase, &h.scan_tmp, &h.hist, &h.c_begin, &h.c_count, &h.c_child,
+                 &h.c_nchild, &h.c_parent, &h.c_level, &h.c_xr, &h.c_pre, &h.c_ref, &h.c_leaf_of_body,
+                 &h.leaves, &h.pre_tmp, &h.ctmp, &h.geom, &h.counters, &h.frontier[0], &h.frontier[1],
+                 &h.m2l_raw, &h.p2p_raw, &h.m2l_off, &h.m2l_ent, &h.p2p_off, &h.p2p_ent, &h.fill, &h.M, &h.L,
+                 &h.m2l_units, &h.stage};
+  for (Buf *b : bufs) b->release();
+  if (h.ev_ok)
+    for (int p = 0; p < PH_COUNT + 1; p++)
+      for (int k = 0; k < 2; k++) cudaEventDestroy(h.ev[p][k]);
+  if (h.stream) cudaStreamDestroy(h.stream);
+  delete H;
+  return EXAFMM_OK;
+}
+
+const char *exafmm_b200_last_error(const exafmm_b200 *H) {
+  if (!H) return g_create_err.c_str();
+  return H->h.err.c_str();
+}
+
+int exafmm_b200_set_params(exafmm_b200 *H, const exafmm_params *params) {
+  return guarded(H, [&](Handle &h) {
+    if (!params) throw Error{EXAFMM_ERR_ARG, "null params"};
+    check_params(*params);
+    if (params->device != h.prm.device) throw Error{EXAFMM_ERR_ARG, "a handle stays on its device"};
+    h.prm = *params;
+    h.nterm = nterm_of(params->P);
+    h.have_tree = h.have_lists = h.have_up = h.have_horiz = h.have_down = false;
+  });
+}
+
+int exafmm_b200_set_bodies(exafmm_b200 *H, const double *rec, int64_t n, int where) {
+  return guarded(H, [&](Handle &h) {
+    if (!rec || n <= 0) throw Error{EXAFMM_ERR_ARG, "need a body array with n > 0"};
+    if (n >= (1ll << 31)) throw Error{EXAFMM_ERR_ARG, "n must be below 2^31"};
+    if (where != EXAFMM_HOST && where != EXAFMM_DEVICE) throw Error{EXAFMM_ERR_ARG, "where must be HOST or DEVICE"};
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    h.n = n;
+    h.in.need(n * sizeof(double4));
+    h.counters.need(sizeof(DevCounters));
+    const double *drec = rec;
+    if (where == EXAFMM_HOST) {
+      h.stage.need(n * 8 * sizeof(double));
+      FMM_CUDA(cudaMemcpyAsync(h.stage.p, rec, n * 8 * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+      drec = h.stage.as<double>();
+    }
+    int *bad = &h.counters.as<DevCounters>()->overflow;
+    FMM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), h.stream));
+    k_pack_in<<<grid_for(n, 256), 256, 0, h.stream>>>(drec, n, h.in.as<double4>(), bad);
+    h.launches++;
+    FMM_LAUNCH();
+    int hb = 0;
+    FMM_CUDA(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    FMM_CUDA(cudaStreamSynchronize(h.stream));
+    if (hb) throw Error{EXAFMM_ERR_ARG, "non-finite body position or charge"};
+    h.have_tree = h.have_lists = h.have_up = h.have_horiz = h.have_down = false;
+  });
+}
+
+int exafmm_b200_build_tree(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) { do_tree(h); sync(h); });
+}
+int exafmm_b200_build_lists(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) { do_lists(h); sync(h); });
+}
+int exafmm_b200_upward(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) { do_up(h); sync(h); });
+}
+int exafmm_b200_horizontal(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) { do_horiz(h); sync(h); });
+}
+int exafmm_b200_downward(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) { do_down(h); sync(h); });
+}
+
+int exafmm_b200_evaluate(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) {
+    h.launches = 0;
+    do_tree(h);
+    do_lists(h);
+    do_up(h);
+    do_horiz(h);
+    do_down(h);
+    sync(h);
+  });
+}
+
+int exafmm_b200_get_bodies(exafmm_b200 *H, double *rec, int where) {
+  return guarded(H, [&](Handle &h) {
+    if (!rec) throw Error{EXAFMM_ERR_ARG, "null output"};
+    if (!h.have_down) throw Error{EXAFMM_ERR_STATE, "no completed evaluation"};
+    double *drec = rec;
+    if (where == EXAFMM_HOST) {
+      h.stage.need(h.n * 8 * sizeof(double));
+      drec = h.stage.as<double>();
+    }
+    k_unpack_out<<<grid_for(h.n, 256), 256, 0, h.stream>>>(h.src.as<double4>(), h.out.as<double4>(), h.n, drec);
+    FMM_LAUNCH();
+    if (where == EXAFMM_HOST)
+      FMM_CUDA(cudaMemcpyAsync(rec, drec, h.n * 8 * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    FMM_CUDA(cudaStreamSynchronize(h.stream));
+  });
+}
+
+int exafmm_b200_get_perm(exafmm_b200 *H, int64_t *perm, int where) {
+  return guarded(H, [&](Handle &h) {
+    need_tree(h);
+    if (!perm) throw Error{EXAFMM_ERR_ARG, "null output"};
+    std::vector<int> p(h.n);
+    FMM_CUDA(cudaMemcpy(p.data(), h.perm.p, h.n * 4, cudaMemcpyDeviceToHost));
+    std::vector<int64_t> q(p.begin(), p.end());
+    FMM_CUDA(cudaMemcpy(perm, q.data(), h.n * 8, where == EXAFMM_HOST ? cudaMemcpyHostToHost : cudaMemcpyHostToDevice));
+  });
+}
+
+int64_t exafmm_b200_num_cells(exafmm_b200 *H) { return H && H->h.have_tree ? H->h.ncells : -1; }
+
+int exafmm_b200_get_tree(exafmm_b200 *H, int *nchild, int *child, int *body, int *nbody, int *level, double *xr) {
+  return guarded(H, [&](Handle &h) {
+    need_tree(h);
+    const int C = h.ncells;
+    std::vector<int> nc(C), ch(C), bg(C), ct(C), lv(C), rf(C);
+    std::vector<double4> x(C);
+    FMM_CUDA(cudaMemcpy(nc.data(), h.c_nchild.p, C * 4, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpy(ch.data(), h.c_child.p, C * 4, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpy(bg.data(), h.c_begin.p, C * 4, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpy(ct.data(), h.c_count.p, C * 4, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpy(lv.data(), h.c_level.p, C * 4, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpy(rf.data(), h.c_ref.p, C * 4, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpy(x.data(), h.c_xr.p, C * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (int b = 0; b < C; b++) {
+      const int r = rf[b];
+      if (r < 0 || r >= C) throw Error{EXAFMM_ERR_STATE, "corrupt cell numbering"};
+      if (nchild) nchild[r] = nc[b];
+      if (child) child[r] = nc[b] ? rf[ch[b]] : -1;
+      if (body) body[r] = bg[b];
+      if (nbody) nbody[r] = ct[b];
+      if (level) level[r] = lv[b];
+      if (xr) { xr[4 * r] = x[b].x; xr[4 * r + 1] = x[b].y; xr[4 * r + 2] = x[b].z; xr[4 * r + 3] = x[b].w; }
+    }
+  });
+}
+
+int exafmm_b200_count_lists(exafmm_b200 *H, int64_t *a, int64_t *b) {
+  return guarded(H, [&](Handle &h) {
+    if (!h.have_lists) throw Error{EXAFMM_ERR_STATE, "lists not built"};
+    if (a) *a = h.n_m2l;
+    if (b) *b = h.n_p2p;
+  });
+}
+
+int exafmm_b200_get_lists(exafmm_b200 *H, int *mo, int *ms, int *mi, int *po, int *ps, int *pi) {
+  return guarded(H, [&](Handle &h) {
+    if (!h.have_lists) throw Error{EXAFMM_ERR_STATE, "lists not built"};
+    if (!mo || !ms || !mi || !po || !ps || !pi) throw Error{EXAFMM_ERR_ARG, "null output"};
+    export_lists(h, mo, ms, mi, po, ps, pi);
+  });
+}
+
+int exafmm_b200_get_expansions(exafmm_b200 *H, double *M, double *L) {
+  return guarded(H, [&](Handle &h) {
+    if (!h.have_up) throw Error{EXAFMM_ERR_STATE, "upward() has not run"};
+    const int C = h.ncells, nt = h.nterm;
+    std::vector<int> rf(C);
+    std::vector<double2> m((size_t)C * nt), l((size_t)C * nt);
+    FMM_CUDA(cudaMemcpy(rf.data(), h.c_ref.p, C * 4, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpy(m.data(), h.M.p, (size_t)C * nt * 16, cudaMemcpyDeviceToHost));
+    if (h.have_horiz) FMM_CUDA(cudaMemcpy(l.data(), h.L.p, (size_t)C * nt * 16, cudaMemcpyDeviceToHost));
+    for (int b = 0; b < C; b++)
+      for (int k = 0; k < nt; k++) {
+        const size_t d = ((size_t)rf[b] * nt + k) * 2, s = (size_t)b * nt + k;
+        if (M) { M[d] = m[s].x; M[d + 1] = m[s].y; }
+        if (L) { L[d] = l[s].x; L[d + 1] = l[s].y; }
+      }
+  });
+}
+
+int exafmm_b200_direct(exafmm_b200 *H, double *targets, int64_t nt, int where) {
+  return guarded(H, [&](Handle &h) {
+    need_tree(h);
+    if (!targets || nt <= 0) throw Error{EXAFMM_ERR_ARG, "need targets"};
+    Buf rec, xq, pf;
+    rec.need(nt * 64);
+    xq.need(nt * sizeof(double4));
+    pf.need(nt * sizeof(double4));
+    FMM_CUDA(cudaMemcpyAsync(rec.p, targets, nt * 64, where == EXAFMM_HOST ? cudaMemcpyHostToDevice
+                                                                          : cudaMemcpyDeviceToDevice, h.stream));
+    k_direct_prep<<<grid_for(nt, 256), 256, 0, h.stream>>>(rec.as<double>(), nt, xq.as<double4>(), pf.as<double4>());
+    FMM_LAUNCH();
+    direct_sum(h, xq.as<double4>(), pf.as<double4>(), nt);
+    k_direct_back<<<grid_for(nt, 256), 256, 0, h.stream>>>(pf.as<double4>(), nt, rec.as<double>());
+    FMM_LAUNCH();
+    FMM_CUDA(cudaMemcpyAsync(targets, rec.p, nt * 64, where == EXAFMM_HOST ? cudaMemcpyDeviceToHost
+                                                                          : cudaMemcpyDeviceToDevice, h.stream));
+    FMM_CUDA(cudaStreamSynchronize(h.stream));
+    rec.release();
+    xq.release();
+    pf.release();
+  });
+}
+
+int exafmm_b200_get_timings(exafmm_b200 *H, double *ms7) {
+  return guarded(H, [&](Handle &h) {
+    if (!ms7) throw Error{EXAFMM_ERR_ARG, "null output"};
+    for (int p = 0; p <= PH_COUNT; p++) ms7[p] = h.ms[p];
+  });
+}
+
+int64_t exafmm_b200_last_launches(exafmm_b200 *H) { return H ? H->h.launches : -1; }
+
+int exafmm_b200_fma_peak(exafmm_b200 *H, int precision, double *tflops) {
+  return guarded(H, [&](Handle &h) {
+    if (!tflops) throw Error{EXAFMM_ERR_ARG, "null output"};
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    *tflops = fma_peak_tflops(precision);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+// Internal definitions of the exafmm_b200 library: the handle, device buffer
+// management, error plumbing and the launchers each .cu file provides.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/exafmm_b200.h"
+
+namespace fmm {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define FMM_CUDA(call)                                                                                     \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess)                                                                                 \
+      throw ::fmm::Error{EXAFMM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +   \
+                                              __FILE__ + ":" + std::to_string(__LINE__)};                  \
+  } while (0)
+
+#define FMM_LAUNCH()                                                                                       \
+  do {                                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                                   \
+    if (e_ != cudaSuccess)                                                                                 \
+      throw ::fmm::Error{EXAFMM_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_) + " at " + \
+                                              __FILE__ + ":" + std::to_string(__LINE__)};                  \
+  } while (0)
+
+// A device allocation that grows on demand and is kept between evaluations.
+struct Buf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  template <class T>
+  T *as() const { return (T *)p; }
+  void need(size_t b) {
+    if (b <= bytes) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t nb = b + b / 4 + 256;
+    if (cudaMalloc(&p, nb) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{EXAFMM_ERR_NOMEM, "cudaMalloc of " + std::to_string(nb) + " bytes failed"};
+    }
+    bytes = nb;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+// Geometry of the root cell, computed on the device (bounds kernel).
+struct RootGeom {
+  double X0[3];
+  double R0;
+};
+
+// Counters written by device code and read once per phase by the host.
+struct DevCounters {
+  int ncells;          // cells in the tree
+  int level_count[EXAFMM_MAX_LEVEL + 2];
+  int overflow;        // a cell at the deepest key level still had > ncrit bodies
+  int nleaves;
+  unsigned long long n_m2l, n_p2p;  // emitted list entries (may exceed capacity)
+  unsigned long long frontier[2];   // BFS pair frontier sizes (ping-pong)
+  int list_overflow;   // an emission or the frontier exceeded its capacity
+  int max_m2l_seg, max_p2p_seg;
+};
+
+// Per-phase timing slots (CUDA events on the handle stream).
+enum Phase { PH_TREE = 0, PH_LISTS, PH_UP, PH_M2L, PH_P2P, PH_DOWN, PH_COUNT };
+
+struct Handle {
+  exafmm_params prm{};
+  int nterm = 0;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+
+  // bodies
+  int64_t n = 0;
+  Buf in;      // double4 (x,y,z,q), caller order
+  Buf src;     // double4 (x,y,z,q), tree order
+  Buf out;     // double4 (p,Fx,Fy,Fz), tree order
+  Buf perm;    // int, tree position -> input index
+  Buf srcf;    // float4 (x,y,z rel. to leaf centre, q), tree order (mixed form)
+  Buf stage;   // staging for Body records crossing the boundary
+
+  // tree build scratch
+  Buf keys[2], vals[2];  // radix sort ping-pong (u64 keys, u32 values)
+  Buf lfirst, chain, prebase, scan_tmp, hist;
+  int key_levels = 0;
+
+  // tree (BFS order: by level, then first body)
+  int ncells = 0, nleaves = 0, depth = 0;
+  int level_base[EXAFMM_MAX_LEVEL + 3] = {0};
+  Buf c_begin, c_count, c_child, c_nchild, c_parent, c_level, c_xr, c_pre, c_ref, c_leaf_of_body;
+  Buf leaves;  // BFS indices of leaves
+  Buf pre_tmp; // preorder tables
+  Buf ctmp;    // cell-count scratch (level sort, index maps)
+  Buf geom;    // RootGeom
+  Buf counters;  // DevCounters
+  DevCounters hc{};  // host copy
+
+  // lists (CSR by target, BFS indices)
+  Buf frontier[2];
+  size_t frontier_cap = 0;
+  Buf m2l_raw, p2p_raw;  // emitted (tgt, src|img) pairs
+  size_t m2l_cap = 0, p2p_cap = 0;
+  Buf m2l_off, m2l_ent, p2p_off, p2p_ent, fill;
+  int64_t n_m2l = 0, n_p2p = 0;
+
+  // expansions
+  Buf M, L;   // double2 [ncells][nterm]
+  Buf m2l_units;  // balanced contraction table for the M2L kernel (per P)
+  int m2l_units_P = -1;
+
+  // phase state
+  bool have_tree = false, have_lists = false, have_up = false, have_horiz = false, have_down = false;
+
+  cudaEvent_t ev[PH_COUNT + 1][2];
+  float ms[PH_COUNT + 1] = {0};
+  bool ev_ok = false;
+};
+
+// ---- launchers (each .cu file) ----
+// scan.cu / sort.cu
+void scan_exclusive_int(Handle &h, const int *in, int *out, long n, int *total_dev);
+void radix_sort_pairs(Handle &h, u64 *&k, u32 *&v, u64 *&k2, u32 *&v2, long n, int lo_bit, int hi_bit);
+// tree.cu
+void build_tree(Handle &h);
+// lists.cu
+void build_lists(Handle &h);
+void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img);
+// expansions.cu
+void upward_pass(Handle &h);
+void downward_pass(Handle &h);
+// m2l.cu
+void m2l_pass(Handle &h);
+// p2p.cu
+void p2p_pass(Handle &h);
+void direct_sum(Handle &h, double4 *targets_pq /*x,y,z,q*/, double4 *out, long nt);
+
+inline int nterm_of(int P) { return P * (P + 1) / 2; }
+inline unsigned grid_for(long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace fmm

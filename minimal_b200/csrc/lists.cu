@@ -1,0 +1,299 @@
+// GPU interaction-list builder: the reference's dual-tree traversal
+// (3d/traverse_eager.h:147-165, recorded as lists by 3d/traverse_lazy.h:27-44;
+// periodic shifts 3dp/traverse_lazy.h:39-58 and the 27-image loop :276-293)
+// run breadth first over a frontier of (target, source, image) cell pairs.
+//
+// Each step applies the reference's branch rules to every pair of the
+// frontier with the same rounded FP64 arithmetic (no FMA):
+//   |Xi - Xj - iX*cycle|^2 * theta^2 > (Ri + Rj)^2  -> M2L entry
+//   else both leaves                                 -> P2P entry
+//   else Cj leaf or (Ri >= Rj and Ci not a leaf)     -> (children of Ci, Cj)
+//   else                                             -> (Ci, children of Cj)
+// Emission uses warp-aggregated atomics.  The entries are then bucketed per
+// target cell (CSR) and each target's entries are ordered as the recursion
+// would have recorded them: image-loop order first (x outermost), then the
+// source's depth-first pre-order rank (a depth-first walk meets the sources
+// of one target in pre-order, because a target-side split never reorders
+// them).  The result equals getList's per-cell lists entry for entry.
+#include "fmm.cuh"
+
+namespace fmm {
+
+namespace {
+
+constexpr int TB = 256;
+constexpr int IMG_SHIFT = 26;             // entry = src | img << 26
+constexpr u32 IDX_MASK = (1u << IMG_SHIFT) - 1;
+
+struct CellView {
+  const double4 *xr;
+  const int *child, *nchild;
+};
+
+__device__ __forceinline__ void img3(int img, int &x, int &y, int &z) {
+  x = img % 3 - 1;
+  y = (img / 3) % 3 - 1;
+  z = img / 9 - 1;
+}
+
+// Warp-aggregated append of k items: returns this lane's first slot.
+__device__ __forceinline__ unsigned long long warp_append(unsigned long long *ctr, int k) {
+  const int lane = threadIdx.x & 31;
+  int incl = k;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && total) base = atomicAdd(ctr, (unsigned long long)total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return base + (unsigned long long)(incl - k);
+}
+
+__global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const unsigned long long *nin_p,
+                                            int2 *fout, unsigned long long *nout, u64 fcap, int2 *m2l,
+                                            unsigned long long *nm2l, u64 mcap, int2 *p2p,
+                                            unsigned long long *np2p, u64 pcap, double theta, double cycle,
+                                            int *overflow) {
+  const u64 nin = *nin_p;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  // every lane of a warp iterates the same number of times (warp-wide appends)
+  for (u64 base = (u64)blockIdx.x * blockDim.x; base < nin; base += stride) {
+    const u64 idx = base + threadIdx.x;
+    const bool act = idx < nin;
+    int i = 0, j = 0, img = 13, kind = -1;  // 0 m2l, 1 p2p, 2 split i, 3 split j
+    int nk = 0, first = 0;
+    if (act) {
+      const int2 pr = fin[idx];
+      i = pr.x & (int)IDX_MASK;
+      img = (int)((u32)pr.x >> IMG_SHIFT);
+      j = pr.y;
+      int ix, iy, iz;
+      img3(img, ix, iy, iz);
+      const double4 a = cv.xr[i], b = cv.xr[j];
+      const double dx = __dadd_rn(__dadd_rn(a.x, -b.x), -__dmul_rn((double)ix, cycle));
+      const double dy = __dadd_rn(__dadd_rn(a.y, -b.y), -__dmul_rn((double)iy, cycle));
+      const double dz = __dadd_rn(__dadd_rn(a.z, -b.z), -__dmul_rn((double)iz, cycle));
+      const double nrm = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      const double R2 = __dmul_rn(__dmul_rn(nrm, theta), theta);
+      const double rs = __dadd_rn(a.w, b.w);
+      const int ci = cv.nchild[i], cj = cv.nchild[j];
+      if (R2 > __dmul_rn(rs, rs)) {
+        kind = 0;
+      } else if (ci == 0 && cj == 0) {
+        kind = 1;
+      } else if (cj == 0 || (a.w >= b.w && ci != 0)) {
+        kind = 2;
+        nk = ci;
+        first = cv.child[i];
+      } else {
+        kind = 3;
+        nk = cj;
+        first = cv.child[j];
+      }
+    }
+    const int packed_i = i | (img << IMG_SHIFT);
+    {
+      const unsigned long long s = warp_append(nm2l, kind == 0);
+      if (kind == 0) {
+        if (s < mcap) m2l[s] = make_int2(packed_i, j); else *overflow = 1;
+      }
+    }
+    {
+      const unsigned long long s = warp_append(np2p, kind == 1);
+      if (kind == 1) {
+        if (s < pcap) p2p[s] = make_int2(packed_i, j); else *overflow = 1;
+      }
+    }
+    {
+      const unsigned long long s = warp_append(nout, nk);
+      for (int c = 0; c < nk; c++) {
+        if (s + c < fcap) {
+          fout[s + c] = kind == 2 ? make_int2((first + c) | (img << IMG_SHIFT), j) : make_int2(packed_i, first + c);
+        } else {
+          *overflow = 1;
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_seed(int2 *f, unsigned long long *n, int images) {
+  const int t = threadIdx.x;
+  if (images == 0) {
+    if (t == 0) { f[0] = make_int2(0 | (13 << IMG_SHIFT), 0); *n = 1; }
+  } else if (t < 27) {
+    // image loop order of the reference: x outermost, z innermost; img is
+    // periodic1D = (x+1) + 3(y+1) + 9(z+1)
+    const int x = t / 9 - 1, y = (t / 3) % 3 - 1, z = t % 3 - 1;
+    const int img = (x + 1) + 3 * (y + 1) + 9 * (z + 1);
+    f[t] = make_int2(0 | (img << IMG_SHIFT), 0);
+    if (t == 0) *n = 27;
+  }
+}
+
+__global__ void k_zero_u64(unsigned long long *p) { *p = 0; }
+
+__global__ void k_count_tgt(const int2 *e, const unsigned long long *n_p, int *cnt) {
+  const u64 n = *n_p;
+  for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[e[k].x & (int)IDX_MASK], 1);
+}
+
+__global__ void k_bucket(const int2 *e, const unsigned long long *n_p, const int *off, int *fill, u32 *ent) {
+  const u64 n = *n_p;
+  for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x) {
+    const int2 v = e[k];
+    const int t = v.x & (int)IDX_MASK;
+    const u32 img = (u32)v.x >> IMG_SHIFT;
+    const int pos = off[t] + atomicAdd(&fill[t], 1);
+    ent[pos] = (u32)v.y | (img << IMG_SHIFT);
+  }
+}
+
+// Recording order of the reference inside one target's list.
+__device__ __forceinline__ u64 order_key(u32 e, const int *pre) {
+  const u32 img = e >> IMG_SHIFT;
+  const u32 x = img % 3, y = (img / 3) % 3, z = img / 9;  // (x+1),(y+1),(z+1)
+  const u64 loop = x * 9 + y * 3 + z;                     // x outermost
+  return (loop << 32) | (u64)(u32)pre[e & IDX_MASK];
+}
+
+// One warp per target: rank sort of the target's entries by order_key, keys
+// staged in shared memory (segments longer than SEG_SMEM rank from global).
+constexpr int SEG_WARPS = 4;
+constexpr int SEG_SMEM = 512;
+
+__global__ void __launch_bounds__(SEG_WARPS * 32) k_order_segments(const int *off, int ncells, const u32 *in,
+                                                                  u32 *out, const int *pre) {
+  __shared__ u64 keys[SEG_WARPS][SEG_SMEM];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * SEG_WARPS + wid;
+  if (w >= ncells) return;
+  const int b = off[w], m = off[w + 1] - b;
+  if (m <= SEG_SMEM) {
+    for (int a = lane; a < m; a += 32) keys[wid][a] = order_key(in[b + a], pre);
+    __syncwarp();
+    for (int a = lane; a < m; a += 32) {
+      const u64 key = keys[wid][a];
+      int r = 0;
+      for (int k = 0; k < m; k++) r += keys[wid][k] < key;
+      out[b + r] = in[b + a];
+    }
+  } else {
+    for (int a = lane; a < m; a += 32) {
+      const u32 e = in[b + a];
+      const u64 key = order_key(e, pre);
+      int r = 0;
+      for (int k = 0; k < m; k++) r += order_key(in[b + k], pre) < key;
+      out[b + r] = e;
+    }
+  }
+}
+
+}  // namespace
+
+static void bucket(Handle &h, const int2 *raw, unsigned long long *n_dev, int64_t n, Buf &off_b, Buf &ent_b) {
+  cudaStream_t s = h.stream;
+  const int C = h.ncells;
+  off_b.need((size_t)(C + 1) * 4);
+  ent_b.need((size_t)(n > 0 ? n : 1) * 4 * 2);
+  h.fill.need((size_t)(C + 1) * 4);
+  int *cnt = h.fill.as<int>();
+  FMM_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(C + 1) * 4, s));
+  const int g = 148 * 8;
+  k_count_tgt<<<g, TB, 0, s>>>(raw, n_dev, cnt);
+  scan_exclusive_int(h, cnt, off_b.as<int>(), C + 1, nullptr);
+  FMM_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(C + 1) * 4, s));
+  u32 *tmp = ent_b.as<u32>() + (n > 0 ? n : 1);
+  k_bucket<<<g, TB, 0, s>>>(raw, n_dev, off_b.as<int>(), cnt, tmp);
+  k_order_segments<<<grid_for(C, SEG_WARPS), SEG_WARPS * 32, 0, s>>>(off_b.as<int>(), C, tmp, ent_b.as<u32>(),
+                                                                    h.c_pre.as<int>());
+  h.launches += 3;
+  FMM_LAUNCH();
+}
+
+void build_lists(Handle &h) {
+  cudaStream_t s = h.stream;
+  DevCounters *ctr = h.counters.as<DevCounters>();
+  const int C = h.ncells;
+  if (h.frontier_cap == 0) {
+    h.frontier_cap = (size_t)C * 64 + 1024;
+    h.m2l_cap = (size_t)C * 200 + 1024;
+    h.p2p_cap = (size_t)h.nleaves * 90 + 1024;
+  }
+  const int images = h.prm.images;
+  for (int attempt = 0;; attempt++) {
+    h.frontier[0].need(h.frontier_cap * sizeof(int2));
+    h.frontier[1].need(h.frontier_cap * sizeof(int2));
+    h.m2l_raw.need(h.m2l_cap * sizeof(int2));
+    h.p2p_raw.need(h.p2p_cap * sizeof(int2));
+    FMM_CUDA(cudaMemsetAsync(&ctr->n_m2l, 0, sizeof(unsigned long long) * 4, s));
+    FMM_CUDA(cudaMemsetAsync(&ctr->list_overflow, 0, sizeof(int), s));
+    k_seed<<<1, 32, 0, s>>>(h.frontier[0].as<int2>(), &ctr->frontier[0], images);
+    h.launches++;
+    CellView cv{h.c_xr.as<double4>(), h.c_child.as<int>(), h.c_nchild.as<int>()};
+    const int steps = 2 * h.depth + 3;
+    for (int st = 0; st < steps; st++) {
+      const int a = st & 1, b = a ^ 1;
+      k_zero_u64<<<1, 1, 0, s>>>(&ctr->frontier[b]);
+      k_walk<<<148 * 8, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[a], h.frontier[b].as<int2>(),
+                                    &ctr->frontier[b], h.frontier_cap, h.m2l_raw.as<int2>(), &ctr->n_m2l, h.m2l_cap,
+                                    h.p2p_raw.as<int2>(), &ctr->n_p2p, h.p2p_cap, h.prm.theta,
+                                    images ? h.prm.cycle : 0.0, &ctr->list_overflow);
+      h.launches += 2;
+      FMM_LAUNCH();
+    }
+    FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    const unsigned long long left = h.hc.frontier[steps & 1];
+    if (left != 0)
+      throw Error{EXAFMM_ERR_STATE, "dual-tree walk did not finish in 2*depth+3 steps"};
+    if (h.hc.list_overflow) {
+      if (attempt >= 4) throw Error{EXAFMM_ERR_CAPACITY, "interaction list buffers kept overflowing"};
+      h.m2l_cap = std::max<size_t>(h.m2l_cap, (size_t)(h.hc.n_m2l * 5 / 4 + 1024));
+      h.p2p_cap = std::max<size_t>(h.p2p_cap, (size_t)(h.hc.n_p2p * 5 / 4 + 1024));
+      h.frontier_cap *= 2;
+      continue;
+    }
+    break;
+  }
+  h.n_m2l = (int64_t)h.hc.n_m2l;
+  h.n_p2p = (int64_t)h.hc.n_p2p;
+  bucket(h, h.m2l_raw.as<int2>(), &ctr->n_m2l, h.n_m2l, h.m2l_off, h.m2l_ent);
+  bucket(h, h.p2p_raw.as<int2>(), &ctr->n_p2p, h.n_p2p, h.p2p_off, h.p2p_ent);
+}
+
+// Lists in the reference's cell numbering (host arrays, CSR over ref index).
+void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img) {
+  const int C = h.ncells;
+  std::vector<int> ref(C), moff(C + 1), poff(C + 1);
+  std::vector<u32> ment(h.n_m2l > 0 ? h.n_m2l : 1), pent(h.n_p2p > 0 ? h.n_p2p : 1);
+  FMM_CUDA(cudaMemcpy(ref.data(), h.c_ref.p, C * 4, cudaMemcpyDeviceToHost));
+  FMM_CUDA(cudaMemcpy(moff.data(), h.m2l_off.p, (C + 1) * 4, cudaMemcpyDeviceToHost));
+  FMM_CUDA(cudaMemcpy(poff.data(), h.p2p_off.p, (C + 1) * 4, cudaMemcpyDeviceToHost));
+  if (h.n_m2l) FMM_CUDA(cudaMemcpy(ment.data(), h.m2l_ent.p, h.n_m2l * 4, cudaMemcpyDeviceToHost));
+  if (h.n_p2p) FMM_CUDA(cudaMemcpy(pent.data(), h.p2p_ent.p, h.n_p2p * 4, cudaMemcpyDeviceToHost));
+  std::vector<int> bfs_of_ref(C);
+  for (int b = 0; b < C; b++) bfs_of_ref[ref[b]] = b;
+  int a = 0, q = 0;
+  for (int r = 0; r < C; r++) {
+    const int b = bfs_of_ref[r];
+    m2l_off[r] = a;
+    p2p_off[r] = q;
+    for (int k = moff[b]; k < moff[b + 1]; k++, a++) {
+      m2l_src[a] = ref[ment[k] & IDX_MASK];
+      m2l_img[a] = (int)(ment[k] >> IMG_SHIFT);
+    }
+    for (int k = poff[b]; k < poff[b + 1]; k++, q++) {
+      p2p_src[q] = ref[pent[k] & IDX_MASK];
+      p2p_img[q] = (int)(pent[k] >> IMG_SHIFT);
+    }
+  }
+  m2l_off[C] = a;
+  p2p_off[C] = q;
+}
+
+}  // namespace fmm
