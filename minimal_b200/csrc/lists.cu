@@ -57,7 +57,9 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
                                             unsigned long long *nm2l, u64 mcap, int2 *p2p,
                                             unsigned long long *np2p, u64 pcap, double theta, double cycle,
                                             int *overflow) {
-  const u64 nin = *nin_p;
+  // the producer counts appends past its capacity (to size the retry); only
+  // the stored entries may be read
+  const u64 nin = min((u64)*nin_p, fcap);
   const u64 stride = (u64)gridDim.x * blockDim.x;
   // every lane of a warp iterates the same number of times (warp-wide appends)
   for (u64 base = (u64)blockIdx.x * blockDim.x; base < nin; base += stride) {
@@ -136,14 +138,15 @@ __global__ void k_seed(int2 *f, unsigned long long *n, int images) {
 
 __global__ void k_zero_u64(unsigned long long *p) { *p = 0; }
 
-__global__ void k_count_tgt(const int2 *e, const unsigned long long *n_p, int *cnt) {
-  const u64 n = *n_p;
+__global__ void k_count_tgt(const int2 *e, const unsigned long long *n_p, u64 cap, int *cnt) {
+  const u64 n = min((u64)*n_p, cap);
   for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x)
     atomicAdd(&cnt[e[k].x & (int)IDX_MASK], 1);
 }
 
-__global__ void k_bucket(const int2 *e, const unsigned long long *n_p, const int *off, int *fill, u32 *ent) {
-  const u64 n = *n_p;
+__global__ void k_bucket(const int2 *e, const unsigned long long *n_p, u64 cap, const int *off, int *fill,
+                         u32 *ent) {
+  const u64 n = min((u64)*n_p, cap);
   for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x) {
     const int2 v = e[k];
     const int t = v.x & (int)IDX_MASK;
@@ -204,11 +207,11 @@ static void bucket(Handle &h, const int2 *raw, unsigned long long *n_dev, int64_
   int *cnt = h.fill.as<int>();
   FMM_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(C + 1) * 4, s));
   const int g = 148 * 8;
-  k_count_tgt<<<g, TB, 0, s>>>(raw, n_dev, cnt);
+  k_count_tgt<<<g, TB, 0, s>>>(raw, n_dev, (u64)n, cnt);
   scan_exclusive_int(h, cnt, off_b.as<int>(), C + 1, nullptr);
   FMM_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(C + 1) * 4, s));
   u32 *tmp = ent_b.as<u32>() + (n > 0 ? n : 1);
-  k_bucket<<<g, TB, 0, s>>>(raw, n_dev, off_b.as<int>(), cnt, tmp);
+  k_bucket<<<g, TB, 0, s>>>(raw, n_dev, (u64)n, off_b.as<int>(), cnt, tmp);
   k_order_segments<<<grid_for(C, SEG_WARPS), SEG_WARPS * 32, 0, s>>>(off_b.as<int>(), C, tmp, ent_b.as<u32>(),
                                                                     h.c_pre.as<int>());
   h.launches += 3;
@@ -219,11 +222,10 @@ void build_lists(Handle &h) {
   cudaStream_t s = h.stream;
   DevCounters *ctr = h.counters.as<DevCounters>();
   const int C = h.ncells;
-  if (h.frontier_cap == 0) {
-    h.frontier_cap = (size_t)C * 64 + 1024;
-    h.m2l_cap = (size_t)C * 200 + 1024;
-    h.p2p_cap = (size_t)h.nleaves * 90 + 1024;
-  }
+  // capacities: kept between calls, never below a size estimate for this tree
+  h.frontier_cap = std::max<size_t>(h.frontier_cap, (size_t)C * 256 + 4096);
+  h.m2l_cap = std::max<size_t>(h.m2l_cap, (size_t)C * 200 + 1024);
+  h.p2p_cap = std::max<size_t>(h.p2p_cap, (size_t)h.nleaves * 90 + 1024);
   const int images = h.prm.images;
   for (int attempt = 0;; attempt++) {
     h.frontier[0].need(h.frontier_cap * sizeof(int2));
@@ -248,16 +250,17 @@ void build_lists(Handle &h) {
     }
     FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
     FMM_CUDA(cudaStreamSynchronize(s));
-    const unsigned long long left = h.hc.frontier[steps & 1];
-    if (left != 0)
-      throw Error{EXAFMM_ERR_STATE, "dual-tree walk did not finish in 2*depth+3 steps"};
     if (h.hc.list_overflow) {
+      // a dropped frontier pair also hides its descendants' entries: grow
+      // everything and walk again
       if (attempt >= 4) throw Error{EXAFMM_ERR_CAPACITY, "interaction list buffers kept overflowing"};
-      h.m2l_cap = std::max<size_t>(h.m2l_cap, (size_t)(h.hc.n_m2l * 5 / 4 + 1024));
-      h.p2p_cap = std::max<size_t>(h.p2p_cap, (size_t)(h.hc.n_p2p * 5 / 4 + 1024));
-      h.frontier_cap *= 2;
+      h.m2l_cap = std::max<size_t>(2 * h.m2l_cap, (size_t)(h.hc.n_m2l * 5 / 4 + 1024));
+      h.p2p_cap = std::max<size_t>(2 * h.p2p_cap, (size_t)(h.hc.n_p2p * 5 / 4 + 1024));
+      h.frontier_cap *= 4;
       continue;
     }
+    if (h.hc.frontier[steps & 1] != 0)
+      throw Error{EXAFMM_ERR_STATE, "dual-tree walk did not finish in 2*depth+3 steps"};
     break;
   }
   h.n_m2l = (int64_t)h.hc.n_m2l;

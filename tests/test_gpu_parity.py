@@ -155,7 +155,7 @@ def test_direct_vs_oracle(port):
     fmm.set_bodies(xq)
     fmm.build_tree()
     tgt = np.zeros((300, 8))
-    tgt[:, :4] = xq[::67][:300]
+    tgt[:, :4] = xq[::66][:300]
     d = fmm.direct(tgt)
     src = np.zeros((len(xq), 8))
     src[:, :4] = xq
