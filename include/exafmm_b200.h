@@ -141,6 +141,25 @@ EXAFMM_API int exafmm_b200_arch(void);
  * FP32 rooflines. */
 EXAFMM_API int exafmm_b200_fma_peak(exafmm_b200 *h, int precision, double *tflops);
 
+/* Direct summation that allocates nothing.  No counterpart in the reference:
+ * it exists for callers that may not allocate device memory -- programs that
+ * hand all of HBM to their own pool at start-up, or loops that must never
+ * enter the CUDA allocator -- and so cannot create a handle.  sources8 (ns
+ * Body records) and targets8 (nt Body records) are device pointers owned by
+ * the caller; p and F of the targets accumulate, in FP64, as in
+ * exafmm_b200_direct().  The only other memory used is a fixed scratch array
+ * built into the library (two 32-byte records per target, 4 MiB per GPU that
+ * loads the library, kept until exit), so nt may not exceed
+ * EXAFMM_DIRECT_STATIC_MAX_TARGETS (larger nt returns EXAFMM_ERR_ARG).  The
+ * work is queued on `stream` (a cudaStream_t; NULL = default stream) and the
+ * call returns without waiting.  All calls share the scratch: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first
+ * call on each device looks up the scratch address; make it before any
+ * stream capture.  Errors: exafmm_b200_last_error(NULL). */
+#define EXAFMM_DIRECT_STATIC_MAX_TARGETS 65536
+EXAFMM_API int exafmm_b200_direct_static(const double *sources8, int64_t ns, double *targets8, int64_t nt,
+                                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,7 +36,7 @@ API = [
     "exafmm_b200_horizontal", "exafmm_b200_downward", "exafmm_b200_evaluate", "exafmm_b200_get_bodies",
     "exafmm_b200_get_perm", "exafmm_b200_num_cells", "exafmm_b200_get_tree", "exafmm_b200_count_lists",
     "exafmm_b200_get_lists", "exafmm_b200_get_expansions", "exafmm_b200_direct", "exafmm_b200_get_timings",
-    "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak",
+    "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak", "exafmm_b200_direct_static",
 ]
 
 PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
@@ -90,6 +90,7 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_last_launches": (i64, [vp]),
         "exafmm_b200_arch": (i, []),
         "exafmm_b200_fma_peak": (i, [vp, i, vp]),
+        "exafmm_b200_direct_static": (i, [vp, i64, vp, i64, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

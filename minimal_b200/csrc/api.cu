@@ -18,9 +18,12 @@ struct exafmm_b200 {
   Handle h;
 };
 
+// Message of the last failed call on this thread that had no handle to hold
+// it (create, direct_static); read back through exafmm_b200_last_error(NULL).
+thread_local std::string exafmm_b200_static_err;
+
 namespace {
 
-thread_local std::string g_create_err;
 
 template <class F>
 int guarded(exafmm_b200 *H, F f) {
@@ -188,7 +191,7 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     expansions_set_attributes();
     FMM_CUDA(cudaGetLastError());
   } catch (const Error &e) {
-    g_create_err = e.msg;
+    exafmm_b200_static_err = e.msg;
     delete H;
     return e.code;
   }
@@ -217,7 +220,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
 }
 
 const char *exafmm_b200_last_error(const exafmm_b200 *H) {
-  if (!H) return g_create_err.c_str();
+  if (!H) return exafmm_b200_static_err.c_str();
   return H->h.err.c_str();
 }
 
