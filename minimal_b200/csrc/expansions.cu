@@ -23,7 +23,38 @@ __device__ __forceinline__ double2 ylook(const double2 *Y, int n, int o) {
 
 __device__ __forceinline__ int sgn(int n) { return (n & 1) ? -1 : 1; }
 
-// P2M (3d/kernel.h:187-202): M[n][m] += q * Y_n^m(rho, alpha, -beta).
+// 1/k for the Legendre and factorial recurrences (k = 1..2*EXAFMM_MAX_P+2).
+__constant__ double c_recip[2 * EXAFMM_MAX_P + 4];
+
+// All regular harmonics of one offset, generated order by order: calls
+// f(n, m, Y_n^m, dY_n^m) for m = 0..P-1, n = m..P-1, in that (uniform) order
+// so that lanes working on different bodies stay in lock step.
+template <bool WITH_DY, class F>
+__device__ __forceinline__ void regular_all(int P, const Sph &g, double2 e1, F f) {
+  double2 em = make_double2(1, 0);
+  double pmm = 1, odd = 1, cm = 1;
+  for (int m = 0; m < P; m++) {
+    double p = pmm, p1 = 0, cn = cm;
+    for (int n = m; n < P; n++) {
+      const double pn1 = n == m ? g.c * (2 * m + 1) * p : (g.c * (2 * n + 1) * p - (n + m) * p1) * c_recip[n - m + 1];
+      const double2 Y = cscale(em, cn * p);
+      double2 dY = make_double2(0, 0);
+      if (WITH_DY) dY = cscale(em, cn * ((n - m + 1) * pn1 - (n + 1) * g.c * p) * g.inv_s);
+      f(n, m, Y, dY);
+      p1 = p;
+      p = pn1;
+      cn *= -g.r * c_recip[n + 1 + m];
+    }
+    cm *= -g.r * c_recip[2 * m + 2] * c_recip[2 * m + 1];
+    pmm = -pmm * odd * g.s;
+    odd += 2;
+    em = cmul(em, e1);
+  }
+}
+
+// P2M (3d/kernel.h:187-202): M[n][m] += q * Y_n^m(rho, alpha, -beta).  One
+// warp per leaf, one lane per body; each coefficient is summed over the
+// warp's bodies with a butterfly and added by lane 0.
 __global__ void __launch_bounds__(WARPS * 32) k_p2m(const int *leaves, int nleaves, const int *begin,
                                                     const int *count, const double4 *xr, const double4 *src,
                                                     double2 *M, int P) {
@@ -37,16 +68,23 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m(const int *leaves, int nleav
   __syncwarp();
   const int c = leaves[w];
   const double4 C = xr[c];
-  for (int b = begin[c]; b < begin[c] + count[c]; b++) {
-    const double4 B = src[b];
+  const int b0 = begin[c], nb = count[c];
+  for (int t = 0; t < nb; t += 32) {
+    const bool ok = t + lane < nb;
+    const double4 B = ok ? src[b0 + t + lane] : make_double4(C.x, C.y, C.z, 0.0);
     const Sph g = sph_of(B.x - C.x, B.y - C.y, B.z - C.z);
-    if (lane < P) {
-      regular_column(lane, P, g.r, g, cconj(g.e), [&](int n, double2 Y, double2) {
-        double2 &a = acc[tri(n) + lane];
-        a.x += B.w * Y.x;
-        a.y += B.w * Y.y;
-      });
-    }
+    regular_all<false>(P, g, cconj(g.e), [&](int n, int m, double2 Y, double2) {
+      double x = B.w * Y.x, y = B.w * Y.y;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+      }
+      if (lane == 0) {
+        acc[tri(n) + m].x += x;
+        acc[tri(n) + m].y += y;
+      }
+    });
   }
   __syncwarp();
   for (int k = lane; k < nt; k += 32) M[(long)c * nt + k] = acc[k];
@@ -160,31 +198,26 @@ __global__ void __launch_bounds__(WARPS * 32) k_l2p(const int *leaves, int nleav
   for (int k = lane; k < nt; k += 32) Lc[k] = L[(long)c * nt + k];
   __syncwarp();
   const double4 C = xr[c];
-  for (int b = begin[c]; b < begin[c] + count[c]; b++) {
-    const double4 B = src[b];
+  const int b0 = begin[c], nb = count[c];
+  for (int t = 0; t < nb; t += 32) {
+    const int b = b0 + t + lane;
+    const bool ok = t + lane < nb;
+    const double4 B = ok ? src[b] : make_double4(C.x + 1, C.y, C.z, 0.0);
     const Sph g = sph_of(B.x - C.x, B.y - C.y, B.z - C.z);
     double pot = 0, s0 = 0, s1 = 0, s2 = 0;
-    if (lane < P) {
-      const int m = lane;
+    regular_all<true>(P, g, g.e, [&](int n, int m, double2 Y, double2 dY) {
+      const double2 l = Lc[tri(n) + m];  // same coefficient on every lane: broadcast
       const double w2 = m == 0 ? 1.0 : 2.0;
-      regular_column(m, P, g.r, g, g.e, [&](int n, double2 Y, double2 dY) {
-        const double2 l = Lc[tri(n) + m];
-        const double re = l.x * Y.x - l.y * Y.y;        // Re(L Y)
-        const double red = l.x * dY.x - l.y * dY.y;     // Re(L dY)
-        const double rei = -(l.x * Y.y + l.y * Y.x);    // Re(L Y i)
-        pot += w2 * re;
-        if (g.r != 0) s0 += w2 * re / g.r * n;
-        s1 += w2 * red;
-        s2 += w2 * rei * m;
-      });
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      pot += __shfl_xor_sync(0xffffffffu, pot, o);
-      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    }
-    if (lane == 0) {
+      const double re = l.x * Y.x - l.y * Y.y;        // Re(L Y)
+      const double red = l.x * dY.x - l.y * dY.y;     // Re(L dY)
+      const double rei = -(l.x * Y.y + l.y * Y.x);    // Re(L Y i)
+      pot += w2 * re;
+      s0 += w2 * re * n;
+      s1 += w2 * red;
+      s2 += w2 * rei * m;
+    });
+    s0 = g.r != 0 ? s0 / g.r : 0.0;
+    if (ok) {
       // sph2cart (3d/kernel.h:31-40); the 1/sin(theta) term is dropped on the
       // polar axis, where every m>0 term (s2) vanishes.
       const double st = g.s, ct = g.c, cp = g.e.x, sp = g.e.y, r = g.r;
@@ -210,6 +243,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_l2p(const int *leaves, int nleav
 }  // namespace
 
 void expansions_set_attributes() {
+  double rc[2 * EXAFMM_MAX_P + 4];
+  rc[0] = 0;
+  for (int k = 1; k < 2 * EXAFMM_MAX_P + 4; k++) rc[k] = 1.0 / k;
+  FMM_CUDA(cudaMemcpyToSymbol(c_recip, rc, sizeof(rc)));
   cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
