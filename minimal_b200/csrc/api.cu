@@ -9,6 +9,7 @@
 namespace fmm {
 double fma_peak_tflops(int precision);
 void m2l_set_attributes();
+void m2l_grouped_set_attributes();
 void expansions_set_attributes();
 }  // namespace fmm
 
@@ -188,6 +189,7 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
       for (int k = 0; k < 2; k++)
         if (cudaEventCreate(&h.ev[p][k]) != cudaSuccess) h.ev_ok = false;
     m2l_set_attributes();
+    m2l_grouped_set_attributes();
     expansions_set_attributes();
     FMM_CUDA(cudaGetLastError());
   } catch (const Error &e) {
@@ -209,7 +211,8 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
                  &h.c_nchild, &h.c_parent, &h.c_level, &h.c_xr, &h.c_pre, &h.c_ref, &h.c_leaf_of_body,
                  &h.leaves, &h.pre_tmp, &h.ctmp, &h.geom, &h.counters, &h.frontier[0], &h.frontier[1],
                  &h.m2l_raw, &h.p2p_raw, &h.m2l_off, &h.m2l_ent, &h.p2p_off, &h.p2p_ent, &h.fill, &h.M, &h.L,
-                 &h.m2l_units, &h.stage};
+                 &h.m2l_units, &h.stage, &h.g_mt, &h.g_ekey, &h.g_occ, &h.g_cnt, &h.g_keyof, &h.g_ops,
+                 &h.g_tk, &h.g_tile, &h.g_seg, &h.g_tg};
   for (Buf *b : bufs) b->release();
   if (h.ev_ok)
     for (int p = 0; p < PH_COUNT + 1; p++)

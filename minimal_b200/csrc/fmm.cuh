@@ -76,6 +76,8 @@ struct DevCounters {
   unsigned long long frontier[2];   // BFS pair frontier sizes (ping-pong)
   int list_overflow;   // an emission or the frontier exceeded its capacity
   int max_m2l_seg, max_p2p_seg;
+  int gcounts[4];      // grouped M2L: residual entries, flagged targets, groups, segments
+  unsigned long long gfill;
 };
 
 // Per-phase timing slots (CUDA events on the handle stream).
@@ -125,6 +127,11 @@ struct Handle {
   Buf M, L;   // double2 [ncells][nterm]
   Buf m2l_units;  // balanced contraction table for the M2L kernel (per P)
   int m2l_units_P = -1;
+
+  // grouped M2L (m2l_group.cu)
+  Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg;
+  int g_ntiles = 0, g_ngroups = 0, g_nseg = 0;
+  bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only
 
   // phase state
   bool have_tree = false, have_lists = false, have_up = false, have_horiz = false, have_down = false;

@@ -22,8 +22,11 @@ constexpr int WARPS = 4;
 constexpr int IMG_SHIFT = 26;
 constexpr u32 IDX_MASK = (1u << IMG_SHIFT) - 1;
 
+// ekey == nullptr: every entry, L stored.  Otherwise only the entries the
+// grouped path left out (ekey < 0), added to L.
 __global__ void __launch_bounds__(WARPS * 32) k_m2l(int ncells, const int *off, const u32 *ent, const double4 *xr,
-                                                    const double2 *M, double2 *L, int P, double cycle) {
+                                                    const double2 *M, double2 *L, int P, double cycle,
+                                                    const int *ekey) {
   extern __shared__ double2 sh[];
   const int nt = tri(P);
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -33,6 +36,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_m2l(int ncells, const int *off, 
   for (int k = lane; k < nt; k += 32) acc[k] = make_double2(0, 0);
   const double4 X = xr[c];
   for (int e = off[c]; e < off[c + 1]; e++) {
+    if (ekey && ekey[e] >= 0) continue;
     const u32 en = ent[e];
     const int src = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
     const double4 Y = xr[src];
@@ -66,19 +70,36 @@ __global__ void __launch_bounds__(WARPS * 32) k_m2l(int ncells, const int *off, 
     }
   }
   __syncwarp();
-  for (int k = lane; k < nt; k += 32) L[(long)c * nt + k] = acc[k];
+  for (int k = lane; k < nt; k += 32) {
+    if (ekey) {
+      L[(long)c * nt + k].x += acc[k].x;
+      L[(long)c * nt + k].y += acc[k].y;
+    } else {
+      L[(long)c * nt + k] = acc[k];
+    }
+  }
 }
 
 }  // namespace
 
-void m2l_pass(Handle &h) {
+bool m2l_grouped_available(int P);
+void m2l_grouped_pass(Handle &h);
+
+static void launch_direct_form(Handle &h, const int *ekey) {
   const int P = h.prm.P, nt = tri(P);
-  h.L.need((size_t)h.ncells * nt * sizeof(double2));
   k_m2l<<<grid_for(h.ncells, WARPS), WARPS * 32, WARPS * 3 * nt * sizeof(double2), h.stream>>>(
       h.ncells, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(), h.c_xr.as<double4>(), h.M.as<double2>(),
-      h.L.as<double2>(), P, h.prm.images ? h.prm.cycle : 0.0);
+      h.L.as<double2>(), P, h.prm.images ? h.prm.cycle : 0.0, ekey);
   h.launches++;
   FMM_LAUNCH();
+}
+
+void m2l_residual(Handle &h, const int *ekey) { launch_direct_form(h, ekey); }
+
+void m2l_pass(Handle &h) {
+  h.L.need((size_t)h.ncells * tri(h.prm.P) * sizeof(double2));
+  if (!h.force_direct_m2l && m2l_grouped_available(h.prm.P)) m2l_grouped_pass(h);
+  else launch_direct_form(h, nullptr);
 }
 
 void m2l_set_attributes() {

@@ -1,0 +1,478 @@
+// Grouped M2L: the translation as dense contractions of precomputed operators
+// (3d/kernel.h:233-260 is the per-pair operator being grouped).
+//
+// Scaling makes one operator serve every level.  With M~_n = M_n / R_s^n,
+// L~_j = L_j * R_t^(j+1), r_f the radius of the finer of target and source,
+// and v = (X_t - X_s) / r_f (an exact integer vector: level-l centres sit at
+// X0 + odd * R0/2^l), the truncated M2L becomes
+//   L~_j^k = sum_{n,m} s(j,k,m) rho^n 2^(d'(j+1)) Z_{j+n}^{m-k}(v) A~_n^m,
+// rho = 2^max(0, lt-ls), d' = max(0, ls-lt): the operator depends only on the
+// group key (lt - ls, v).  Realified (2x2 real blocks per complex input
+// with conj(M) folded in), it is a 2NT x 2NT real matrix, zero for j+n >= P.
+//
+// Pipeline per evaluation:
+//   k_gkeys    key of every M2L entry (periodic images, far-out offsets or
+//              level gaps beyond the key range stay "residual" and are done
+//              by the direct-form kernel), occupancy of the key space;
+//   scan       group ids of the occupied keys;
+//   k_gops     the realified operator of every group (FP64);
+//   tiles      targets with grouped entries sorted by (level, child rank) and
+//              cut into tiles of 32; every grouped entry gets the sort key
+//              (tile, group) and one radix sort yields the (tile, group)
+//              segments, each with the source cell of every tile slot;
+//   k_gemm64   one CTA (8 warps) per tile: for each group of the tile, stage
+//              the operator and the 32 gathered scaled multipoles in shared
+//              memory and accumulate with FP64 DMMA (mma.m8n8k4) in registers;
+//              then reduce the warps' pieces, unscale and store L.
+#include <map>
+#include <mutex>
+
+#include "fmm.cuh"
+#include "harmonics.cuh"
+#include "m2l_group.h"
+
+namespace fmm {
+
+void m2l_residual(Handle &h, const int *ekey);  // m2l.cu
+
+namespace {
+
+constexpr int TB = 256;
+constexpr int IMG_SHIFT = 26;
+constexpr u32 IDX_MASK = (1u << IMG_SHIFT) - 1;
+constexpr int KEY_DL = 4;   // level difference lt - ls in [-4, 3]
+constexpr int KEY_V = 32;   // offset components in [-32, 31]
+constexpr int KEY_SPACE = 8 << 18;
+constexpr int XS = 36;      // padded row stride of the staged multipoles (doubles)
+
+__global__ void k_gkeys(int ncells, const int *off, const u32 *ent, const double4 *xr, const int *level, int *ekey,
+                        int *occ, int *gcount, int *counts /*[0] residual entries, [1] flagged targets*/) {
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (c >= ncells) return;
+  const double4 X = xr[c];
+  const int lt = level[c];
+  int grouped = 0, resid = 0;
+  for (int e = off[c] + lane; e < off[c + 1]; e += 32) {
+    const u32 en = ent[e];
+    const int s = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
+    int key = -1;
+    if (img == 13) {
+      const double4 Y = xr[s];
+      const int dl = lt - level[s];
+      const double rf = fmin(X.w, Y.w);
+      const double vx = rint((X.x - Y.x) / rf), vy = rint((X.y - Y.y) / rf), vz = rint((X.z - Y.z) / rf);
+      if (dl >= -KEY_DL && dl < KEY_DL && vx >= -KEY_V && vx < KEY_V && vy >= -KEY_V && vy < KEY_V &&
+          vz >= -KEY_V && vz < KEY_V) {
+        key = ((dl + KEY_DL) << 18) | (((int)vx + KEY_V) << 12) | (((int)vy + KEY_V) << 6) | ((int)vz + KEY_V);
+        occ[key] = 1;
+      }
+    }
+    ekey[e] = key;
+    grouped += key >= 0;
+    resid += key < 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    grouped += __shfl_xor_sync(0xffffffffu, grouped, o);
+    resid += __shfl_xor_sync(0xffffffffu, resid, o);
+  }
+  if (lane == 0) {
+    gcount[c] = grouped;
+    if (resid) atomicAdd(&counts[0], resid);
+    if (grouped) atomicAdd(&counts[1], 1);
+  }
+}
+
+__global__ void k_key_of_gid(const int *occ, const int *gidx, int *key_of) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < KEY_SPACE && occ[k]) key_of[gidx[k]] = k;
+}
+
+struct PlanDev {
+  int P, NT, KP, nrb, wsize, maxrank;
+  const int *woff, *jmin, *pieces, *prank;
+};
+
+// One CTA per group: the realified, scaled operator in row-block layout.
+__global__ void k_gops(const int *key_of, PlanDev pd, double *ops) {
+  extern __shared__ double2 Zsh[];  // NT irregular harmonics of v
+  const int g = blockIdx.x;
+  const int key = key_of[g];
+  const int dl = (key >> 18) - KEY_DL;
+  const int vx = ((key >> 12) & 63) - KEY_V, vy = ((key >> 6) & 63) - KEY_V, vz = (key & 63) - KEY_V;
+  const int P = pd.P;
+  if (threadIdx.x < P) {
+    const Sph sg = sph_of((double)vx, (double)vy, (double)vz);
+    const int m = threadIdx.x;
+    irregular_column(m, P, sg.r, sg, [&](int n, double2 z) { Zsh[tri(n) + m] = z; });
+  }
+  __syncthreads();
+  const double rho = dl > 0 ? (double)(1 << dl) : 1.0;  // source coarser: R_s / r_f
+  const int dp = dl < 0 ? -dl : 0;                        // source finer: R_t / r_f = 2^dp
+  double *W = ops + (size_t)g * pd.wsize;
+  for (int i = threadIdx.x; i < pd.wsize; i += blockDim.x) {
+    // locate row block
+    int rb = 0;
+    while (pd.woff[rb + 1] <= i) rb++;
+    const int li = i - pd.woff[rb];
+    const int k = li >> 3, r = li & 7;
+    const int row = rb * 8 + r;
+    double w = 0;
+    if (row < 2 * pd.NT) {
+      const int o = row >> 1, cr = row & 1;
+      int j = 0;
+      while (tri(j + 1) <= o) j++;
+      const int kk = o - tri(j);
+      const int ci = k >> 1, cc = k & 1;
+      if (ci < pd.NT) {
+        int n = 0;
+        while (tri(n + 1) <= ci) n++;
+        const int mu = ci - tri(n);
+        if (j + n <= P - 1) {
+          const int d = j + n;
+          const double f = pow(rho, (double)n) * pow(2.0, (double)(dp * (j + 1))) * ((j & 1) ? -1.0 : 1.0);
+          // T(m) = sigma(kk, m) * f * Z_d^{m - kk}
+          auto T = [&](int m) {
+            const int e = m < 0 ? 0 : (m <= kk ? m : kk);
+            const int om = m - kk;
+            double2 z = Zsh[tri(d) + (om < 0 ? -om : om)];
+            if (om < 0) z.y = -z.y;
+            const double s = ((e & 1) ? -1.0 : 1.0) * f;
+            return make_double2(s * z.x, s * z.y);
+          };
+          const double2 tp = T(mu);
+          const double2 tm = mu > 0 ? T(-mu) : make_double2(0, 0);
+          if (cr == 0 && cc == 0) w = tp.x + tm.x;
+          else if (cr == 0 && cc == 1) w = -(tp.y - tm.y);
+          else if (cr == 1 && cc == 0) w = tp.y + tm.y;
+          else w = tp.x - tm.x;
+        }
+      }
+    }
+    W[i] = w;
+  }
+}
+
+// Scaled, realified multipoles: Mt[c][2*(tri(n)+m)+{0,1}] = M[c][n,m] / R_c^n.
+__global__ void k_mscale(int ncells, int P, int KP, const double4 *xr, const double2 *M, double *Mt) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int NT = tri(P);
+  if (i >= (long)ncells * KP) return;
+  const int c = (int)(i / KP), k = (int)(i - (long)c * KP);
+  double v = 0;
+  if (k < 2 * NT) {
+    const int ci = k >> 1;
+    int n = 0;
+    while (tri(n + 1) <= ci) n++;
+    const double inv = 1.0 / xr[c].w;
+    double s = 1;
+    for (int q = 0; q < n; q++) s *= inv;
+    const double2 m = M[(long)c * NT + ci];
+    v = (k & 1 ? m.y : m.x) * s;
+  }
+  Mt[i] = v;
+}
+
+__global__ void k_tkeys(int ncells, const int *gcount, const int *level, const int *parent, const int *child,
+                        u64 *keys, u32 *vals) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const int pa = parent[c];
+  const int cls = pa < 0 ? 0 : c - child[pa];
+  keys[c] = gcount[c] > 0 ? (u64)(level[c] * 8 + cls) : 255ull;
+  vals[c] = (u32)c;
+}
+
+__global__ void k_tiles(int ntiles, int nflag, const u32 *sorted, int *tile_tgt, int *tslot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntiles * GP_TILE) return;
+  if (i < nflag) {
+    const int c = (int)sorted[i];
+    tile_tgt[i] = c;
+    tslot[c] = i;
+  } else {
+    tile_tgt[i] = -1;
+  }
+}
+
+__global__ void k_gentries(int ncells, const int *off, const u32 *ent, const int *ekey, const int *gidx,
+                           const int *gcount, const int *tslot, int gbits, unsigned long long *fill, u64 *keys,
+                           u32 *vals) {
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (c >= ncells || gcount[c] == 0) return;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(fill, (unsigned long long)gcount[c]);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const int ts = tslot[c];
+  const u64 tile = (u64)(ts / GP_TILE);
+  const u32 slot = (u32)(ts % GP_TILE);
+  int pos = 0;
+  for (int e0 = off[c]; e0 < off[c + 1]; e0 += 32) {
+    const int e = e0 + lane;
+    const bool ok = e < off[c + 1] && ekey[e] >= 0;
+    const unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (ok) {
+      const int r = pos + __popc(b & ((1u << lane) - 1));
+      keys[base + r] = (tile << gbits) | (u64)gidx[ekey[e]];
+      vals[base + r] = (slot << IMG_SHIFT) | (ent[e] & IDX_MASK);
+    }
+    pos += __popc(b);
+  }
+}
+
+__global__ void k_segflags(const u64 *keys, long n, int gbits, int *flag) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = i == 0 || keys[i] != keys[i - 1];
+}
+
+__global__ void k_segments(const u64 *keys, const u32 *vals, long n, int gbits, const int *segid, int *tg_gid,
+                           int *tg_src, int *tg_off) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const u64 k = keys[i];
+  const bool first = i == 0 || k != keys[i - 1];
+  // segid is the exclusive scan of the segment-start flags: it already counts
+  // the start of this entry's own segment unless the entry is that start
+  const int s = segid[i] - (first ? 0 : 1);
+  if (first) tg_gid[s] = (int)(k & ((1ull << gbits) - 1));
+  const u32 v = vals[i];
+  tg_src[(long)s * GP_TILE + (v >> IMG_SHIFT)] = (int)(v & IDX_MASK);
+  const u64 tile = k >> gbits;
+  if (i == 0 || (keys[i - 1] >> gbits) != tile) tg_off[tile] = s;
+}
+
+__global__ void k_set_int(int *p, const int *v) { *p = *v; }
+
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, const int *tg_off, const int *tg_gid,
+                                                          const int *tg_src, const double *ops, const double *Mt,
+                                                          const double4 *xr, double2 *L, PlanDev pd) {
+  extern __shared__ double smd[];
+  double *Wsm = smd;
+  double *Xsm = smd + pd.wsize;
+  const int tile = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int pc[GP_MAXP], wo[GP_MAXP];
+#pragma unroll
+  for (int p = 0; p < GP_MAXP; p++) {
+    pc[p] = pd.pieces[warp * GP_MAXP + p];
+    wo[p] = pc[p] >= 0 ? pd.woff[pc[p] & 255] : 0;
+  }
+  double acc[GP_MAXP][4][2];
+#pragma unroll
+  for (int p = 0; p < GP_MAXP; p++)
+#pragma unroll
+    for (int cb = 0; cb < 4; cb++) acc[p][cb][0] = acc[p][cb][1] = 0;
+  const int KP = pd.KP;
+  const int ar = lane >> 2, ak = lane & 3;
+  for (int g = tg_off[tile]; g < tg_off[tile + 1]; g++) {
+    const double *Wg = ops + (size_t)tg_gid[g] * pd.wsize;
+    __syncthreads();
+    for (int i = tid; i < pd.wsize / 2; i += blockDim.x) ((double2 *)Wsm)[i] = ((const double2 *)Wg)[i];
+    for (int i = tid; i < GP_TILE * KP; i += blockDim.x) {
+      const int col = i / KP, k = i - col * KP;
+      const int s = tg_src[(long)g * GP_TILE + col];
+      Xsm[k * XS + col] = s >= 0 ? Mt[(long)s * KP + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < GP_MAXP; p++) {
+      if (pc[p] < 0) continue;
+      const int k0 = (pc[p] >> 8) & 4095, k1 = pc[p] >> 20;
+      const double *Wb = Wsm + wo[p];
+      for (int k = k0; k < k1; k += 4) {
+        const double a = Wb[(k + ak) * 8 + ar];
+        const double *xb = Xsm + (k + ak) * XS + ar;
+#pragma unroll
+        for (int cb = 0; cb < 4; cb++) dmma(acc[p][cb][0], acc[p][cb][1], a, xb[cb * 8]);
+      }
+    }
+  }
+  // reduce the pieces into Y[row][col] (rank 0 stores, higher ranks add)
+  double *Y = smd;
+  __syncthreads();
+  for (int rank = 0; rank <= pd.maxrank; rank++) {
+#pragma unroll
+    for (int p = 0; p < GP_MAXP; p++) {
+      if (pc[p] < 0 || pd.prank[warp * GP_MAXP + p] != rank) continue;
+      const int rb = pc[p] & 255;
+#pragma unroll
+      for (int cb = 0; cb < 4; cb++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          double &y = Y[(rb * 8 + ar) * GP_TILE + cb * 8 + ak * 2 + h];
+          y = rank == 0 ? acc[p][cb][h] : y + acc[p][cb][h];
+        }
+    }
+    __syncthreads();
+  }
+  // unscale (L = L~ / R_t^(j+1)) and store
+  for (int i = tid; i < GP_TILE * pd.NT; i += blockDim.x) {
+    const int col = i / pd.NT, o = i - col * pd.NT;
+    const int t = tile_tgt[tile * GP_TILE + col];
+    if (t < 0) continue;
+    int j = 0;
+    while (tri(j + 1) <= o) j++;
+    const double inv = 1.0 / xr[t].w;
+    double s = inv;
+    for (int q = 0; q < j; q++) s *= inv;
+    L[(long)t * pd.NT + o] = make_double2(Y[(2 * o) * GP_TILE + col] * s, Y[(2 * o + 1) * GP_TILE + col] * s);
+  }
+}
+
+struct PlanCache {
+  GroupPlan host;
+  int *dev = nullptr;
+};
+
+PlanCache &plan_cache(int P) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, PlanCache> cache;
+  int dev = 0;
+  FMM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_pair(dev, P);
+  auto it = cache.find(key);
+  if (it == cache.end()) {
+    PlanCache pc;
+    pc.host = make_group_plan(P);
+    if (pc.host.P == P) {
+      const GroupPlan &g = pc.host;
+      std::vector<int> buf;
+      buf.insert(buf.end(), g.woff.begin(), g.woff.end());
+      buf.insert(buf.end(), g.jmin.begin(), g.jmin.end());
+      buf.insert(buf.end(), g.pieces.begin(), g.pieces.end());
+      buf.insert(buf.end(), g.prank.begin(), g.prank.end());
+      FMM_CUDA(cudaMalloc(&pc.dev, buf.size() * sizeof(int)));
+      FMM_CUDA(cudaMemcpy(pc.dev, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    it = cache.emplace(key, pc).first;
+  }
+  return it->second;
+}
+
+PlanDev plan_dev(const PlanCache &pc) {
+  const GroupPlan &g = pc.host;
+  PlanDev d;
+  d.P = g.P; d.NT = g.NT; d.KP = g.KP; d.nrb = g.nrb; d.wsize = g.wsize; d.maxrank = g.maxrank;
+  d.woff = pc.dev;
+  d.jmin = d.woff + g.nrb + 1;
+  d.pieces = d.jmin + g.nrb;
+  d.prank = d.pieces + GP_WARPS * GP_MAXP;
+  return d;
+}
+
+size_t gemm64_smem(const GroupPlan &g) {
+  const size_t stage = (size_t)g.wsize + (size_t)g.KP * XS;
+  const size_t red = (size_t)g.nrb * 8 * GP_TILE;
+  return std::max(stage, red) * sizeof(double);
+}
+
+int bits_for(long v) {
+  int b = 1;
+  while ((1l << b) < v) b++;
+  return b;
+}
+
+}  // namespace
+
+bool m2l_grouped_available(int P) {
+  PlanCache &pc = plan_cache(P);
+  return pc.host.P == P && gemm64_smem(pc.host) <= 200 * 1024;
+}
+
+void m2l_grouped_set_attributes() {
+  cudaFuncSetAttribute(k_gemm64, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+// Grouped M2L of the whole tree: L stored for every cell (zero where no
+// M2L entry), residual entries added by the direct-form kernel.
+void m2l_grouped_pass(Handle &h) {
+  cudaStream_t s = h.stream;
+  const int P = h.prm.P, NT = tri(P), C = h.ncells;
+  PlanCache &pc = plan_cache(P);
+  const GroupPlan &gp = pc.host;
+  const PlanDev pd = plan_dev(pc);
+  const long nent = h.n_m2l;
+  h.L.need((size_t)C * NT * sizeof(double2));
+  FMM_CUDA(cudaMemsetAsync(h.L.p, 0, (size_t)C * NT * sizeof(double2), s));
+  if (nent == 0) return;
+
+  // scaled multipoles
+  h.g_mt.need((size_t)C * gp.KP * sizeof(double));
+  k_mscale<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>(C, P, gp.KP, h.c_xr.as<double4>(), h.M.as<double2>(),
+                                                        h.g_mt.as<double>());
+  // keys, occupancy, counts
+  h.g_ekey.need(nent * sizeof(int));
+  h.g_occ.need((size_t)KEY_SPACE * sizeof(int) * 2 + 64);
+  int *occ = h.g_occ.as<int>(), *gidx = occ + KEY_SPACE;
+  h.g_cnt.need(C * sizeof(int) * 2 + 64);
+  int *gcount = h.g_cnt.as<int>(), *tslot = gcount + C;
+  DevCounters *ctr = h.counters.as<DevCounters>();
+  int *counts = ctr->gcounts;
+  FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
+  FMM_CUDA(cudaMemsetAsync(counts, 0, 4 * sizeof(int), s));
+  k_gkeys<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(), h.c_xr.as<double4>(),
+                                                    h.c_level.as<int>(), h.g_ekey.as<int>(), occ, gcount, counts);
+  scan_exclusive_int(h, occ, gidx, KEY_SPACE, &counts[2]);
+  FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+  FMM_CUDA(cudaStreamSynchronize(s));
+  const int nres = h.hc.gcounts[0], nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
+  h.launches += 3;
+  if (ngroups > 0) {
+    // operators
+    h.g_keyof.need(ngroups * sizeof(int));
+    k_key_of_gid<<<grid_for(KEY_SPACE, TB), TB, 0, s>>>(occ, gidx, h.g_keyof.as<int>());
+    h.g_ops.need((size_t)ngroups * gp.wsize * sizeof(double));
+    k_gops<<<ngroups, 128, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), pd, h.g_ops.as<double>());
+    // tiles of targets
+    const int ntiles = (nflag + GP_TILE - 1) / GP_TILE;
+    h.g_tk.need((size_t)C * 2 * (sizeof(u64) + sizeof(u32)) + 64);
+    u64 *tk = h.g_tk.as<u64>(), *tk2 = tk + C;
+    u32 *tv = (u32 *)(tk2 + C), *tv2 = tv + C;
+    k_tkeys<<<grid_for(C, TB), TB, 0, s>>>(C, gcount, h.c_level.as<int>(), h.c_parent.as<int>(), h.c_child.as<int>(),
+                                           tk, tv);
+    radix_sort_pairs(h, tk, tv, tk2, tv2, C, 0, 8);
+    h.g_tile.need((size_t)ntiles * GP_TILE * sizeof(int) + 64);
+    k_tiles<<<grid_for((long)ntiles * GP_TILE, TB), TB, 0, s>>>(ntiles, nflag, tv, h.g_tile.as<int>(), tslot);
+    // (tile, group) segments
+    const long ngent = nent - nres;
+    const int gbits = bits_for(ngroups), tbits = bits_for(ntiles + 1);
+    h.keys[0].need(ngent * 8); h.keys[1].need(ngent * 8);
+    h.vals[0].need(ngent * 4); h.vals[1].need(ngent * 4);
+    u64 *ek = h.keys[0].as<u64>(), *ek2 = h.keys[1].as<u64>();
+    u32 *ev = h.vals[0].as<u32>(), *ev2 = h.vals[1].as<u32>();
+    FMM_CUDA(cudaMemsetAsync(&ctr->gfill, 0, sizeof(unsigned long long), s));
+    k_gentries<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
+                                                        h.g_ekey.as<int>(), gidx, gcount, tslot, gbits, &ctr->gfill,
+                                                        ek, ev);
+    radix_sort_pairs(h, ek, ev, ek2, ev2, ngent, 0, gbits + tbits);
+    h.g_seg.need((ngent + 1) * sizeof(int) * 2);
+    int *flag = h.g_seg.as<int>(), *segid = flag + ngent + 1;
+    k_segflags<<<grid_for(ngent, TB), TB, 0, s>>>(ek, ngent, gbits, flag);
+    scan_exclusive_int(h, flag, segid, ngent, &counts[3]);
+    FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    const int nseg = h.hc.gcounts[3];
+    h.g_tg.need(((size_t)nseg * (GP_TILE + 1) + ntiles + 2) * sizeof(int));
+    int *tg_gid = h.g_tg.as<int>(), *tg_off = tg_gid + nseg, *tg_src = tg_off + ntiles + 1;
+    FMM_CUDA(cudaMemsetAsync(tg_src, 0xff, (size_t)nseg * GP_TILE * sizeof(int), s));
+    k_segments<<<grid_for(ngent, TB), TB, 0, s>>>(ek, ev, ngent, gbits, segid, tg_gid, tg_src, tg_off);
+    k_set_int<<<1, 1, 0, s>>>(tg_off + ntiles, &counts[3]);
+    // contraction
+    k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                            h.g_ops.as<double>(), h.g_mt.as<double>(),
+                                                            h.c_xr.as<double4>(), h.L.as<double2>(), pd);
+    h.launches += 10;
+    h.g_ntiles = ntiles;
+    h.g_ngroups = ngroups;
+    h.g_nseg = nseg;
+    FMM_LAUNCH();
+  }
+  if (nres > 0) m2l_residual(h, h.g_ekey.as<int>());
+}
+
+}  // namespace fmm
