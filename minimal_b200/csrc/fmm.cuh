@@ -78,6 +78,7 @@ struct DevCounters {
   int max_m2l_seg, max_p2p_seg;
   int gcounts[4];      // grouped M2L: residual entries, flagged targets, groups, segments
   unsigned long long gfill;
+  int tc_error;        // a bounded tensor-core wait ran out
 };
 
 // Per-phase timing slots (CUDA events on the handle stream).
@@ -129,8 +130,9 @@ struct Handle {
   int m2l_units_P = -1;
 
   // grouped M2L (m2l_group.cu)
-  Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg;
+  Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg, g_m16;
   int g_ntiles = 0, g_ngroups = 0, g_nseg = 0;
+  bool g_used_tc = false;
   bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only
 
   // phase state

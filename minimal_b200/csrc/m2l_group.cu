@@ -30,6 +30,7 @@
 #include "fmm.cuh"
 #include "harmonics.cuh"
 #include "m2l_group.h"
+#include "tc.cuh"
 
 namespace fmm {
 
@@ -44,6 +45,9 @@ constexpr int KEY_DL = 4;   // level difference lt - ls in [-4, 3]
 constexpr int KEY_V = 32;   // offset components in [-32, 31]
 constexpr int KEY_SPACE = 8 << 18;
 constexpr int XS = 36;      // padded row stride of the staged multipoles (doubles)
+constexpr int SLOT_SHIFT = 25;  // sorted entry value = tile slot << 25 | source cell
+constexpr u32 SLOT_MASK = (1u << SLOT_SHIFT) - 1;
+constexpr int TC_TILE = 128;    // targets per tile on the tensor core (MMA M)
 
 __global__ void k_gkeys(int ncells, const int *off, const u32 *ent, const double4 *xr, const int *level, int *ekey,
                         int *occ, int *gcount, int *counts /*[0] residual entries, [1] flagged targets*/) {
@@ -92,64 +96,96 @@ struct PlanDev {
   const int *woff, *jmin, *pieces, *prank;
 };
 
-// One CTA per group: the realified, scaled operator in row-block layout.
-__global__ void k_gops(const int *key_of, PlanDev pd, double *ops) {
-  extern __shared__ double2 Zsh[];  // NT irregular harmonics of v
-  const int g = blockIdx.x;
-  const int key = key_of[g];
+// Irregular harmonics of the group's integer offset into shared memory
+// (threads m < P build column m); returns the level difference.
+__device__ int group_harmonics(int key, int P, double2 *Zsh) {
   const int dl = (key >> 18) - KEY_DL;
   const int vx = ((key >> 12) & 63) - KEY_V, vy = ((key >> 6) & 63) - KEY_V, vz = (key & 63) - KEY_V;
-  const int P = pd.P;
   if (threadIdx.x < P) {
     const Sph sg = sph_of((double)vx, (double)vy, (double)vz);
     const int m = threadIdx.x;
     irregular_column(m, P, sg.r, sg, [&](int n, double2 z) { Zsh[tri(n) + m] = z; });
   }
   __syncthreads();
+  return dl;
+}
+
+// Entry (row, col) of the realified, scaled operator (zero outside 2NT x 2NT
+// and outside the truncation j + n < P).
+__device__ double op_value(int row, int col, int P, int NT, int dl, const double2 *Zsh) {
+  if (row >= 2 * NT || col >= 2 * NT) return 0.0;
+  const int o = row >> 1, cr = row & 1;
+  int j = 0;
+  while (tri(j + 1) <= o) j++;
+  const int kk = o - tri(j);
+  const int ci = col >> 1, cc = col & 1;
+  int n = 0;
+  while (tri(n + 1) <= ci) n++;
+  const int mu = ci - tri(n);
+  if (j + n > P - 1) return 0.0;
+  const int d = j + n;
   const double rho = dl > 0 ? (double)(1 << dl) : 1.0;  // source coarser: R_s / r_f
   const int dp = dl < 0 ? -dl : 0;                        // source finer: R_t / r_f = 2^dp
+  const double f = pow(rho, (double)n) * pow(2.0, (double)(dp * (j + 1))) * ((j & 1) ? -1.0 : 1.0);
+  // T(m) = sigma(kk, m) * f * Z_d^{m - kk}
+  auto T = [&](int m) {
+    const int e = m < 0 ? 0 : (m <= kk ? m : kk);
+    const int om = m - kk;
+    double2 z = Zsh[tri(d) + (om < 0 ? -om : om)];
+    if (om < 0) z.y = -z.y;
+    const double s = ((e & 1) ? -1.0 : 1.0) * f;
+    return make_double2(s * z.x, s * z.y);
+  };
+  const double2 tp = T(mu);
+  const double2 tm = mu > 0 ? T(-mu) : make_double2(0, 0);
+  if (cr == 0 && cc == 0) return tp.x + tm.x;
+  if (cr == 0 && cc == 1) return -(tp.y - tm.y);
+  if (cr == 1 && cc == 0) return tp.y + tm.y;
+  return tp.x - tm.x;
+}
+
+// One CTA per group: the realified, scaled operator in row-block layout.
+__global__ void k_gops(const int *key_of, PlanDev pd, double *ops) {
+  extern __shared__ double2 Zsh[];  // NT irregular harmonics of v
+  const int g = blockIdx.x;
+  const int dl = group_harmonics(key_of[g], pd.P, Zsh);
   double *W = ops + (size_t)g * pd.wsize;
   for (int i = threadIdx.x; i < pd.wsize; i += blockDim.x) {
-    // locate row block
     int rb = 0;
     while (pd.woff[rb + 1] <= i) rb++;
     const int li = i - pd.woff[rb];
-    const int k = li >> 3, r = li & 7;
-    const int row = rb * 8 + r;
-    double w = 0;
-    if (row < 2 * pd.NT) {
-      const int o = row >> 1, cr = row & 1;
-      int j = 0;
-      while (tri(j + 1) <= o) j++;
-      const int kk = o - tri(j);
-      const int ci = k >> 1, cc = k & 1;
-      if (ci < pd.NT) {
-        int n = 0;
-        while (tri(n + 1) <= ci) n++;
-        const int mu = ci - tri(n);
-        if (j + n <= P - 1) {
-          const int d = j + n;
-          const double f = pow(rho, (double)n) * pow(2.0, (double)(dp * (j + 1))) * ((j & 1) ? -1.0 : 1.0);
-          // T(m) = sigma(kk, m) * f * Z_d^{m - kk}
-          auto T = [&](int m) {
-            const int e = m < 0 ? 0 : (m <= kk ? m : kk);
-            const int om = m - kk;
-            double2 z = Zsh[tri(d) + (om < 0 ? -om : om)];
-            if (om < 0) z.y = -z.y;
-            const double s = ((e & 1) ? -1.0 : 1.0) * f;
-            return make_double2(s * z.x, s * z.y);
-          };
-          const double2 tp = T(mu);
-          const double2 tm = mu > 0 ? T(-mu) : make_double2(0, 0);
-          if (cr == 0 && cc == 0) w = tp.x + tm.x;
-          else if (cr == 0 && cc == 1) w = -(tp.y - tm.y);
-          else if (cr == 1 && cc == 0) w = tp.y + tm.y;
-          else w = tp.x - tm.x;
-        }
-      }
-    }
-    W[i] = w;
+    W[i] = op_value(rb * 8 + (li & 7), li >> 3, pd.P, pd.NT, dl, Zsh);
   }
+}
+
+// One CTA per group: the operator split into FP16 hi + lo parts, as the
+// tensor core's B operand (N = KP output rows, K-major, no swizzle).
+__global__ void k_gops16(const int *key_of, int P, int KP, __half *ops16) {
+  extern __shared__ double2 Zsh[];
+  const int g = blockIdx.x, NT = tri(P);
+  const int dl = group_harmonics(key_of[g], P, Zsh);
+  __half *Wh = ops16 + (size_t)g * 2 * KP * KP, *Wl = Wh + KP * KP;
+  for (int i = threadIdx.x; i < KP * KP; i += blockDim.x) {
+    const int row = i / KP, col = i - row * KP;
+    const double w = op_value(row, col, P, NT, dl, Zsh);
+    const __half hi = __double2half(w);
+    const __half lo = __double2half(w - (double)__half2float(hi));
+    const int pos = tc::canon(row, col, KP);
+    Wh[pos] = hi;
+    Wl[pos] = lo;
+  }
+}
+
+// Scaled multipoles split into FP16 hi + lo rows (KP values per cell each).
+__global__ void k_msplit16(long total, int KP, const double *Mt, __half *M16) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const long c = i / KP;
+  const int k = (int)(i - c * KP);
+  const double v = Mt[i];
+  const __half hi = __double2half(v);
+  M16[c * 2 * KP + k] = hi;
+  M16[c * 2 * KP + KP + k] = __double2half(v - (double)__half2float(hi));
 }
 
 // Scaled, realified multipoles: Mt[c][2*(tri(n)+m)+{0,1}] = M[c][n,m] / R_c^n.
@@ -182,9 +218,9 @@ __global__ void k_tkeys(int ncells, const int *gcount, const int *level, const i
   vals[c] = (u32)c;
 }
 
-__global__ void k_tiles(int ntiles, int nflag, const u32 *sorted, int *tile_tgt, int *tslot) {
+__global__ void k_tiles(int ntiles, int tile_n, int nflag, const u32 *sorted, int *tile_tgt, int *tslot) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ntiles * GP_TILE) return;
+  if (i >= ntiles * tile_n) return;
   if (i < nflag) {
     const int c = (int)sorted[i];
     tile_tgt[i] = c;
@@ -195,16 +231,16 @@ __global__ void k_tiles(int ntiles, int nflag, const u32 *sorted, int *tile_tgt,
 }
 
 __global__ void k_gentries(int ncells, const int *off, const u32 *ent, const int *ekey, const int *gidx,
-                           const int *gcount, const int *tslot, int gbits, unsigned long long *fill, u64 *keys,
-                           u32 *vals) {
+                           const int *gcount, const int *tslot, int tile_n, int gbits, unsigned long long *fill,
+                           u64 *keys, u32 *vals) {
   const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (c >= ncells || gcount[c] == 0) return;
   unsigned long long base = 0;
   if (lane == 0) base = atomicAdd(fill, (unsigned long long)gcount[c]);
   base = __shfl_sync(0xffffffffu, base, 0);
   const int ts = tslot[c];
-  const u64 tile = (u64)(ts / GP_TILE);
-  const u32 slot = (u32)(ts % GP_TILE);
+  const u64 tile = (u64)(ts / tile_n);
+  const u32 slot = (u32)(ts % tile_n);
   int pos = 0;
   for (int e0 = off[c]; e0 < off[c + 1]; e0 += 32) {
     const int e = e0 + lane;
@@ -213,7 +249,7 @@ __global__ void k_gentries(int ncells, const int *off, const u32 *ent, const int
     if (ok) {
       const int r = pos + __popc(b & ((1u << lane) - 1));
       keys[base + r] = (tile << gbits) | (u64)gidx[ekey[e]];
-      vals[base + r] = (slot << IMG_SHIFT) | (ent[e] & IDX_MASK);
+      vals[base + r] = (slot << SLOT_SHIFT) | (ent[e] & IDX_MASK);
     }
     pos += __popc(b);
   }
@@ -224,8 +260,8 @@ __global__ void k_segflags(const u64 *keys, long n, int gbits, int *flag) {
   if (i < n) flag[i] = i == 0 || keys[i] != keys[i - 1];
 }
 
-__global__ void k_segments(const u64 *keys, const u32 *vals, long n, int gbits, const int *segid, int *tg_gid,
-                           int *tg_src, int *tg_off) {
+__global__ void k_segments(const u64 *keys, const u32 *vals, long n, int tile_n, int gbits, const int *segid,
+                           int *tg_gid, int *tg_src, int *tg_off) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const u64 k = keys[i];
@@ -235,7 +271,7 @@ __global__ void k_segments(const u64 *keys, const u32 *vals, long n, int gbits, 
   const int s = segid[i] - (first ? 0 : 1);
   if (first) tg_gid[s] = (int)(k & ((1ull << gbits) - 1));
   const u32 v = vals[i];
-  tg_src[(long)s * GP_TILE + (v >> IMG_SHIFT)] = (int)(v & IDX_MASK);
+  tg_src[(long)s * tile_n + (v >> SLOT_SHIFT)] = (int)(v & SLOT_MASK);
   const u64 tile = k >> gbits;
   if (i == 0 || (keys[i - 1] >> gbits) != tile) tg_off[tile] = s;
 }
@@ -323,6 +359,102 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
   }
 }
 
+// Mixed form on the tensor core: one CTA (4 warps) per tile of 128 targets.
+// For every group of the tile the operator (B: KP outputs x KP inputs) and
+// the 128 gathered scaled multipoles (A: 128 targets x KP inputs), both as
+// FP16 hi + lo parts, are staged in shared memory (K-major, no swizzle); one
+// thread issues the three products hi*hi + hi*lo + lo*hi per K step of 16
+// (tcgen05.mma kind::f16), accumulating in FP32 in tensor memory (128 lanes x
+// KP columns) across all groups of the tile.  The epilogue reads TMEM by warp
+// (lane = target), unscales and stores L in FP64.  Every mbarrier wait is
+// bounded; on timeout the CTA flags the error, waits again (bounded) for its
+// MMAs, frees TMEM and returns.
+__global__ void __launch_bounds__(TC_TILE) k_m2l_tc(const int *tile_tgt, const int *tg_off, const int *tg_gid,
+                                                    const int *tg_src, const __half *ops16, const __half *M16,
+                                                    const double4 *xr, double2 *L, int P, int KP, uint32_t ncols,
+                                                    int *err, long spin) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __half *Ah = (__half *)smraw, *Al = Ah + TC_TILE * KP, *Bh = Al + TC_TILE * KP, *Bl = Bh + KP * KP;
+  uint64_t *bar = (uint64_t *)(Bl + KP * KP);
+  uint32_t *tslot = (uint32_t *)(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, tile = blockIdx.x, NT = tri(P);
+  if (warp == 0) tc::alloc(tslot, ncols);
+  if (tid == 0) tc::mbar_init(bar, 1);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = tc::idesc_f16_f32(TC_TILE, KP);
+  const uint32_t lbo = 128, sbo = (uint32_t)(KP / 8) * 128;
+  const uint32_t aH = tc::smem_u32(Ah), aL = tc::smem_u32(Al), bH = tc::smem_u32(Bh), bL = tc::smem_u32(Bl);
+  uint32_t phase = 0;
+  bool ok = true, issued = false;
+  const int g0 = tg_off[tile], g1 = tg_off[tile + 1];
+  for (int g = g0; g < g1; g++) {
+    const uint4 *srcB = (const uint4 *)(ops16 + (size_t)tg_gid[g] * 2 * KP * KP);
+    uint4 *dstB = (uint4 *)Bh;  // Bh and Bl are contiguous, as in global memory
+    for (int i = tid; i < 2 * KP * KP / 8; i += TC_TILE) dstB[i] = srcB[i];
+    const int s = tg_src[(long)g * TC_TILE + tid];
+    const uint4 *mrow = (const uint4 *)(M16 + (size_t)(s < 0 ? 0 : s) * 2 * KP);
+    const uint4 z4 = make_uint4(0, 0, 0, 0);
+    for (int c = 0; c < KP / 8; c++) {
+      const int pos = tc::canon(tid, c * 8, KP);
+      *(uint4 *)(Ah + pos) = s >= 0 ? mrow[c] : z4;
+      *(uint4 *)(Al + pos) = s >= 0 ? mrow[KP / 8 + c] : z4;
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (tid == 0) {
+      for (int ks = 0; ks < KP / 16; ks++) {
+        const uint32_t o = (uint32_t)ks * 256;  // two 16-byte K chunks per K step
+        const uint64_t dAh = tc::smem_desc(aH + o, lbo, sbo), dAl = tc::smem_desc(aL + o, lbo, sbo);
+        const uint64_t dBh = tc::smem_desc(bH + o, lbo, sbo), dBl = tc::smem_desc(bL + o, lbo, sbo);
+        tc::mma_f16(tmem, dAh, dBh, idesc, (issued || ks > 0) ? 1u : 0u);
+        tc::mma_f16(tmem, dAh, dBl, idesc, 1u);
+        tc::mma_f16(tmem, dAl, dBh, idesc, 1u);
+      }
+      tc::commit(bar);
+    }
+    issued = true;
+    const bool done = tc::mbar_wait(bar, phase, spin);
+    phase ^= 1;
+    ok = __syncthreads_and(done) != 0;
+    if (!ok) break;
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    tc::mbar_wait(bar, phase ^ 1, spin);  // the MMAs of the failed step, bounded
+  }
+  tc::fence_after();
+  if (ok && issued) {
+    const int t = tile_tgt[tile * TC_TILE + tid];
+    const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
+    const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
+    int j = 0;
+    double sj = inv;  // inv^(j+1)
+    for (int c0 = 0; c0 < KP; c0 += 16) {
+      float v[16];
+      tc::ld_32x32b_x16(row + (uint32_t)c0, v);
+      if (t >= 0) {
+        for (int k = 0; k < 16; k += 2) {
+          const int o = (c0 + k) >> 1;
+          if (o >= NT) break;
+          while (tri(j + 1) <= o) {
+            j++;
+            sj *= inv;
+          }
+          L[(long)t * NT + o] = make_double2((double)v[k] * sj, (double)v[k + 1] * sj);
+        }
+      }
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::dealloc(tmem, ncols);
+}
+
 struct PlanCache {
   GroupPlan host;
   int *dev = nullptr;
@@ -377,6 +509,13 @@ int bits_for(long v) {
   return b;
 }
 
+size_t tc_smem(int KP) { return (size_t)(2 * TC_TILE * KP + 2 * KP * KP) * sizeof(__half) + 64; }
+
+bool tc_available(int P) {
+  const int KP = (P * (P + 1) + 15) / 16 * 16;
+  return KP <= 256 && tc_smem(KP) <= 200 * 1024;
+}
+
 }  // namespace
 
 bool m2l_grouped_available(int P) {
@@ -386,19 +525,25 @@ bool m2l_grouped_available(int P) {
 
 void m2l_grouped_set_attributes() {
   cudaFuncSetAttribute(k_gemm64, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 // Grouped M2L of the whole tree: L stored for every cell (zero where no
-// M2L entry), residual entries added by the direct-form kernel.
+// M2L entry), residual entries added by the direct-form kernel.  FP64 form:
+// DMMA over tiles of 32 targets; mixed form: tcgen05 split-FP16 over tiles of
+// 128 targets (orders whose operator does not fit fall back to DMMA).
 void m2l_grouped_pass(Handle &h) {
   cudaStream_t s = h.stream;
   const int P = h.prm.P, NT = tri(P), C = h.ncells;
   PlanCache &pc = plan_cache(P);
   const GroupPlan &gp = pc.host;
   const PlanDev pd = plan_dev(pc);
+  const bool tcore = h.prm.precision == EXAFMM_MIXED && tc_available(P);
+  const int tile_n = tcore ? TC_TILE : GP_TILE;
   const long nent = h.n_m2l;
   h.L.need((size_t)C * NT * sizeof(double2));
   FMM_CUDA(cudaMemsetAsync(h.L.p, 0, (size_t)C * NT * sizeof(double2), s));
+  h.g_used_tc = false;
   if (nent == 0) return;
 
   // scaled multipoles
@@ -426,18 +571,26 @@ void m2l_grouped_pass(Handle &h) {
     // operators
     h.g_keyof.need(ngroups * sizeof(int));
     k_key_of_gid<<<grid_for(KEY_SPACE, TB), TB, 0, s>>>(occ, gidx, h.g_keyof.as<int>());
-    h.g_ops.need((size_t)ngroups * gp.wsize * sizeof(double));
-    k_gops<<<ngroups, 128, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), pd, h.g_ops.as<double>());
+    if (tcore) {
+      h.g_ops.need((size_t)ngroups * 2 * gp.KP * gp.KP * sizeof(__half));
+      k_gops16<<<ngroups, 256, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), P, gp.KP, h.g_ops.as<__half>());
+      h.g_m16.need((size_t)C * 2 * gp.KP * sizeof(__half));
+      k_msplit16<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>((long)C * gp.KP, gp.KP, h.g_mt.as<double>(),
+                                                              h.g_m16.as<__half>());
+    } else {
+      h.g_ops.need((size_t)ngroups * gp.wsize * sizeof(double));
+      k_gops<<<ngroups, 128, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), pd, h.g_ops.as<double>());
+    }
     // tiles of targets
-    const int ntiles = (nflag + GP_TILE - 1) / GP_TILE;
+    const int ntiles = (nflag + tile_n - 1) / tile_n;
     h.g_tk.need((size_t)C * 2 * (sizeof(u64) + sizeof(u32)) + 64);
     u64 *tk = h.g_tk.as<u64>(), *tk2 = tk + C;
     u32 *tv = (u32 *)(tk2 + C), *tv2 = tv + C;
     k_tkeys<<<grid_for(C, TB), TB, 0, s>>>(C, gcount, h.c_level.as<int>(), h.c_parent.as<int>(), h.c_child.as<int>(),
                                            tk, tv);
     radix_sort_pairs(h, tk, tv, tk2, tv2, C, 0, 8);
-    h.g_tile.need((size_t)ntiles * GP_TILE * sizeof(int) + 64);
-    k_tiles<<<grid_for((long)ntiles * GP_TILE, TB), TB, 0, s>>>(ntiles, nflag, tv, h.g_tile.as<int>(), tslot);
+    h.g_tile.need((size_t)ntiles * tile_n * sizeof(int) + 64);
+    k_tiles<<<grid_for((long)ntiles * tile_n, TB), TB, 0, s>>>(ntiles, tile_n, nflag, tv, h.g_tile.as<int>(), tslot);
     // (tile, group) segments
     const long ngent = nent - nres;
     const int gbits = bits_for(ngroups), tbits = bits_for(ntiles + 1);
@@ -447,8 +600,8 @@ void m2l_grouped_pass(Handle &h) {
     u32 *ev = h.vals[0].as<u32>(), *ev2 = h.vals[1].as<u32>();
     FMM_CUDA(cudaMemsetAsync(&ctr->gfill, 0, sizeof(unsigned long long), s));
     k_gentries<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
-                                                        h.g_ekey.as<int>(), gidx, gcount, tslot, gbits, &ctr->gfill,
-                                                        ek, ev);
+                                                        h.g_ekey.as<int>(), gidx, gcount, tslot, tile_n, gbits,
+                                                        &ctr->gfill, ek, ev);
     radix_sort_pairs(h, ek, ev, ek2, ev2, ngent, 0, gbits + tbits);
     h.g_seg.need((ngent + 1) * sizeof(int) * 2);
     int *flag = h.g_seg.as<int>(), *segid = flag + ngent + 1;
@@ -457,15 +610,25 @@ void m2l_grouped_pass(Handle &h) {
     FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
     FMM_CUDA(cudaStreamSynchronize(s));
     const int nseg = h.hc.gcounts[3];
-    h.g_tg.need(((size_t)nseg * (GP_TILE + 1) + ntiles + 2) * sizeof(int));
+    h.g_tg.need(((size_t)nseg * (tile_n + 1) + ntiles + 2) * sizeof(int));
     int *tg_gid = h.g_tg.as<int>(), *tg_off = tg_gid + nseg, *tg_src = tg_off + ntiles + 1;
-    FMM_CUDA(cudaMemsetAsync(tg_src, 0xff, (size_t)nseg * GP_TILE * sizeof(int), s));
-    k_segments<<<grid_for(ngent, TB), TB, 0, s>>>(ek, ev, ngent, gbits, segid, tg_gid, tg_src, tg_off);
+    FMM_CUDA(cudaMemsetAsync(tg_src, 0xff, (size_t)nseg * tile_n * sizeof(int), s));
+    k_segments<<<grid_for(ngent, TB), TB, 0, s>>>(ek, ev, ngent, tile_n, gbits, segid, tg_gid, tg_src, tg_off);
     k_set_int<<<1, 1, 0, s>>>(tg_off + ntiles, &counts[3]);
     // contraction
-    k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                            h.g_ops.as<double>(), h.g_mt.as<double>(),
-                                                            h.c_xr.as<double4>(), h.L.as<double2>(), pd);
+    if (tcore) {
+      FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
+      const uint32_t ncols = gp.KP <= 128 ? 128u : 256u;
+      k_m2l_tc<<<ntiles, TC_TILE, tc_smem(gp.KP), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                       h.g_ops.as<__half>(), h.g_m16.as<__half>(),
+                                                       h.c_xr.as<double4>(), h.L.as<double2>(), P, gp.KP, ncols,
+                                                       &ctr->tc_error, 20000000L);
+      h.g_used_tc = true;
+    } else {
+      k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                              h.g_ops.as<double>(), h.g_mt.as<double>(),
+                                                              h.c_xr.as<double4>(), h.L.as<double2>(), pd);
+    }
     h.launches += 10;
     h.g_ntiles = ntiles;
     h.g_ngroups = ngroups;

@@ -100,13 +100,126 @@ __global__ void __launch_bounds__(DT) k_direct(const double4 *tgt, long nt, cons
   }
 }
 
+// ---------------------------------------------------------------- mixed form
+// Bodies as float offsets from their own leaf centre (FP64 subtraction, one
+// rounding), so the pair offset dx = (xi - ci) + (ci - cj) - (xj - cj) keeps
+// the bits that an FP32 copy of the absolute coordinates would lose.
+__global__ void k_make_srcf(const int *leaves, int nleaves, const int *begin, const int *count, const double4 *xr,
+                            const double4 *src, float4 *srcf) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  const double4 C = xr[c];
+  for (int b = begin[c] + lane; b < begin[c] + count[c]; b += 32) {
+    const double4 B = src[b];
+    srcf[b] = make_float4((float)(B.x - C.x), (float)(B.y - C.y), (float)(B.z - C.z), (float)B.w);
+  }
+}
+
+// Error-free sum s + p = t + e (Knuth's TwoSum), accumulated as (s, e).
+__device__ __forceinline__ void two_sum_acc(float &s, float &e, float p) {
+  const float t = s + p;
+  const float bp = t - s;
+  e += (s - (t - bp)) + (p - bp);
+  s = t;
+}
+
+__device__ __forceinline__ void pair_f32(float xi, float yi, float zi, const float4 s, float &pot, float &ax,
+                                         float &ay, float &az) {
+  const float dx = xi - s.x, dy = yi - s.y, dz = zi - s.z;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
+  const float qir = s.w * ir;
+  const float qir3 = qir * ir * ir;
+  pot += qir;
+  ax = fmaf(dx, qir3, ax);
+  ay = fmaf(dy, qir3, ay);
+  az = fmaf(dz, qir3, az);
+}
+
+// FP32 P2P: same mapping as k_p2p; FP32 partial sums per source leaf, then a
+// compensated (TwoSum) accumulation per target across the source leaves.
+__global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int nleaves, const int *begin,
+                                                        const int *count, const int *off, const u32 *ent,
+                                                        const double4 *xr, const float4 *srcf, double4 *out,
+                                                        double cycle) {
+  __shared__ float4 tile[WARPS][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * WARPS + wid;
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  const int tb = begin[c], tn = count[c];
+  const double4 CA = xr[c];
+  for (int t0 = 0; t0 < tn; t0 += 64) {
+    const int ia = tb + t0 + lane, ib = ia + 32;
+    const bool va = t0 + lane < tn, vb = t0 + lane + 32 < tn;
+    const float4 A = va ? srcf[ia] : make_float4(0, 0, 0, 0);
+    const float4 B = vb ? srcf[ib] : make_float4(0, 0, 0, 0);
+    float sa[4] = {0, 0, 0, 0}, ea[4] = {0, 0, 0, 0}, sb[4] = {0, 0, 0, 0}, eb[4] = {0, 0, 0, 0};
+    for (int e = off[c]; e < off[c + 1]; e++) {
+      const u32 en = ent[e];
+      const int sc = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
+      const double4 CB = xr[sc];
+      const float ox = (float)(CA.x - CB.x - (img % 3 - 1) * cycle);
+      const float oy = (float)(CA.y - CB.y - ((img / 3) % 3 - 1) * cycle);
+      const float oz = (float)(CA.z - CB.z - (img / 9 - 1) * cycle);
+      const float xa = A.x + ox, ya = A.y + oy, za = A.z + oz;
+      const float xb = B.x + ox, yb = B.y + oy, zb = B.z + oz;
+      float pa = 0, qa = 0, ra = 0, ta = 0, pb = 0, qb = 0, rb = 0, tb2 = 0;
+      const int sbeg = begin[sc], sn = count[sc];
+      for (int s0 = 0; s0 < sn; s0 += 32) {
+        const int m = min(32, sn - s0);
+        __syncwarp();
+        if (lane < m) tile[wid][lane] = srcf[sbeg + s0 + lane];
+        __syncwarp();
+        if (vb) {
+          for (int k = 0; k < m; k++) {
+            const float4 s = tile[wid][k];
+            pair_f32(xa, ya, za, s, pa, qa, ra, ta);
+            pair_f32(xb, yb, zb, s, pb, qb, rb, tb2);
+          }
+        } else {
+          for (int k = 0; k < m; k++) pair_f32(xa, ya, za, tile[wid][k], pa, qa, ra, ta);
+        }
+      }
+      two_sum_acc(sa[0], ea[0], pa);
+      two_sum_acc(sa[1], ea[1], qa);
+      two_sum_acc(sa[2], ea[2], ra);
+      two_sum_acc(sa[3], ea[3], ta);
+      two_sum_acc(sb[0], eb[0], pb);
+      two_sum_acc(sb[1], eb[1], qb);
+      two_sum_acc(sb[2], eb[2], rb);
+      two_sum_acc(sb[3], eb[3], tb2);
+    }
+    if (va)
+      out[ia] = make_double4((double)sa[0] + ea[0], -((double)sa[1] + ea[1]), -((double)sa[2] + ea[2]),
+                             -((double)sa[3] + ea[3]));
+    if (vb)
+      out[ib] = make_double4((double)sb[0] + eb[0], -((double)sb[1] + eb[1]), -((double)sb[2] + eb[2]),
+                             -((double)sb[3] + eb[3]));
+  }
+}
+
 }  // namespace
 
 void p2p_pass(Handle &h) {
   h.out.need((size_t)h.n * sizeof(double4));
+  const double cyc = h.prm.images ? h.prm.cycle : 0.0;
+  if (h.prm.precision == EXAFMM_MIXED) {
+    h.srcf.need((size_t)h.n * sizeof(float4));
+    k_make_srcf<<<grid_for((long)h.nleaves * 32, 256), 256, 0, h.stream>>>(
+        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
+        h.src.as<double4>(), h.srcf.as<float4>());
+    k_p2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
+        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
+        h.p2p_ent.as<u32>(), h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
+    h.launches += 2;
+    FMM_LAUNCH();
+    return;
+  }
   k_p2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
       h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
-      h.p2p_ent.as<u32>(), h.src.as<double4>(), h.out.as<double4>(), h.prm.images ? h.prm.cycle : 0.0);
+      h.p2p_ent.as<u32>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
   h.launches++;
   FMM_LAUNCH();
 }
