@@ -10,6 +10,7 @@ namespace fmm {
 double fma_peak_tflops(int precision);
 void m2l_set_attributes();
 void m2l_grouped_set_attributes();
+void p2p_set_attributes();
 void expansions_set_attributes();
 }  // namespace fmm
 
@@ -190,6 +191,7 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
         if (cudaEventCreate(&h.ev[p][k]) != cudaSuccess) h.ev_ok = false;
     m2l_set_attributes();
     m2l_grouped_set_attributes();
+    p2p_set_attributes();
     expansions_set_attributes();
     FMM_CUDA(cudaGetLastError());
   } catch (const Error &e) {

@@ -48,6 +48,10 @@ constexpr int XS = 36;      // padded row stride of the staged multipoles (doubl
 constexpr int SLOT_SHIFT = 25;  // sorted entry value = tile slot << 25 | source cell
 constexpr u32 SLOT_MASK = (1u << SLOT_SHIFT) - 1;
 constexpr int TC_TILE = 128;    // targets per tile on the tensor core (MMA M)
+// Groups accumulated in FP32 in tensor memory before the partial sum is added
+// to the FP64 local expansion: keeps the FP32 accumulation short enough that
+// the mixed form's potential error stays within a few percent of FP64's.
+constexpr int TC_FLUSH_EVERY = 16;
 
 __global__ void k_gkeys(int ncells, const int *off, const u32 *ent, const double4 *xr, const int *level, int *ekey,
                         int *occ, int *gcount, int *counts /*[0] residual entries, [1] flagged targets*/) {
@@ -369,10 +373,34 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
 // (lane = target), unscales and stores L in FP64.  Every mbarrier wait is
 // bounded; on timeout the CTA flags the error, waits again (bounded) for its
 // MMAs, frees TMEM and returns.
+// Adds the FP32 accumulator in TMEM (this thread's row = target t) into the
+// FP64 local expansion, unscaled (L = L~ / R_t^(j+1)).
+__device__ __forceinline__ void tc_flush(uint32_t row, int t, double inv, int KP, int NT, double2 *L) {
+  int j = 0;
+  double sj = inv;  // inv^(j+1)
+  for (int c0 = 0; c0 < KP; c0 += 16) {
+    float v[16];
+    tc::ld_32x32b_x16(row + (uint32_t)c0, v);
+    if (t >= 0) {
+      for (int k = 0; k < 16; k += 2) {
+        const int o = (c0 + k) >> 1;
+        if (o >= NT) break;
+        while (tri(j + 1) <= o) {
+          j++;
+          sj *= inv;
+        }
+        double2 &d = L[(long)t * NT + o];
+        d.x += (double)v[k] * sj;
+        d.y += (double)v[k + 1] * sj;
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(TC_TILE) k_m2l_tc(const int *tile_tgt, const int *tg_off, const int *tg_gid,
                                                     const int *tg_src, const __half *ops16, const __half *M16,
                                                     const double4 *xr, double2 *L, int P, int KP, uint32_t ncols,
-                                                    int *err, long spin) {
+                                                    int flush_every, int *err, long spin) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __half *Ah = (__half *)smraw, *Al = Ah + TC_TILE * KP, *Bh = Al + TC_TILE * KP, *Bl = Bh + KP * KP;
   uint64_t *bar = (uint64_t *)(Bl + KP * KP);
@@ -388,8 +416,12 @@ __global__ void __launch_bounds__(TC_TILE) k_m2l_tc(const int *tile_tgt, const i
   const uint32_t lbo = 128, sbo = (uint32_t)(KP / 8) * 128;
   const uint32_t aH = tc::smem_u32(Ah), aL = tc::smem_u32(Al), bH = tc::smem_u32(Bh), bL = tc::smem_u32(Bl);
   uint32_t phase = 0;
-  bool ok = true, issued = false;
+  bool ok = true;
   const int g0 = tg_off[tile], g1 = tg_off[tile + 1];
+  const int t = tile_tgt[tile * TC_TILE + tid];
+  const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
+  const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
+  int pending = 0;  // groups accumulated in TMEM since the last flush
   for (int g = g0; g < g1; g++) {
     const uint4 *srcB = (const uint4 *)(ops16 + (size_t)tg_gid[g] * 2 * KP * KP);
     uint4 *dstB = (uint4 *)Bh;  // Bh and Bl are contiguous, as in global memory
@@ -411,45 +443,31 @@ __global__ void __launch_bounds__(TC_TILE) k_m2l_tc(const int *tile_tgt, const i
         const uint32_t o = (uint32_t)ks * 256;  // two 16-byte K chunks per K step
         const uint64_t dAh = tc::smem_desc(aH + o, lbo, sbo), dAl = tc::smem_desc(aL + o, lbo, sbo);
         const uint64_t dBh = tc::smem_desc(bH + o, lbo, sbo), dBl = tc::smem_desc(bL + o, lbo, sbo);
-        tc::mma_f16(tmem, dAh, dBh, idesc, (issued || ks > 0) ? 1u : 0u);
+        tc::mma_f16(tmem, dAh, dBh, idesc, (pending > 0 || ks > 0) ? 1u : 0u);
         tc::mma_f16(tmem, dAh, dBl, idesc, 1u);
         tc::mma_f16(tmem, dAl, dBh, idesc, 1u);
       }
       tc::commit(bar);
     }
-    issued = true;
+    pending++;
     const bool done = tc::mbar_wait(bar, phase, spin);
     phase ^= 1;
     ok = __syncthreads_and(done) != 0;
     if (!ok) break;
+    if (pending == flush_every) {  // FP32 accumulation restarts: FP64 across groups
+      tc::fence_after();
+      tc_flush(row, t, inv, KP, NT, L);
+      tc::fence_before();
+      __syncthreads();
+      pending = 0;
+    }
   }
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
     tc::mbar_wait(bar, phase ^ 1, spin);  // the MMAs of the failed step, bounded
   }
   tc::fence_after();
-  if (ok && issued) {
-    const int t = tile_tgt[tile * TC_TILE + tid];
-    const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
-    const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
-    int j = 0;
-    double sj = inv;  // inv^(j+1)
-    for (int c0 = 0; c0 < KP; c0 += 16) {
-      float v[16];
-      tc::ld_32x32b_x16(row + (uint32_t)c0, v);
-      if (t >= 0) {
-        for (int k = 0; k < 16; k += 2) {
-          const int o = (c0 + k) >> 1;
-          if (o >= NT) break;
-          while (tri(j + 1) <= o) {
-            j++;
-            sj *= inv;
-          }
-          L[(long)t * NT + o] = make_double2((double)v[k] * sj, (double)v[k + 1] * sj);
-        }
-      }
-    }
-  }
+  if (ok && pending > 0) tc_flush(row, t, inv, KP, NT, L);
   tc::fence_before();
   __syncthreads();
   if (warp == 0) tc::dealloc(tmem, ncols);
@@ -622,6 +640,7 @@ void m2l_grouped_pass(Handle &h) {
       k_m2l_tc<<<ntiles, TC_TILE, tc_smem(gp.KP), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
                                                        h.g_ops.as<__half>(), h.g_m16.as<__half>(),
                                                        h.c_xr.as<double4>(), h.L.as<double2>(), P, gp.KP, ncols,
+                                                       TC_FLUSH_EVERY,
                                                        &ctr->tc_error, 20000000L);
       h.g_used_tc = true;
     } else {

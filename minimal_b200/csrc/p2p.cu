@@ -200,26 +200,195 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int n
   }
 }
 
+// ------------------------------------------------ CTA-per-leaf near field
+// One CTA per target leaf.  The bodies of up to 32 source leaves at a time
+// are staged in shared memory already shifted into the target's frame, so
+// the inner loop is a plain (target, source) sweep.  Thread t takes the
+// targets i, i+H, i+2H, i+3H with i = t % H, H = ceil(tn/4), and every G-th
+// staged source starting at g = t / H, G = floor(128/H): for leaves of 20-64
+// bodies nearly all 128 threads are busy, and each staged source is read once
+// per four pairs.  Partial sums of the G source groups are
+// combined in a fixed order at the end.  Leaves are limited to 64 bodies
+// (ncrit <= 64); larger leaves use the warp kernels above.
+constexpr int CT = 128;           // threads per CTA
+constexpr int CT_LEAVES = 32;     // source leaves staged at once
+constexpr int CT_MAXLEAF = 64;    // bodies per leaf the staging buffer allows
+constexpr int CT_TPT = 2;         // targets per thread (register blocking)
+
+template <bool F32>
+struct NearBody;
+template <>
+struct NearBody<false> {
+  typedef double4 T;
+  typedef double R;
+};
+template <>
+struct NearBody<true> {
+  typedef float4 T;
+  typedef float R;
+};
+
+template <bool F32>
+__global__ void __launch_bounds__(CT) k_p2p_cta(const int *leaves, const int *begin, const int *count,
+                                                const int *off, const u32 *ent, const double4 *xr,
+                                                const typename NearBody<F32>::T *bodies, double4 *out,
+                                                double cycle) {
+  typedef typename NearBody<F32>::T BT;
+  typedef typename NearBody<F32>::R RT;
+  extern __shared__ __align__(16) unsigned char stage_raw[];  // CT_LEAVES * CT_MAXLEAF bodies
+  BT *stage = (BT *)stage_raw;
+  __shared__ int soff[CT_LEAVES + 1];
+  __shared__ double red[CT * CT_TPT * 4];
+  const int c = leaves[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int tb = begin[c], tn = count[c];
+  const int H = (tn + CT_TPT - 1) / CT_TPT, G = CT / H;
+  const int i = tid % H, g = tid / H;
+  const bool act = g < G;
+  BT A[CT_TPT];
+#pragma unroll
+  for (int u = 0; u < CT_TPT; u++) A[u] = act && i + u * H < tn ? bodies[tb + i + u * H] : BT{};
+  const double4 CA = xr[c];
+  // accumulators: FP64 form plain; FP32 form compensated (s, e) per quantity
+  RT sacc[CT_TPT][4], eacc[CT_TPT][4];
+#pragma unroll
+  for (int u = 0; u < CT_TPT; u++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) sacc[u][q] = eacc[u][q] = 0;
+  const int eb = off[c], ee = off[c + 1];
+  for (int e0i = eb; e0i < ee; e0i += CT_LEAVES) {
+    const int nl = min(CT_LEAVES, ee - e0i);
+    __syncthreads();
+    if (tid < 32) {  // offsets of the chunk's leaves in the staging buffer
+      const int n = lane < nl ? count[ent[e0i + lane] & IDX_MASK] : 0;
+      int inc = n;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+      }
+      soff[lane + 1] = inc;
+      if (lane == 0) soff[0] = 0;
+    }
+    __syncthreads();
+    const int T = soff[nl];
+    for (int b = tid; b < T; b += CT) {
+      int k = 0;
+      while (soff[k + 1] <= b) k++;
+      const u32 en = ent[e0i + k];
+      const int sc = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
+      const BT s = bodies[begin[sc] + (b - soff[k])];
+      const double sx = (img % 3 - 1) * cycle, sy = ((img / 3) % 3 - 1) * cycle, sz = (img / 9 - 1) * cycle;
+      BT t;
+      if constexpr (F32) {  // source relative to its leaf -> relative to the target leaf
+        const double4 CB = xr[sc];
+        t.x = s.x - (float)(CA.x - CB.x - sx);
+        t.y = s.y - (float)(CA.y - CB.y - sy);
+        t.z = s.z - (float)(CA.z - CB.z - sz);
+      } else {
+        t.x = s.x + sx;
+        t.y = s.y + sy;
+        t.z = s.z + sz;
+      }
+      t.w = s.w;
+      stage[b] = t;
+    }
+    __syncthreads();
+    if (act) {
+      for (int b0 = g; b0 < T; b0 += 32 * G) {
+        RT p[CT_TPT][4];
+#pragma unroll
+        for (int u = 0; u < CT_TPT; u++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) p[u][q] = 0;
+        const int bend = min(T, b0 + 32 * G);
+        int b = b0;
+        for (; b + G < bend; b += 2 * G) {
+          const BT s0 = stage[b], s1 = stage[b + G];
+#pragma unroll
+          for (int u = 0; u < CT_TPT; u++) {
+            if constexpr (F32) {
+              pair_f32(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
+              pair_f32(A[u].x, A[u].y, A[u].z, s1, p[u][0], p[u][1], p[u][2], p[u][3]);
+            } else {
+              pair(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
+              pair(A[u].x, A[u].y, A[u].z, s1, p[u][0], p[u][1], p[u][2], p[u][3]);
+            }
+          }
+        }
+        if (b < bend) {
+          const BT s0 = stage[b];
+#pragma unroll
+          for (int u = 0; u < CT_TPT; u++) {
+            if constexpr (F32) pair_f32(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
+            else pair(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < CT_TPT; u++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            if constexpr (F32) two_sum_acc(sacc[u][q], eacc[u][q], p[u][q]);  // compensated per 32 sources
+            else sacc[u][q] += p[u][q];
+          }
+      }
+    }
+  }
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int u = 0; u < CT_TPT; u++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) red[(g * CT_TPT * H + i + u * H) * 4 + q] = (double)sacc[u][q] + (double)eacc[u][q];
+  }
+  __syncthreads();
+  if (tid < tn) {
+    double r[4] = {0, 0, 0, 0};
+    for (int gg = 0; gg < G; gg++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) r[q] += red[(gg * CT_TPT * H + tid) * 4 + q];
+    out[tb + tid] = make_double4(r[0], -r[1], -r[2], -r[3]);
+  }
+}
+
 }  // namespace
+
+void p2p_set_attributes() {
+  cudaFuncSetAttribute(k_p2p_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       CT_LEAVES * CT_MAXLEAF * (int)sizeof(double4));
+  cudaFuncSetAttribute(k_p2p_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       CT_LEAVES * CT_MAXLEAF * (int)sizeof(float4));
+}
 
 void p2p_pass(Handle &h) {
   h.out.need((size_t)h.n * sizeof(double4));
   const double cyc = h.prm.images ? h.prm.cycle : 0.0;
+  const bool cta = h.prm.ncrit <= CT_MAXLEAF;  // every leaf fits the staging layout
   if (h.prm.precision == EXAFMM_MIXED) {
     h.srcf.need((size_t)h.n * sizeof(float4));
     k_make_srcf<<<grid_for((long)h.nleaves * 32, 256), 256, 0, h.stream>>>(
         h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
         h.src.as<double4>(), h.srcf.as<float4>());
-    k_p2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
-        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
-        h.p2p_ent.as<u32>(), h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
+    if (cta)
+      k_p2p_cta<true><<<h.nleaves, CT, CT_LEAVES * CT_MAXLEAF * sizeof(float4), h.stream>>>(
+          h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
+          h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
+    else
+      k_p2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
+          h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
+          h.p2p_ent.as<u32>(), h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
     h.launches += 2;
     FMM_LAUNCH();
     return;
   }
-  k_p2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
-      h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
-      h.p2p_ent.as<u32>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
+  if (cta)
+    k_p2p_cta<false><<<h.nleaves, CT, CT_LEAVES * CT_MAXLEAF * sizeof(double4), h.stream>>>(
+        h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
+        h.c_xr.as<double4>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
+  else
+    k_p2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
+        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
+        h.p2p_ent.as<u32>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
   h.launches++;
   FMM_LAUNCH();
 }

@@ -64,9 +64,16 @@ __global__ void k_bounds_partial(const double4 *in, long n, double *part) {
 // getBounds (3d/build_tree.h:7-21): centre = (max+min)/2, R0 = largest
 // half-extent about that centre, times 1.00001.
 __global__ void k_bounds_final(const double *part, int nb, RootGeom *g) {
+  // min/max are exact, so the reduction order cannot change the result
+  __shared__ double s[TB][6];
   double lo[3] = {part[0], part[1], part[2]}, hi[3] = {part[3], part[4], part[5]};
-  for (int k = 1; k < nb; k++)
+  for (int k = threadIdx.x; k < nb; k += blockDim.x)
     for (int d = 0; d < 3; d++) { lo[d] = dmin(part[6 * k + d], lo[d]); hi[d] = dmax(part[6 * k + 3 + d], hi[d]); }
+  for (int d = 0; d < 3; d++) { s[threadIdx.x][d] = lo[d]; s[threadIdx.x][3 + d] = hi[d]; }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  for (int k = 1; k < blockDim.x; k++)
+    for (int d = 0; d < 3; d++) { lo[d] = dmin(s[k][d], lo[d]); hi[d] = dmax(s[k][3 + d], hi[d]); }
   double R0 = 0;
   for (int d = 0; d < 3; d++) {
     g->X0[d] = __ddiv_rn(__dadd_rn(hi[d], lo[d]), 2.0);
@@ -299,7 +306,7 @@ void build_tree(Handle &h) {
   const int nbp = (int)std::min<long>(4 * 148, (n + TB - 1) / TB);
   h.hist.need((size_t)nbp * 6 * sizeof(double));
   k_bounds_partial<<<nbp, TB, 0, s>>>(h.in.as<double4>(), n, h.hist.as<double>());
-  k_bounds_final<<<1, 1, 0, s>>>(h.hist.as<double>(), nbp, g);
+  k_bounds_final<<<1, TB, 0, s>>>(h.hist.as<double>(), nbp, g);
   h.launches += 2;
   FMM_LAUNCH();
 
