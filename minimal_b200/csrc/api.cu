@@ -146,6 +146,11 @@ void do_down(Handle &h) {
 
 void sync(Handle &h) {
   FMM_CUDA(cudaStreamSynchronize(h.stream));
+  if (h.flags_host && h.flags_host[0]) {
+    h.flags_host[0] = 0;
+    h.have_horiz = h.have_down = false;
+    throw Error{EXAFMM_ERR_TIMEOUT, "tensor-core M2L: a bounded wait ran out (results discarded)"};
+  }
   if (h.ev_ok) {
     for (int p = 0; p < PH_COUNT; p++) {
       float ms = 0;
@@ -185,6 +190,8 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     h.prm = *params;
     h.nterm = nterm_of(params->P);
     FMM_CUDA(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    FMM_CUDA(cudaMallocHost(&h.flags_host, 4 * sizeof(int)));
+    h.flags_host[0] = 0;
     h.ev_ok = true;
     for (int p = 0; p < PH_COUNT + 1; p++)
       for (int k = 0; k < 2; k++)
@@ -220,6 +227,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
     for (int p = 0; p < PH_COUNT + 1; p++)
       for (int k = 0; k < 2; k++) cudaEventDestroy(h.ev[p][k]);
   if (h.stream) cudaStreamDestroy(h.stream);
+  if (h.flags_host) cudaFreeHost(h.flags_host);
   delete H;
   return EXAFMM_OK;
 }

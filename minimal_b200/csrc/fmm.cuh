@@ -138,6 +138,10 @@ struct Handle {
   // phase state
   bool have_tree = false, have_lists = false, have_up = false, have_horiz = false, have_down = false;
 
+  // device error flags copied back on the stream (pinned), checked after
+  // each synchronisation: [0] a bounded tensor-core wait ran out
+  int *flags_host = nullptr;
+
   cudaEvent_t ev[PH_COUNT + 1][2];
   float ms[PH_COUNT + 1] = {0};
   bool ev_ok = false;

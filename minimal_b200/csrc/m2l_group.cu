@@ -48,6 +48,11 @@ constexpr int XS = 36;      // padded row stride of the staged multipoles (doubl
 constexpr int SLOT_SHIFT = 25;  // sorted entry value = tile slot << 25 | source cell
 constexpr u32 SLOT_MASK = (1u << SLOT_SHIFT) - 1;
 constexpr int TC_TILE = 128;    // targets per tile on the tensor core (MMA M)
+constexpr int TC_EPI_WARPS = 4; // warps 0-3: epilogue (warp w owns TMEM lanes 32w..32w+31)
+constexpr int TC_LOAD_WARP = 4; // first of the producer warps
+constexpr int TC_LOAD_WARPS = 4;
+constexpr int TC_MMA_WARP = TC_LOAD_WARP + TC_LOAD_WARPS;  // MMA issuer, TMEM owner
+constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
 // Groups accumulated in FP32 in tensor memory before the partial sum is added
 // to the FP64 local expansion: keeps the FP32 accumulation short enough that
 // the mixed form's potential error stays within a few percent of FP64's.
@@ -162,21 +167,60 @@ __global__ void k_gops(const int *key_of, PlanDev pd, double *ops) {
   }
 }
 
-// One CTA per group: the operator split into FP16 hi + lo parts, as the
-// tensor core's B operand (N = KP output rows, K-major, no swizzle).
-__global__ void k_gops16(const int *key_of, int P, int KP, __half *ops16) {
+// Tensor-core layout of the operators.  Output rows (N) are cut into blocks
+// of 64, one MMA N per block; a block whose smallest output order is j only
+// reads inputs of order n < P - j (the operator is zero beyond), so it keeps
+// 16 * ksteps input columns.  Each block is stored K-major with the 128-byte
+// swizzle: atoms of 64 input columns, each atom `rows` x 128 bytes.  The
+// multipole tile (A) is 128 rows x atomsA atoms, hi and lo parts.
+struct TcPlan {
+  int nb;                            // output row blocks
+  int rows[4], ksteps[4], boff[4];   // rows, K steps of 16, byte offset in one image
+  int bimg;                          // bytes of one (hi or lo) operator image
+  int atomsA;                        // 64-column atoms of the multipole tile
+  int abytes;                        // bytes of one (hi or lo) multipole tile
+};
+
+TcPlan make_tc_plan(int P, int KP) {
+  TcPlan t{};
+  t.nb = (KP + 63) / 64;
+  int off = 0;
+  for (int b = 0; b < t.nb; b++) {
+    t.rows[b] = KP - 64 * b < 64 ? KP - 64 * b : 64;
+    int j = 0;
+    while (tri(j + 1) <= 32 * b) j++;  // order of the block's first output
+    const int kreal = 2 * tri(P - j);
+    const int k16 = (kreal + 15) / 16 * 16;
+    t.ksteps[b] = (k16 < KP ? k16 : KP) / 16;
+    t.boff[b] = off;
+    off += (t.ksteps[b] + 3) / 4 * t.rows[b] * 128;
+  }
+  t.bimg = off;
+  t.atomsA = (KP + 63) / 64;
+  t.abytes = TC_TILE * 128 * t.atomsA;
+  return t;
+}
+
+// One CTA per group: the operator split into FP16 hi + lo parts, written as
+// the byte image the MMA reads from shared memory (hi image, then lo image).
+__global__ void k_gops16(const int *key_of, int P, TcPlan pl, __half *ops16) {
   extern __shared__ double2 Zsh[];
   const int g = blockIdx.x, NT = tri(P);
   const int dl = group_harmonics(key_of[g], P, Zsh);
-  __half *Wh = ops16 + (size_t)g * 2 * KP * KP, *Wl = Wh + KP * KP;
-  for (int i = threadIdx.x; i < KP * KP; i += blockDim.x) {
-    const int row = i / KP, col = i - row * KP;
-    const double w = op_value(row, col, P, NT, dl, Zsh);
+  const int nh = pl.bimg / 2;  // halves per image
+  __half *Wh = ops16 + (size_t)g * 2 * nh, *Wl = Wh + nh;
+  for (int e = threadIdx.x; e < nh; e += blockDim.x) {
+    const int byte = 2 * e;
+    int b = 0;
+    while (b + 1 < pl.nb && pl.boff[b + 1] <= byte) b++;
+    const int ab = pl.rows[b] * 128, rem = byte - pl.boff[b];
+    const int a = rem / ab, r2 = rem - a * ab;
+    const int rb = r2 >> 7, chunk = (r2 >> 4) & 7, q = (r2 >> 1) & 7;
+    const int k = a * 64 + ((chunk ^ (rb & 7)) << 3) + q;  // undo the swizzle
+    const double w = k < 16 * pl.ksteps[b] ? op_value(64 * b + rb, k, P, NT, dl, Zsh) : 0.0;
     const __half hi = __double2half(w);
-    const __half lo = __double2half(w - (double)__half2float(hi));
-    const int pos = tc::canon(row, col, KP);
-    Wh[pos] = hi;
-    Wl[pos] = lo;
+    Wh[e] = hi;
+    Wl[e] = __double2half(w - (double)__half2float(hi));
   }
 }
 
@@ -363,114 +407,278 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
   }
 }
 
-// Mixed form on the tensor core: one CTA (4 warps) per tile of 128 targets.
-// For every group of the tile the operator (B: KP outputs x KP inputs) and
-// the 128 gathered scaled multipoles (A: 128 targets x KP inputs), both as
-// FP16 hi + lo parts, are staged in shared memory (K-major, no swizzle); one
+// Mixed form on the tensor core: one CTA per tile of 128 targets, warp
+// specialised.  For every group of the tile the operator (B: N = output rows
+// in blocks of 64, K-truncated per block) and the 128 gathered scaled
+// multipoles (A: 128 targets x KP inputs), both as FP16 hi + lo parts in the
+// 128-byte swizzled K-major layout, are staged in shared memory, and one
 // thread issues the three products hi*hi + hi*lo + lo*hi per K step of 16
-// (tcgen05.mma kind::f16), accumulating in FP32 in tensor memory (128 lanes x
-// KP columns) across all groups of the tile.  The epilogue reads TMEM by warp
-// (lane = target), unscales and stores L in FP64.  Every mbarrier wait is
-// bounded; on timeout the CTA flags the error, waits again (bounded) for its
-// MMAs, frees TMEM and returns.
-// Adds the FP32 accumulator in TMEM (this thread's row = target t) into the
-// FP64 local expansion, unscaled (L = L~ / R_t^(j+1)).
-__device__ __forceinline__ void tc_flush(uint32_t row, int t, double inv, int KP, int NT, double2 *L) {
+// (tcgen05.mma kind::f16), accumulating in FP32 in tensor memory.
+//   producer warp: per group, waits for its stage to be free, then one bulk
+//     copy (operator) and 4-row TMA gathers (multipoles) land on the stage's
+//     barrier; two stages;
+//   MMA warp: waits for the stage, issues the MMAs, commits the stage back;
+//     two TMEM accumulators alternate every `flush_every` groups;
+//   epilogue warps: fold each finished accumulator into a double-FP32
+//     running sum in TMEM (or into L when TMEM has no room) while the tensor
+//     core fills the other, so no FP32 sum runs over more than `flush_every`
+//     groups; finally store L in FP64.
+// Every mbarrier wait is bounded; a role that times out flags the error and
+// stops, the others time out in turn, in-flight copies and MMAs are drained
+// (bounded) and TMEM is freed.
+// Accumulator epilogues.  Row = target t of this thread (TMEM lane).
+// tc_fold adds the FP32 accumulator into a double-FP32 running sum (hi, lo)
+// kept in TMEM beside it: Knuth's TwoSum per element, error terms summed in
+// lo, so the running sum carries ~48 bits.
+__device__ __forceinline__ void tc_fold(uint32_t acc, uint32_t hi, uint32_t lo, int cb, int ce) {
+  for (int c0 = cb; c0 < ce; c0 += 16) {
+    uint32_t a[16], h[16], l[16];
+    tc::ld_32x32b_x16_async(acc + (uint32_t)c0, a);
+    tc::ld_32x32b_x16_async(hi + (uint32_t)c0, h);
+    tc::ld_32x32b_x16_async(lo + (uint32_t)c0, l);
+    tc::wait_ld();
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const float x = __uint_as_float(a[k]), s0 = __uint_as_float(h[k]);
+      const float sum = s0 + x, bp = sum - s0;
+      const float e = (s0 - (sum - bp)) + (x - bp);
+      h[k] = __float_as_uint(sum);
+      l[k] = __float_as_uint(__uint_as_float(l[k]) + e);
+    }
+    tc::st_32x32b_x16(hi + (uint32_t)c0, h);
+    tc::st_32x32b_x16(lo + (uint32_t)c0, l);
+  }
+  tc::wait_st();
+}
+
+__device__ __forceinline__ void tc_zero(uint32_t cols, int cb, int ce) {
+  const uint32_t z[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int c0 = cb; c0 < ce; c0 += 16) tc::st_32x32b_x16(cols + (uint32_t)c0, z);
+  tc::wait_st();
+}
+
+// Stores the running sum as the FP64 local expansion, unscaled
+// (L = L~ / R_t^(j+1)).  The tile is the only grouped writer of its targets.
+__device__ __forceinline__ void tc_store(uint32_t hi, uint32_t lo, int t, double inv, int cb, int ce, int NT,
+                                         double2 *L) {
   int j = 0;
   double sj = inv;  // inv^(j+1)
-  for (int c0 = 0; c0 < KP; c0 += 16) {
-    float v[16];
-    tc::ld_32x32b_x16(row + (uint32_t)c0, v);
-    if (t >= 0) {
-      for (int k = 0; k < 16; k += 2) {
-        const int o = (c0 + k) >> 1;
-        if (o >= NT) break;
-        while (tri(j + 1) <= o) {
-          j++;
-          sj *= inv;
-        }
-        double2 &d = L[(long)t * NT + o];
-        d.x += (double)v[k] * sj;
-        d.y += (double)v[k + 1] * sj;
+  for (int c0 = cb; c0 < ce; c0 += 16) {
+    uint32_t h[16], l[16];
+    tc::ld_32x32b_x16_async(hi + (uint32_t)c0, h);
+    tc::ld_32x32b_x16_async(lo + (uint32_t)c0, l);
+    tc::wait_ld();
+    if (t < 0) continue;
+    for (int k = 0; k < 16; k += 2) {
+      const int o = (c0 + k) >> 1;
+      if (o >= NT) break;
+      while (tri(j + 1) <= o) {
+        j++;
+        sj *= inv;
       }
+      const double re = (double)__uint_as_float(h[k]) + (double)__uint_as_float(l[k]);
+      const double im = (double)__uint_as_float(h[k + 1]) + (double)__uint_as_float(l[k + 1]);
+      L[(long)t * NT + o] = make_double2(re * sj, im * sj);
     }
   }
 }
 
-__global__ void __launch_bounds__(TC_TILE) k_m2l_tc(const int *tile_tgt, const int *tg_off, const int *tg_gid,
-                                                    const int *tg_src, const __half *ops16, const __half *M16,
-                                                    const double4 *xr, double2 *L, int P, int KP, uint32_t ncols,
-                                                    int flush_every, int *err, long spin) {
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __half *Ah = (__half *)smraw, *Al = Ah + TC_TILE * KP, *Bh = Al + TC_TILE * KP, *Bl = Bh + KP * KP;
-  uint64_t *bar = (uint64_t *)(Bl + KP * KP);
-  uint32_t *tslot = (uint32_t *)(bar + 1);
-  const int tid = threadIdx.x, warp = tid >> 5, tile = blockIdx.x, NT = tri(P);
-  if (warp == 0) tc::alloc(tslot, ncols);
-  if (tid == 0) tc::mbar_init(bar, 1);
+// Without room in TMEM for the running sum (KP > 128): the accumulator is
+// added into the FP64 L in global memory, eight independent
+// read-modify-writes at a time.
+__device__ __forceinline__ void tc_flush_global(uint32_t acc, int t, double inv, int cb, int ce, int NT,
+                                                double2 *L) {
+  int j = 0;
+  double sj = inv;
+  for (int c0 = cb; c0 < ce; c0 += 16) {
+    float v[16];
+    tc::ld_32x32b_x16(acc + (uint32_t)c0, v);
+    if (t < 0) continue;
+    double2 cur[8];
+    double sc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int o = (c0 >> 1) + k;
+      sc[k] = 0;
+      if (o < NT) {
+        while (tri(j + 1) <= o) {
+          j++;
+          sj *= inv;
+        }
+        sc[k] = sj;
+        cur[k] = L[(long)t * NT + o];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int o = (c0 >> 1) + k;
+      if (o < NT)
+        L[(long)t * NT + o] =
+            make_double2(cur[k].x + (double)v[2 * k] * sc[k], cur[k].y + (double)v[2 * k + 1] * sc[k]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, const int *tg_off, const int *tg_gid,
+                                                          const int *tg_src, const unsigned char *ops,
+                                                          const __half *M16, const double4 *xr, double2 *L, int P,
+                                                          int KP, TcPlan pl,
+                                                          int nstage, uint32_t half_cols, int fold, int flush_every,
+                                                          int *err, long spin) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  unsigned char *base = smraw + ((1024u - (tc::smem_u32(smraw) & 1023u)) & 1023u);  // swizzle atoms: 1024-aligned
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, tile = blockIdx.x;
+  const uint32_t abytes = (uint32_t)pl.abytes, bimg = (uint32_t)pl.bimg;
+  const uint32_t stage_bytes = 2 * abytes + 2 * bimg;  // A hi, A lo, B hi, B lo
+  uint64_t *full = (uint64_t *)(base + (size_t)nstage * stage_bytes);  // [2] multipoles landed (producer warps)
+  uint64_t *bful = full + 2;                                           // [2] operator landed (bulk copy bytes)
+  uint64_t *empty = full + 4;                                          // [2] MMAs reading the stage finished
+  uint64_t *accf = full + 6;                                           // [2] accumulator window complete
+  uint64_t *acce = full + 8;                                           // [2] accumulator folded, reusable
+  uint32_t *tslot = (uint32_t *)(full + 10);
+  // TMEM columns: accumulators [0, H) and [H, 2H); with `fold`, the running
+  // sum hi at [2H, 3H) and lo at [3H, 4H)
+  const uint32_t ncols = (fold ? 4u : 2u) * half_cols;
+  if (warp == TC_MMA_WARP) tc::alloc(tslot, ncols);
+  if (tid == 0) {
+    for (int b = 0; b < 2; b++) tc::mbar_init(&full[b], TC_LOAD_WARPS * 32);
+    for (int b = 2; b < 8; b++) tc::mbar_init(&full[b], 1);
+    for (int b = 8; b < 10; b++) tc::mbar_init(&full[b], TC_EPI_WARPS);
+  }
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t idesc = tc::idesc_f16_f32(TC_TILE, KP);
-  const uint32_t lbo = 128, sbo = (uint32_t)(KP / 8) * 128;
-  const uint32_t aH = tc::smem_u32(Ah), aL = tc::smem_u32(Al), bH = tc::smem_u32(Bh), bL = tc::smem_u32(Bl);
-  uint32_t phase = 0;
-  bool ok = true;
-  const int g0 = tg_off[tile], g1 = tg_off[tile + 1];
-  const int t = tile_tgt[tile * TC_TILE + tid];
-  const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
-  const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
-  int pending = 0;  // groups accumulated in TMEM since the last flush
-  for (int g = g0; g < g1; g++) {
-    const uint4 *srcB = (const uint4 *)(ops16 + (size_t)tg_gid[g] * 2 * KP * KP);
-    uint4 *dstB = (uint4 *)Bh;  // Bh and Bl are contiguous, as in global memory
-    for (int i = tid; i < 2 * KP * KP / 8; i += TC_TILE) dstB[i] = srcB[i];
-    const int s = tg_src[(long)g * TC_TILE + tid];
-    const uint4 *mrow = (const uint4 *)(M16 + (size_t)(s < 0 ? 0 : s) * 2 * KP);
-    const uint4 z4 = make_uint4(0, 0, 0, 0);
-    for (int c = 0; c < KP / 8; c++) {
-      const int pos = tc::canon(tid, c * 8, KP);
-      *(uint4 *)(Ah + pos) = s >= 0 ? mrow[c] : z4;
-      *(uint4 *)(Al + pos) = s >= 0 ? mrow[KP / 8 + c] : z4;
+  const int g0 = tg_off[tile], n = tg_off[tile + 1] - g0;
+  const int nwin = (n + flush_every - 1) / flush_every;
+  auto parity = [&](int k) { return (uint32_t)(k / nstage) & 1u; };
+
+  if (warp < TC_EPI_WARPS) {
+    // ---- epilogue: warp w owns TMEM lanes 32w.. = targets 32w..
+    const int t = tile_tgt[tile * TC_TILE + tid];
+    const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
+    const int NT = tri(P);
+    const uint32_t lanes = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t sum_hi = lanes + 2 * half_cols, sum_lo = lanes + 3 * half_cols;
+    if (fold) {
+      tc_zero(sum_hi, 0, KP);
+      tc_zero(sum_lo, 0, KP);
     }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    tc::fence_after();
-    if (tid == 0) {
-      for (int ks = 0; ks < KP / 16; ks++) {
-        const uint32_t o = (uint32_t)ks * 256;  // two 16-byte K chunks per K step
-        const uint64_t dAh = tc::smem_desc(aH + o, lbo, sbo), dAl = tc::smem_desc(aL + o, lbo, sbo);
-        const uint64_t dBh = tc::smem_desc(bH + o, lbo, sbo), dBl = tc::smem_desc(bL + o, lbo, sbo);
-        tc::mma_f16(tmem, dAh, dBh, idesc, (pending > 0 || ks > 0) ? 1u : 0u);
-        tc::mma_f16(tmem, dAh, dBl, idesc, 1u);
-        tc::mma_f16(tmem, dAl, dBh, idesc, 1u);
-      }
-      tc::commit(bar);
-    }
-    pending++;
-    const bool done = tc::mbar_wait(bar, phase, spin);
-    phase ^= 1;
-    ok = __syncthreads_and(done) != 0;
-    if (!ok) break;
-    if (pending == flush_every) {  // FP32 accumulation restarts: FP64 across groups
+    bool ok = true;
+    for (int w = 0; w < nwin; w++) {
+      const int a = w & 1;
+      ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[a], (uint32_t)(w >> 1) & 1u, spin));
+      if (!ok) break;
       tc::fence_after();
-      tc_flush(row, t, inv, KP, NT, L);
+      const uint32_t acc = lanes + (uint32_t)a * half_cols;
+      if (fold) tc_fold(acc, sum_hi, sum_lo, 0, KP);
+      else tc_flush_global(acc, t, inv, 0, KP, NT, L);
       tc::fence_before();
-      __syncthreads();
-      pending = 0;
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&acce[a]);
     }
+    if (!ok) {
+      if (lane == 0) atomicExch(err, 1);
+    } else if (fold && n > 0) {
+      tc_store(sum_hi, sum_lo, t, inv, 0, KP, NT, L);
+    }
+  } else if (warp < TC_LOAD_WARP + TC_LOAD_WARPS) {
+    // ---- producers: thread r copies target row r of the tile -- the 16-byte
+    // chunks of its source cell's multipole (hi then lo halves, contiguous
+    // in global memory) with cp.async into the swizzled layout; absent
+    // targets are zero-filled.  A warp thus has 32 rows in flight per
+    // instruction.  Producer thread 0 also starts the operator's bulk copy.
+    // Each thread's copies arrive on the stage's barrier by themselves
+    // (cp.async.mbarrier.arrive), so the producers run up to two groups
+    // ahead of the MMAs.
+    const int r = tid - TC_LOAD_WARP * 32;
+    const int nchunk = KP / 4;  // 16-byte chunks per source row (hi and lo)
+    const uint32_t rsw = (uint32_t)(r & 7) << 4;
+    auto src_of = [&](int k) { return k < n ? tg_src[(long)(g0 + k) * TC_TILE + r] : -1; };
+    auto issue = [&](int k, int s) {
+      const int st = k % nstage;
+      unsigned char *S = base + (size_t)st * stage_bytes + r * 128;
+      if (r == 0) {
+        tc::mbar_arrive_expect_tx(&bful[st], 2 * bimg);
+        tc::bulk_g2s(S + 2 * abytes, ops + (size_t)tg_gid[g0 + k] * 2 * bimg, 2 * bimg, &bful[st]);
+      }
+      const __half *src = M16 + (size_t)(s < 0 ? 0 : s) * 2 * KP;
+      const uint32_t nb = s >= 0 ? 16u : 0u;
+      for (int c = 0; c < nchunk; c++) {
+        const int hl = c >= nchunk / 2, cc = c - hl * (nchunk / 2);
+        const uint32_t off = hl * abytes + (cc >> 3) * (TC_TILE * 128) + (((uint32_t)(cc & 7) << 4) ^ rsw);
+        tc::cp_async16(S + off, src + c * 8, nb);
+      }
+      tc::cp_async_commit();
+    };
+    bool ok = true;
+    int last = -1;
+    int s_next = src_of(0);
+    for (int k = 0; k < n; k++) {
+      if (k >= nstage) {  // the stage is free once the MMAs of group k - nstage are done
+        ok = __all_sync(0xffffffffu, tc::mbar_wait(&empty[k % nstage], (uint32_t)(k / nstage - 1) & 1u, spin));
+        if (!ok) break;
+      }
+      issue(k, s_next);
+      tc::cp_async_arrive(&full[k % nstage]);  // arrives when this thread's copies have landed
+      last = k;
+      s_next = src_of(k + 1);
+    }
+    if (!ok && lane == 0) atomicExch(err, 1);
+    tc::cp_async_wait_all();
+    if (r == 0 && last >= 0) tc::mbar_wait(&bful[last % nstage], parity(last), spin);  // drain (bounded)
+  } else if (warp == TC_MMA_WARP) {
+    // ---- MMA issuer (one thread): per group and output block, K steps of
+    // hi*hi + hi*lo + lo*hi into the window's accumulator
+    if (lane == 0) {
+      int rows[4], ksteps[4];
+      uint32_t boff[4], idesc[4];
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        rows[b] = b < pl.nb ? pl.rows[b] : 0;
+        ksteps[b] = b < pl.nb ? pl.ksteps[b] : 0;
+        boff[b] = b < pl.nb ? (uint32_t)pl.boff[b] : 0u;
+        idesc[b] = tc::idesc_f16_f32(TC_TILE, rows[b] > 0 ? rows[b] : 16);
+      }
+      bool ok = true;
+      int last = -1;
+      for (int k = 0; k < n; k++) {
+        const int st = k % nstage, w = k / flush_every, a = w & 1;
+        ok = tc::mbar_wait(&full[st], parity(k), spin) && tc::mbar_wait(&bful[st], parity(k), spin);
+        if (ok && k % flush_every == 0 && w >= 2) ok = tc::mbar_wait(&acce[a], (uint32_t)((w >> 1) - 1) & 1u, spin);
+        if (!ok) break;
+        tc::fence_async_smem();  // the producers' cp.async writes -> the tensor core's reads
+        tc::fence_after();
+        const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
+        const uint64_t dA = tc::smem_desc_sw128(sA), dB = tc::smem_desc_sw128(sB);
+        const uint64_t lo_a = abytes >> 4, lo_b = bimg >> 4;  // descriptor start fields count 16 bytes
+        const bool fresh = k % flush_every == 0;
+        const uint32_t acc = tmem + (uint32_t)a * half_cols;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          if (b >= pl.nb) break;
+          for (int ks = 0; ks < ksteps[b]; ks++) {
+            const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
+            const uint64_t bo = ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * rows[b] * 128 + (uint64_t)(ks & 3) * 32) >> 4;
+            const uint32_t d = acc + 64u * (uint32_t)b;
+            tc::mma_f16(d, dA + ao, dB + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
+            tc::mma_f16(d, dA + ao, dB + lo_b + bo, idesc[b], 1u);
+            tc::mma_f16(d, dA + lo_a + ao, dB + bo, idesc[b], 1u);
+          }
+        }
+        tc::commit(&empty[st]);
+        if (k % flush_every == flush_every - 1 || k == n - 1) tc::commit(&accf[a]);
+        last = k;
+      }
+      if (!ok) atomicExch(err, 1);
+      if (last >= 0) tc::mbar_wait(&empty[last % nstage], parity(last), spin);  // drain (bounded)
+    }
+    __syncwarp();
   }
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-    tc::mbar_wait(bar, phase ^ 1, spin);  // the MMAs of the failed step, bounded
-  }
-  tc::fence_after();
-  if (ok && pending > 0) tc_flush(row, t, inv, KP, NT, L);
   tc::fence_before();
   __syncthreads();
-  if (warp == 0) tc::dealloc(tmem, ncols);
+  tc::fence_after();
+  if (warp == TC_MMA_WARP) tc::dealloc(tmem, ncols);
 }
 
 struct PlanCache {
@@ -527,11 +735,23 @@ int bits_for(long v) {
   return b;
 }
 
-size_t tc_smem(int KP) { return (size_t)(2 * TC_TILE * KP + 2 * KP * KP) * sizeof(__half) + 64; }
+constexpr size_t TC_SMEM_MAX = 227 * 1024;  // opt-in shared memory per CTA on sm_100
+
+int tc_kp(int P) { return (P * (P + 1) + 15) / 16 * 16; }
+size_t tc_stage_bytes(const TcPlan &t) { return 2 * (size_t)t.abytes + 2 * (size_t)t.bimg; }
+// + 1024 to align the stages to the swizzle atom, + 128 for 10 barriers and the TMEM slot
+int tc_stages(const TcPlan &t) { return 2 * tc_stage_bytes(t) + 1024 + 128 <= TC_SMEM_MAX ? 2 : 1; }
+size_t tc_smem(const TcPlan &t) { return tc_stages(t) * tc_stage_bytes(t) + 1024 + 128; }
+// columns of one TMEM accumulator: a power of two >= KP (and >= 32)
+uint32_t tc_half_cols(int KP) {
+  uint32_t c = 32;
+  while (c < (uint32_t)KP) c <<= 1;
+  return c;
+}
 
 bool tc_available(int P) {
-  const int KP = (P * (P + 1) + 15) / 16 * 16;
-  return KP <= 256 && tc_smem(KP) <= 200 * 1024;
+  const int KP = tc_kp(P);
+  return KP <= 256 && tc_smem(make_tc_plan(P, KP)) <= TC_SMEM_MAX;
 }
 
 }  // namespace
@@ -543,7 +763,7 @@ bool m2l_grouped_available(int P) {
 
 void m2l_grouped_set_attributes() {
   cudaFuncSetAttribute(k_gemm64, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
 }
 
 // Grouped M2L of the whole tree: L stored for every cell (zero where no
@@ -557,6 +777,8 @@ void m2l_grouped_pass(Handle &h) {
   const GroupPlan &gp = pc.host;
   const PlanDev pd = plan_dev(pc);
   const bool tcore = h.prm.precision == EXAFMM_MIXED && tc_available(P);
+  const int KP16 = tc_kp(P);
+  const TcPlan tp = make_tc_plan(P, KP16);
   const int tile_n = tcore ? TC_TILE : GP_TILE;
   const long nent = h.n_m2l;
   h.L.need((size_t)C * NT * sizeof(double2));
@@ -590,11 +812,11 @@ void m2l_grouped_pass(Handle &h) {
     h.g_keyof.need(ngroups * sizeof(int));
     k_key_of_gid<<<grid_for(KEY_SPACE, TB), TB, 0, s>>>(occ, gidx, h.g_keyof.as<int>());
     if (tcore) {
-      h.g_ops.need((size_t)ngroups * 2 * gp.KP * gp.KP * sizeof(__half));
-      k_gops16<<<ngroups, 256, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), P, gp.KP, h.g_ops.as<__half>());
-      h.g_m16.need((size_t)C * 2 * gp.KP * sizeof(__half));
-      k_msplit16<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>((long)C * gp.KP, gp.KP, h.g_mt.as<double>(),
-                                                              h.g_m16.as<__half>());
+      h.g_ops.need((size_t)ngroups * 2 * tp.bimg);
+      k_gops16<<<ngroups, 256, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), P, tp, h.g_ops.as<__half>());
+      h.g_m16.need((size_t)C * 2 * KP16 * sizeof(__half));
+      k_msplit16<<<grid_for((long)C * KP16, TB), TB, 0, s>>>((long)C * KP16, KP16, h.g_mt.as<double>(),
+                                                             h.g_m16.as<__half>());
     } else {
       h.g_ops.need((size_t)ngroups * gp.wsize * sizeof(double));
       k_gops<<<ngroups, 128, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), pd, h.g_ops.as<double>());
@@ -629,19 +851,22 @@ void m2l_grouped_pass(Handle &h) {
     FMM_CUDA(cudaStreamSynchronize(s));
     const int nseg = h.hc.gcounts[3];
     h.g_tg.need(((size_t)nseg * (tile_n + 1) + ntiles + 2) * sizeof(int));
-    int *tg_gid = h.g_tg.as<int>(), *tg_off = tg_gid + nseg, *tg_src = tg_off + ntiles + 1;
+    // tg_src first: its rows of tile_n slots stay 16-byte aligned
+    int *tg_src = h.g_tg.as<int>(), *tg_gid = tg_src + (size_t)nseg * tile_n, *tg_off = tg_gid + nseg;
     FMM_CUDA(cudaMemsetAsync(tg_src, 0xff, (size_t)nseg * tile_n * sizeof(int), s));
     k_segments<<<grid_for(ngent, TB), TB, 0, s>>>(ek, ev, ngent, tile_n, gbits, segid, tg_gid, tg_src, tg_off);
     k_set_int<<<1, 1, 0, s>>>(tg_off + ntiles, &counts[3]);
     // contraction
     if (tcore) {
       FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
-      const uint32_t ncols = gp.KP <= 128 ? 128u : 256u;
-      k_m2l_tc<<<ntiles, TC_TILE, tc_smem(gp.KP), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                       h.g_ops.as<__half>(), h.g_m16.as<__half>(),
-                                                       h.c_xr.as<double4>(), h.L.as<double2>(), P, gp.KP, ncols,
-                                                       TC_FLUSH_EVERY,
-                                                       &ctr->tc_error, 20000000L);
+      const uint32_t hc = tc_half_cols(KP16);
+      k_m2l_tc<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                      h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
+                                                      h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
+                                                      tc_stages(tp), hc,
+                                                      4 * hc <= 512 ? 1 : 0, TC_FLUSH_EVERY, &ctr->tc_error,
+                                                      20000000L);
+      FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
       h.g_used_tc = true;
     } else {
       k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,

@@ -124,11 +124,25 @@ __device__ __forceinline__ void two_sum_acc(float &s, float &e, float p) {
   s = t;
 }
 
+// 1/sqrt(r2) from the hardware approximation (relative error below 2^-22),
+// 0 for r2 = 0; subnormal r2 counts as 0 (flush to zero), so pairs closer
+// than ~1e-19 in the leaf frame are skipped like coincident ones.
+__device__ __forceinline__ float rsqrt_or_zero(float r2) {
+  float y;
+  asm("{\n\t.reg .pred p;\n\t"
+      "setp.gt.ftz.f32 p, %1, 0f00000000;\n\t"
+      "rsqrt.approx.ftz.f32 %0, %1;\n\t"
+      "@!p mov.f32 %0, 0f00000000;\n\t}"
+      : "=f"(y)
+      : "f"(r2));
+  return y;
+}
+
 __device__ __forceinline__ void pair_f32(float xi, float yi, float zi, const float4 s, float &pot, float &ax,
                                          float &ay, float &az) {
   const float dx = xi - s.x, dy = yi - s.y, dz = zi - s.z;
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float ir = r2 > 0.f ? rsqrtf(r2) : 0.f;
+  const float ir = rsqrt_or_zero(r2);
   const float qir = s.w * ir;
   const float qir3 = qir * ir * ir;
   pot += qir;
@@ -202,14 +216,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int n
 
 // ------------------------------------------------ CTA-per-leaf near field
 // One CTA per target leaf.  The bodies of up to 32 source leaves at a time
-// are staged in shared memory already shifted into the target's frame, so
-// the inner loop is a plain (target, source) sweep.  Thread t takes the
-// targets i, i+H, i+2H, i+3H with i = t % H, H = ceil(tn/4), and every G-th
-// staged source starting at g = t / H, G = floor(128/H): for leaves of 20-64
-// bodies nearly all 128 threads are busy, and each staged source is read once
-// per four pairs.  Partial sums of the G source groups are
-// combined in a fixed order at the end.  Leaves are limited to 64 bodies
-// (ncrit <= 64); larger leaves use the warp kernels above.
+// are staged in shared memory already shifted into the target's frame (warp
+// w copies source leaves w, w+4, ...; the shift is computed once per leaf),
+// so the inner loop is a plain (target, source) sweep.  Thread t takes the
+// targets i and i+H with i = t % H, H = ceil(tn/2), and every G-th staged
+// source starting at g = t / H, G = floor(128/H): for leaves of 20-64 bodies
+// nearly all 128 threads are busy, and each staged source is read once per
+// two pairs.  Partial sums of the G source groups are combined in a fixed
+// order at the end.  Leaves are limited to 64 bodies (ncrit <= 64); larger
+// leaves use the warp kernels above.
 constexpr int CT = 128;           // threads per CTA
 constexpr int CT_LEAVES = 32;     // source leaves staged at once
 constexpr int CT_MAXLEAF = 64;    // bodies per leaf the staging buffer allows
@@ -272,26 +287,31 @@ __global__ void __launch_bounds__(CT) k_p2p_cta(const int *leaves, const int *be
     }
     __syncthreads();
     const int T = soff[nl];
-    for (int b = tid; b < T; b += CT) {
-      int k = 0;
-      while (soff[k + 1] <= b) k++;
+    for (int k = tid >> 5; k < nl; k += CT / 32) {
       const u32 en = ent[e0i + k];
       const int sc = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
-      const BT s = bodies[begin[sc] + (b - soff[k])];
+      const int sb = begin[sc], sn = count[sc], so = soff[k];
       const double sx = (img % 3 - 1) * cycle, sy = ((img / 3) % 3 - 1) * cycle, sz = (img / 9 - 1) * cycle;
-      BT t;
+      RT ox, oy, oz;
       if constexpr (F32) {  // source relative to its leaf -> relative to the target leaf
         const double4 CB = xr[sc];
-        t.x = s.x - (float)(CA.x - CB.x - sx);
-        t.y = s.y - (float)(CA.y - CB.y - sy);
-        t.z = s.z - (float)(CA.z - CB.z - sz);
+        ox = (float)(CA.x - CB.x - sx);
+        oy = (float)(CA.y - CB.y - sy);
+        oz = (float)(CA.z - CB.z - sz);
       } else {
-        t.x = s.x + sx;
-        t.y = s.y + sy;
-        t.z = s.z + sz;
+        ox = -sx;
+        oy = -sy;
+        oz = -sz;
       }
-      t.w = s.w;
-      stage[b] = t;
+      for (int b = lane; b < sn; b += 32) {
+        const BT s = bodies[sb + b];
+        BT t;
+        t.x = s.x - ox;
+        t.y = s.y - oy;
+        t.z = s.z - oz;
+        t.w = s.w;
+        stage[so + b] = t;
+      }
     }
     __syncthreads();
     if (act) {

@@ -24,6 +24,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
   return d;
 }
 
+// Shared-memory matrix descriptor, K-major operand with the 128-byte swizzle:
+// rows of 64 halves (128 bytes) whose 16-byte chunks are permuted by
+// chunk ^ (row % 8) within 1024-byte atoms of 8 rows (the layout a TMA load
+// with CU_TENSOR_MAP_SWIZZLE_128B writes).  sbo = 1024 (8-row groups); the
+// leading offset is fixed at one 16-byte unit; atoms must be 1024-aligned.
+// A K step of 16 inside an atom advances the start address by 32 bytes.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;            // leading byte offset: 16 bytes
+  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset: 1024 bytes
+  d |= (uint64_t)1 << 46;            // descriptor version (Blackwell)
+  d |= (uint64_t)2 << 61;            // layout type: 128-byte swizzle
+  return d;
+}
+
 // Instruction descriptor, kind::f16: A and B f16, K-major; D f32; M x N.
 __host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
   return (1u << 4)                     // D format f32
@@ -84,6 +100,41 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long l
   return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Arrival that also announces `bytes` of asynchronous copies to land on the
+// barrier (the bulk copy below completes them).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// One-dimensional bulk copy global -> this CTA's shared memory (no
+// multicast); `bytes` and both addresses are multiples of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// 16-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Arrival on the barrier once all of this thread's earlier cp.async copies
+// have landed (the barrier's expected count includes these arrivals).
+__device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// all but the most recently committed group complete
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 // 32 lanes x 32 bit, 16 consecutive columns per thread.
 __device__ __forceinline__ void ld_32x32b_x16(uint32_t taddr, float *v) {
   uint32_t r[16];
@@ -96,6 +147,27 @@ __device__ __forceinline__ void ld_32x32b_x16(uint32_t taddr, float *v) {
 #pragma unroll
   for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
+
+// The same load without the wait, so that several loads share one wait_ld().
+__device__ __forceinline__ void ld_32x32b_x16_async(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 32 lanes x 32 bit, 16 consecutive columns per thread, registers -> TMEM.
+__device__ __forceinline__ void st_32x32b_x16(uint32_t taddr, const uint32_t *r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // Element offset of (row, col) in a K-major no-swizzle operand with kp
 // columns: [row/8][col/8][row%8][col%8].
