@@ -4,9 +4,10 @@
 // the level-synchronous launches respect: a cell's children are complete
 // before its M2M, and its parent's local is final before its L2L).
 //
-// Mapping: one warp per cell.  Harmonic columns are built by lane = order m
-// into shared memory; the translations then give each lane whole output
-// coefficients (j,k), accumulated in a warp-private shared buffer.
+// Mapping: P2M and L2P take one warp per leaf and one lane per body.  M2M
+// and L2L take one thread per (cell, output coefficient (j,k)); the offset
+// harmonics they need depend only on level and octant and come from a
+// table built once per upward pass.
 #include "fmm.cuh"
 #include "harmonics.cuh"
 
@@ -22,6 +23,10 @@ __device__ __forceinline__ double2 ylook(const double2 *Y, int n, int o) {
 }
 
 __device__ __forceinline__ int sgn(int n) { return (n & 1) ? -1 : 1; }
+
+__device__ __forceinline__ int octant_of(const double4 &child, const double4 &parent) {
+  return (child.x > parent.x) | ((child.y > parent.y) << 1) | ((child.z > parent.z) << 2);
+}
 
 // 1/k for the Legendre and factorial recurrences (k = 1..2*EXAFMM_MAX_P+2).
 __constant__ double c_recip[2 * EXAFMM_MAX_P + 4];
@@ -91,96 +96,162 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m(const int *leaves, int nleav
 }
 
 // M2M (3d/kernel.h:204-231), one warp per parent at one level.
-__global__ void __launch_bounds__(WARPS * 32) k_m2m(int c0, int c1, const int *child, const int *nchild,
-                                                    const double4 *xr, double2 *M, int P) {
-  extern __shared__ double2 sh[];
-  const int nt = tri(P);
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = c0 + blockIdx.x * WARPS + wid;
-  if (c >= c1) return;
-  const int nk = nchild[c];
-  if (nk == 0) return;
-  double2 *acc = sh + wid * 3 * nt, *Y = acc + nt, *Mc = Y + nt;
-  for (int k = lane; k < nt; k += 32) acc[k] = make_double2(0, 0);
-  const double4 X = xr[c];
-  for (int q = child[c]; q < child[c] + nk; q++) {
-    const double4 K = xr[q];
-    const Sph g = sph_of(X.x - K.x, X.y - K.y, X.z - K.z);
-    __syncwarp();
-    if (lane < P)
-      regular_column(lane, P, g.r, g, g.e, [&](int n, double2 v, double2) { Y[tri(n) + lane] = v; });
-    for (int k = lane; k < nt; k += 32) Mc[k] = M[(long)q * nt + k];
-    __syncwarp();
-    for (int o = lane; o < nt; o += 32) {
-      int j = 0;
-      while (tri(j + 1) <= o) j++;
-      const int k = o - tri(j);
-      double2 s = make_double2(0, 0);
-      for (int n = 0; n <= j; n++) {
-        const int lo = max(-n, -j + k + n), hi = min(k - 1, n);
-        for (int m = lo; m <= hi; m++) {
-          const double2 a = cmul(Mc[tri(j - n) + k - m], ylook(Y, n, -m));
-          const double f = (double)((m >= 0 ? 1 : sgn(m)) * sgn(n));
-          s.x += a.x * f;
-          s.y += a.y * f;
-        }
-        const int hi2 = min(n, j + k - n);
-        for (int m = k; m <= hi2; m++) {
-          const double2 a = cmul(cconj(Mc[tri(j - n) - k + m]), ylook(Y, n, -m));
-          const double f = (double)sgn(k + n + m);
-          s.x += a.x * f;
-          s.y += a.y * f;
-        }
-      }
-      acc[o].x += s.x;
-      acc[o].y += s.y;
+// M2M and L2L.  A child sits at its parent's centre +-R_child on every
+// axis, so the offset harmonics depend only on the octant and, through
+// rho = R_child, on the level: Y_n = rho^n Yhat_n with Yhat the harmonics of
+// the unit offset (+-1, +-1, +-1).  The 16 unit tables (M2M: parent - child,
+// L2L: child - parent; octant bit b set = child on the + side of axis b) are
+// built once per order P; each launch scales them for its level.
+// ytab[(dir * 8 + oct) * nt + tri(n) + m], dir 0 = M2M, 1 = L2L.
+// Both kernels take one CTA per parent and one thread per (octant, output
+// coefficient (j,k)), all inputs staged in shared memory.
+
+// M2M output (j,k) from one child's multipole Mc and the offset harmonics Y
+// (offset parent - child).
+__device__ double2 m2m_coeff(int j, int k, const double2 *Mc, const double2 *Y) {
+  double2 s = make_double2(0, 0);
+  for (int n = 0; n <= j; n++) {
+    const int lo = max(-n, -j + k + n), hi = min(k - 1, n);
+    for (int m = lo; m <= hi; m++) {
+      const double2 a = cmul(Mc[tri(j - n) + k - m], ylook(Y, n, -m));
+      const double f = (double)((m >= 0 ? 1 : sgn(m)) * sgn(n));
+      s.x += a.x * f;
+      s.y += a.y * f;
+    }
+    const int hi2 = min(n, j + k - n);
+    for (int m = k; m <= hi2; m++) {
+      const double2 a = cmul(cconj(Mc[tri(j - n) - k + m]), ylook(Y, n, -m));
+      const double f = (double)sgn(k + n + m);
+      s.x += a.x * f;
+      s.y += a.y * f;
     }
   }
-  __syncwarp();
-  for (int k = lane; k < nt; k += 32) M[(long)c * nt + k] = acc[k];
+  return s;
 }
 
-// L2L (3d/kernel.h:262-291), one warp per child at one level: the child
-// pulls its parent's local expansion.
-__global__ void __launch_bounds__(WARPS * 32) k_l2l(int c0, int c1, const int *parent, const double4 *xr,
-                                                    double2 *L, int P) {
-  extern __shared__ double2 sh[];
-  const int nt = tri(P);
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = c0 + blockIdx.x * WARPS + wid;
-  if (c >= c1) return;
-  const int pa = parent[c];
-  double2 *Y = sh + wid * 2 * nt, *Lp = Y + nt;
-  const double4 X = xr[c], Q = xr[pa];
-  const Sph g = sph_of(X.x - Q.x, X.y - Q.y, X.z - Q.z);
-  if (lane < P)
-    regular_column(lane, P, g.r, g, g.e, [&](int n, double2 v, double2) { Y[tri(n) + lane] = v; });
-  for (int k = lane; k < nt; k += 32) Lp[k] = L[(long)pa * nt + k];
-  __syncwarp();
-  for (int o = lane; o < nt; o += 32) {
-    int j = 0;
-    while (tri(j + 1) <= o) j++;
-    const int k = o - tri(j);
-    double2 s = make_double2(0, 0);
-    for (int n = j; n < P; n++) {
-      for (int m = j + k - n; m < 0; m++) {
-        const double2 a = cmul(cconj(Lp[tri(n) - m]), ylook(Y, n - j, m - k));
-        const double f = (double)sgn(k);
+// L2L output (j,k) from the parent's local Lp and the offset harmonics Y
+// (offset child - parent).
+__device__ double2 l2l_coeff(int j, int k, int P, const double2 *Lp, const double2 *Y) {
+  double2 s = make_double2(0, 0);
+  for (int n = j; n < P; n++) {
+    for (int m = j + k - n; m < 0; m++) {
+      const double2 a = cmul(cconj(Lp[tri(n) - m]), ylook(Y, n - j, m - k));
+      const double f = (double)sgn(k);
+      s.x += a.x * f;
+      s.y += a.y * f;
+    }
+    for (int m = 0; m <= n; m++) {
+      if (n - j >= abs(m - k)) {
+        const double2 a = cmul(Lp[tri(n) + m], ylook(Y, n - j, m - k));
+        const double f = (double)sgn((m - k) * (m < k));
         s.x += a.x * f;
         s.y += a.y * f;
       }
-      for (int m = 0; m <= n; m++) {
-        if (n - j >= abs(m - k)) {
-          const double2 a = cmul(Lp[tri(n) + m], ylook(Y, n - j, m - k));
-          const double f = (double)sgn((m - k) * (m < k));
-          s.x += a.x * f;
-          s.y += a.y * f;
-        }
-      }
     }
-    double2 &d = L[(long)c * nt + o];
-    d.x += s.x;
-    d.y += s.y;
+  }
+  return s;
+}
+
+__device__ __forceinline__ int order_of(int ci) {
+  int n = 0;
+  while (tri(n + 1) <= ci) n++;
+  return n;
+}
+
+__global__ void k_unit_tables(int P, double2 *ytab) {
+  const int nt = tri(P);
+  const int oct = blockIdx.x & 7, dir = blockIdx.x >> 3;
+  const double sx = (oct & 1) ? 1.0 : -1.0, sy = (oct & 2) ? 1.0 : -1.0, sz = (oct & 4) ? 1.0 : -1.0;
+  const double f = dir == 0 ? -1.0 : 1.0;  // M2M: parent - child; L2L: child - parent
+  const Sph g = sph_of(sx * f, sy * f, sz * f);
+  double2 *Y = ytab + (size_t)blockIdx.x * nt;
+  const int m = threadIdx.x;
+  if (m < P) regular_column(m, P, g.r, g, g.e, [&](int n, double2 v, double2) { Y[tri(n) + m] = v; });
+}
+
+constexpr int SH_O = 64;          // threads per octant (outputs; more loop for P > 10)
+constexpr int SH_T = 8 * SH_O;    // threads per CTA
+
+// Y[oct][idx] = rho^n * Yhat[dir][oct][idx] into shared memory.
+__device__ void stage_tables(double2 *Y, const double2 *ytab, int dir, double rho, int P) {
+  const int nt = tri(P);
+  for (int e = threadIdx.x; e < 8 * nt; e += blockDim.x) {
+    const int oct = e / nt, idx = e - oct * nt;
+    const int n = order_of(idx);
+    double sc = 1;
+    for (int q = 0; q < n; q++) sc *= rho;
+    Y[e] = cscale(ytab[(size_t)(dir * 8 + oct) * nt + idx], sc);
+  }
+}
+
+// M2M of one level: thread (oct, o) translates the child in octant oct (if
+// any); the eight contributions are summed in octant order.
+__global__ void __launch_bounds__(SH_T) k_m2m(int c0, const int *child, const int *nchild, const double4 *xr,
+                                             const double2 *ytab, double2 *M, int P) {
+  extern __shared__ double2 sm2[];  // Y[8][nt], Mc[8][nt], part[8][nt]
+  __shared__ int cho[8];
+  const int nt = tri(P), c = c0 + blockIdx.x;
+  const int nk = nchild[c];
+  if (nk == 0) return;
+  double2 *Y = sm2, *Mc = Y + 8 * nt, *part = Mc + 8 * nt;
+  const double4 X = xr[c];
+  if (threadIdx.x < 8) cho[threadIdx.x] = -1;
+  __syncthreads();
+  if (threadIdx.x < nk) {
+    const int q = child[c] + threadIdx.x;
+    cho[octant_of(xr[q], X)] = q;
+  }
+  stage_tables(Y, ytab, 0, X.w * 0.5, P);
+  __syncthreads();
+  for (int e = threadIdx.x; e < 8 * nt; e += SH_T) {
+    const int oct = e / nt, q = cho[oct];
+    Mc[e] = q >= 0 ? M[(long)q * nt + (e - oct * nt)] : make_double2(0, 0);
+  }
+  __syncthreads();
+  const int oct = threadIdx.x / SH_O;
+  for (int o = threadIdx.x % SH_O; o < nt; o += SH_O) {
+    const int j = order_of(o), k = o - tri(j);
+    part[oct * nt + o] = cho[oct] >= 0 ? m2m_coeff(j, k, Mc + oct * nt, Y + oct * nt) : make_double2(0, 0);
+  }
+  __syncthreads();
+  for (int o = threadIdx.x; o < nt; o += SH_T) {
+    double2 sum = make_double2(0, 0);
+    for (int q = 0; q < 8; q++) {
+      sum.x += part[q * nt + o].x;
+      sum.y += part[q * nt + o].y;
+    }
+    M[(long)c * nt + o] = sum;
+  }
+}
+
+// L2L of one level of parents: thread (oct, o) adds the parent's local,
+// shifted, into output o of its child in octant oct.
+__global__ void __launch_bounds__(SH_T) k_l2l(int c0, const int *child, const int *nchild, const double4 *xr,
+                                             const double2 *ytab, double2 *L, int P) {
+  extern __shared__ double2 sm2[];  // Y[8][nt], Lp[nt]
+  __shared__ int cho[8];
+  const int nt = tri(P), c = c0 + blockIdx.x;
+  const int nk = nchild[c];
+  if (nk == 0) return;
+  double2 *Y = sm2, *Lp = Y + 8 * nt;
+  const double4 X = xr[c];
+  if (threadIdx.x < 8) cho[threadIdx.x] = -1;
+  __syncthreads();
+  if (threadIdx.x < nk) {
+    const int q = child[c] + threadIdx.x;
+    cho[octant_of(xr[q], X)] = q;
+  }
+  stage_tables(Y, ytab, 1, X.w * 0.5, P);
+  for (int e = threadIdx.x; e < nt; e += SH_T) Lp[e] = L[(long)c * nt + e];
+  __syncthreads();
+  const int oct = threadIdx.x / SH_O, q = cho[oct];
+  if (q < 0) return;
+  for (int o = threadIdx.x % SH_O; o < nt; o += SH_O) {
+    const int j = order_of(o), k = o - tri(j);
+    const double2 v = l2l_coeff(j, k, P, Lp, Y + oct * nt);
+    double2 &d = L[(long)q * nt + o];
+    d.x += v.x;
+    d.y += v.y;
   }
 }
 
@@ -248,9 +319,20 @@ void expansions_set_attributes() {
   for (int k = 1; k < 2 * EXAFMM_MAX_P + 4; k++) rc[k] = 1.0 / k;
   FMM_CUDA(cudaMemcpyToSymbol(c_recip, rc, sizeof(rc)));
   cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_l2p, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_l2p, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+// Unit offset harmonics for order P (cached per handle).
+void unit_tables(Handle &h) {
+  const int P = h.prm.P;
+  if (h.shift_P == P) return;
+  h.shift_ops.need((size_t)16 * tri(P) * sizeof(double2));
+  k_unit_tables<<<16, 32, 0, h.stream>>>(P, h.shift_ops.as<double2>());
+  h.launches++;
+  FMM_LAUNCH();
+  h.shift_P = P;
 }
 
 void upward_pass(Handle &h) {
@@ -263,11 +345,13 @@ void upward_pass(Handle &h) {
       h.src.as<double4>(), h.M.as<double2>(), P);
   h.launches++;
   FMM_LAUNCH();
+  unit_tables(h);
   for (int l = h.depth - 1; l >= 0; l--) {
     const int c0 = h.level_base[l], c1 = h.level_base[l + 1];
     if (c1 <= c0) continue;
-    k_m2m<<<grid_for(c1 - c0, WARPS), WARPS * 32, WARPS * 3 * nt * sizeof(double2), s>>>(
-        c0, c1, h.c_child.as<int>(), h.c_nchild.as<int>(), h.c_xr.as<double4>(), h.M.as<double2>(), P);
+    k_m2m<<<c1 - c0, SH_T, 24 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
+                                                          h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
+                                                          h.M.as<double2>(), P);
     h.launches++;
     FMM_LAUNCH();
   }
@@ -276,11 +360,13 @@ void upward_pass(Handle &h) {
 void downward_pass(Handle &h) {
   cudaStream_t s = h.stream;
   const int P = h.prm.P, nt = tri(P);
-  for (int l = 1; l <= h.depth; l++) {
+  unit_tables(h);
+  for (int l = 0; l < h.depth; l++) {  // parents at level l push to their children
     const int c0 = h.level_base[l], c1 = h.level_base[l + 1];
     if (c1 <= c0) continue;
-    k_l2l<<<grid_for(c1 - c0, WARPS), WARPS * 32, WARPS * 2 * nt * sizeof(double2), s>>>(
-        c0, c1, h.c_parent.as<int>(), h.c_xr.as<double4>(), h.L.as<double2>(), P);
+    k_l2l<<<c1 - c0, SH_T, 9 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
+                                                         h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
+                                                         h.L.as<double2>(), P);
     h.launches++;
     FMM_LAUNCH();
   }
