@@ -122,8 +122,24 @@ EXAFMM_API int exafmm_b200_get_expansions(exafmm_b200 *h, double *M, double *L);
 
 /* Direct summation of all current bodies onto nt targets (Body records in
  * host or device memory; p and F accumulate), FP64: replaces direct()
- * (3d/traverse_eager.h:193-202). */
+ * (3d/traverse_eager.h:193-202).  With images > 0 the sources repeat over
+ * (2r+1)^3 copies shifted by multiples of cycle, r = sum_{i<images} 3^i, as
+ * in the periodic direct() (3dp/traverse_eager.h:131-154). */
 EXAFMM_API int exafmm_b200_direct(exafmm_b200 *h, double *targets8, int64_t nt, int where);
+
+/* Periodic systems (images > 0).  Dipole correction of the current results
+ * in place (3dp/fmm.cxx:63-75): with d = sum q X, coef = 4 pi / (3 cycle^3),
+ * p -= coef |d|^2 / N / q and F -= coef d; FP64. */
+EXAFMM_API int exafmm_b200_dipole_correction(exafmm_b200 *h);
+
+/* Ewald summation of the current bodies (all sources, FP64) onto nt targets
+ * (Body records in host or device memory; p and F accumulate): wave part over
+ * the integer wave vectors 0 < |k| <= ksize of initWaves, real part with the
+ * nearest image per axis inside `cutoff`, and the self term, with the
+ * parameters of 3dp/ewald.h (alpha, sigma, cutoff; cycle from the handle).
+ * Replaces wavePart + realPart + selfTerm (3dp/ewald.h:83-149). */
+EXAFMM_API int exafmm_b200_ewald(exafmm_b200 *h, int ksize, double alpha, double sigma, double cutoff,
+                                 double *targets8, int64_t nt, int where);
 
 /* Per-phase device times of the last evaluation in milliseconds, measured
  * with CUDA events on the handle's stream: tree, lists, upward, m2l, p2p,

@@ -37,6 +37,7 @@ API = [
     "exafmm_b200_get_perm", "exafmm_b200_num_cells", "exafmm_b200_get_tree", "exafmm_b200_count_lists",
     "exafmm_b200_get_lists", "exafmm_b200_get_expansions", "exafmm_b200_direct", "exafmm_b200_get_timings",
     "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak", "exafmm_b200_direct_static",
+    "exafmm_b200_dipole_correction", "exafmm_b200_ewald",
 ]
 
 PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
@@ -91,6 +92,8 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_arch": (i, []),
         "exafmm_b200_fma_peak": (i, [vp, i, vp]),
         "exafmm_b200_direct_static": (i, [vp, i64, vp, i64, vp]),
+        "exafmm_b200_dipole_correction": (i, [vp]),
+        "exafmm_b200_ewald": (i, [vp, i, d, d, d, vp, i64, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -228,6 +231,23 @@ class FMM:
         """FP64 direct sum of all loaded bodies onto targets (Body records; p, F accumulate)."""
         t = as_records(targets).copy()
         self._check(self.lib.exafmm_b200_direct(self.h, _p(t), len(t), HOST))
+        return t
+
+    def dipole_correction(self):
+        """Periodic systems: dipole correction of the current results in place
+        (3dp/fmm.cxx:63-75)."""
+        self._check(self.lib.exafmm_b200_dipole_correction(self.h))
+
+    def ewald(self, targets, ksize=11, alpha=None, sigma=0.25 / np.pi, cutoff=None):
+        """FP64 Ewald summation of all loaded bodies onto targets (Body
+        records; p, F accumulate).  Defaults follow 3dp/fmm.cxx:20-23:
+        alpha = ksize / cycle, cutoff = cycle / 2."""
+        cyc = self.params.cycle
+        alpha = ksize / cyc if alpha is None else alpha
+        cutoff = cyc / 2 if cutoff is None else cutoff
+        t = as_records(targets).copy()
+        self._check(self.lib.exafmm_b200_ewald(self.h, int(ksize), float(alpha), float(sigma), float(cutoff), _p(t),
+                                               len(t), HOST))
         return t
 
     def timings(self):

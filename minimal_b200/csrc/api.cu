@@ -125,10 +125,10 @@ void do_up(Handle &h) {
 void do_horiz(Handle &h) {
   if (!h.have_up) throw Error{EXAFMM_ERR_STATE, "upward() must run before horizontal()"};
   if (!h.have_lists) do_lists(h);
-  if (h.prm.images > 0) throw Error{EXAFMM_ERR_STATE, "periodic images are not available in this build"};
   {
     Timer t(h, PH_M2L);
     m2l_pass(h);
+    periodic_pass(h);  // far images beyond the first layer (images >= 2)
   }
   {
     Timer t(h, PH_P2P);
@@ -200,6 +200,7 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     m2l_grouped_set_attributes();
     p2p_set_attributes();
     expansions_set_attributes();
+    periodic_set_attributes();
     FMM_CUDA(cudaGetLastError());
   } catch (const Error &e) {
     exafmm_b200_static_err = e.msg;
@@ -415,6 +416,34 @@ int exafmm_b200_direct(exafmm_b200 *H, double *targets, int64_t nt, int where) {
     rec.release();
     xq.release();
     pf.release();
+  });
+}
+
+int exafmm_b200_dipole_correction(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) {
+    if (!h.have_down) throw Error{EXAFMM_ERR_STATE, "dipole_correction() needs the results of evaluate()"};
+    if (h.prm.images <= 0) throw Error{EXAFMM_ERR_STATE, "dipole_correction() is for periodic systems (images > 0)"};
+    dipole_correction(h);
+  });
+}
+
+int exafmm_b200_ewald(exafmm_b200 *H, int ksize, double alpha, double sigma, double cutoff, double *targets,
+                      int64_t nt, int where) {
+  return guarded(H, [&](Handle &h) {
+    need_tree(h);
+    if (!targets || nt <= 0) throw Error{EXAFMM_ERR_ARG, "need targets"};
+    if (ksize < 1 || ksize > 64 || !(alpha > 0) || !(sigma > 0) || !(cutoff > 0))
+      throw Error{EXAFMM_ERR_ARG, "ewald: ksize in [1, 64] and positive alpha, sigma, cutoff required"};
+    if (!(h.prm.cycle > 0)) throw Error{EXAFMM_ERR_STATE, "ewald() needs a periodic handle (cycle > 0)"};
+    Buf rec;
+    rec.need(nt * 64);
+    FMM_CUDA(cudaMemcpyAsync(rec.p, targets, nt * 64, where == EXAFMM_HOST ? cudaMemcpyHostToDevice
+                                                                          : cudaMemcpyDeviceToDevice, h.stream));
+    ewald(h, ksize, alpha, sigma, cutoff, h.prm.cycle, rec.as<double>(), nt);
+    FMM_CUDA(cudaMemcpyAsync(targets, rec.p, nt * 64, where == EXAFMM_HOST ? cudaMemcpyDeviceToHost
+                                                                          : cudaMemcpyDeviceToDevice, h.stream));
+    FMM_CUDA(cudaStreamSynchronize(h.stream));
+    rec.release();
   });
 }
 

@@ -10,23 +10,13 @@
 // table built once per upward pass.
 #include "fmm.cuh"
 #include "harmonics.cuh"
+#include "translations.cuh"
 
 namespace fmm {
 
 namespace {
 
 constexpr int WARPS = 4;
-
-// Y(deg, o) for any sign of o from the m>=0 table.
-__device__ __forceinline__ double2 ylook(const double2 *Y, int n, int o) {
-  return o >= 0 ? Y[tri(n) + o] : cconj(Y[tri(n) - o]);
-}
-
-__device__ __forceinline__ int sgn(int n) { return (n & 1) ? -1 : 1; }
-
-__device__ __forceinline__ int octant_of(const double4 &child, const double4 &parent) {
-  return (child.x > parent.x) | ((child.y > parent.y) << 1) | ((child.z > parent.z) << 2);
-}
 
 // 1/k for the Legendre and factorial recurrences (k = 1..2*EXAFMM_MAX_P+2).
 __constant__ double c_recip[2 * EXAFMM_MAX_P + 4];
@@ -105,58 +95,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m(const int *leaves, int nleav
 // ytab[(dir * 8 + oct) * nt + tri(n) + m], dir 0 = M2M, 1 = L2L.
 // Both kernels take one CTA per parent and one thread per (octant, output
 // coefficient (j,k)), all inputs staged in shared memory.
-
-// M2M output (j,k) from one child's multipole Mc and the offset harmonics Y
-// (offset parent - child).
-__device__ double2 m2m_coeff(int j, int k, const double2 *Mc, const double2 *Y) {
-  double2 s = make_double2(0, 0);
-  for (int n = 0; n <= j; n++) {
-    const int lo = max(-n, -j + k + n), hi = min(k - 1, n);
-    for (int m = lo; m <= hi; m++) {
-      const double2 a = cmul(Mc[tri(j - n) + k - m], ylook(Y, n, -m));
-      const double f = (double)((m >= 0 ? 1 : sgn(m)) * sgn(n));
-      s.x += a.x * f;
-      s.y += a.y * f;
-    }
-    const int hi2 = min(n, j + k - n);
-    for (int m = k; m <= hi2; m++) {
-      const double2 a = cmul(cconj(Mc[tri(j - n) - k + m]), ylook(Y, n, -m));
-      const double f = (double)sgn(k + n + m);
-      s.x += a.x * f;
-      s.y += a.y * f;
-    }
-  }
-  return s;
-}
-
-// L2L output (j,k) from the parent's local Lp and the offset harmonics Y
-// (offset child - parent).
-__device__ double2 l2l_coeff(int j, int k, int P, const double2 *Lp, const double2 *Y) {
-  double2 s = make_double2(0, 0);
-  for (int n = j; n < P; n++) {
-    for (int m = j + k - n; m < 0; m++) {
-      const double2 a = cmul(cconj(Lp[tri(n) - m]), ylook(Y, n - j, m - k));
-      const double f = (double)sgn(k);
-      s.x += a.x * f;
-      s.y += a.y * f;
-    }
-    for (int m = 0; m <= n; m++) {
-      if (n - j >= abs(m - k)) {
-        const double2 a = cmul(Lp[tri(n) + m], ylook(Y, n - j, m - k));
-        const double f = (double)sgn((m - k) * (m < k));
-        s.x += a.x * f;
-        s.y += a.y * f;
-      }
-    }
-  }
-  return s;
-}
-
-__device__ __forceinline__ int order_of(int ci) {
-  int n = 0;
-  while (tri(n + 1) <= ci) n++;
-  return n;
-}
 
 __global__ void k_unit_tables(int P, double2 *ytab) {
   const int nt = tri(P);

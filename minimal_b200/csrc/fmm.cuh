@@ -166,6 +166,11 @@ void m2l_pass(Handle &h);
 // p2p.cu
 void p2p_pass(Handle &h);
 void direct_sum(Handle &h, double4 *targets_pq /*x,y,z,q*/, double4 *out, long nt);
+// periodic.cu
+void periodic_set_attributes();
+void periodic_pass(Handle &h);
+void dipole_correction(Handle &h);
+void ewald(Handle &h, int ksize, double alpha, double sigma, double cutoff, double cycle, double *rec_dev, long nt);
 
 inline int nterm_of(int P) { return P * (P + 1) / 2; }
 inline unsigned grid_for(long n, int block) { return (unsigned)((n + block - 1) / block); }

@@ -79,7 +79,7 @@ constexpr int DT = 256;
 constexpr int DCHUNK = 8192;
 
 __global__ void __launch_bounds__(DT) k_direct(const double4 *tgt, long nt, const double4 *src, long ns,
-                                               double4 *out) {
+                                               double4 *out, int prange, double cycle) {
   __shared__ double4 tile[DT];
   const long i = (long)blockIdx.x * DT + threadIdx.x;
   const long s0 = (long)blockIdx.y * DCHUNK, s1 = min(ns, s0 + DCHUNK);
@@ -90,7 +90,12 @@ __global__ void __launch_bounds__(DT) k_direct(const double4 *tgt, long nt, cons
     if (b + threadIdx.x < s1) tile[threadIdx.x] = src[b + threadIdx.x];
     __syncthreads();
     const int m = (int)min((long)DT, s1 - b);
-    for (int k = 0; k < m; k++) pair(T.x, T.y, T.z, tile[k], p, ax, ay, az);
+    for (int ix = -prange; ix <= prange; ix++)
+      for (int iy = -prange; iy <= prange; iy++)
+        for (int iz = -prange; iz <= prange; iz++) {
+          const double tx = T.x - ix * cycle, ty = T.y - iy * cycle, tz = T.z - iz * cycle;
+          for (int k = 0; k < m; k++) pair(tx, ty, tz, tile[k], p, ax, ay, az);
+        }
   }
   if (i < nt) {
     atomicAdd(&out[i].x, p);
@@ -415,7 +420,10 @@ void p2p_pass(Handle &h) {
 
 void direct_sum(Handle &h, double4 *targets, double4 *out, long nt) {
   dim3 grid(grid_for(nt, DT), grid_for(h.n, DCHUNK));
-  k_direct<<<grid, DT, 0, h.stream>>>(targets, nt, h.src.as<double4>(), h.n, out);
+  int prange = 0;  // periodic images: r = sum_{i < images} 3^i (3dp/traverse_eager.h:139-142)
+  for (int i = 0, p3 = 1; i < h.prm.images; i++, p3 *= 3) prange += p3;
+  k_direct<<<grid, DT, 0, h.stream>>>(targets, nt, h.src.as<double4>(), h.n, out, prange,
+                                      h.prm.images ? h.prm.cycle : 0.0);
   h.launches++;
   FMM_LAUNCH();
 }
