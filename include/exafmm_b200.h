@@ -141,6 +141,20 @@ EXAFMM_API int exafmm_b200_dipole_correction(exafmm_b200 *h);
 EXAFMM_API int exafmm_b200_ewald(exafmm_b200 *h, int ksize, double alpha, double sigma, double cutoff,
                                  double *targets8, int64_t nt, int where);
 
+/* Batch of independent free-space systems (no reference counterpart: the
+ * reference evaluates one system per process).  bodies8 holds the systems'
+ * Body records one after the other; system q owns records
+ * [offsets[q], offsets[q+1]) (offsets: nsys+1 values, offsets[0] = 0, each
+ * system at least one body).  evaluate() then builds one forest -- every
+ * system with its own bounds and tree, exactly as if built alone -- and runs
+ * each phase once over all systems; get_bodies() returns every system's
+ * bodies in its own tree order, systems in input order, and get_perm() the
+ * input record of each.  Exports of trees, lists and expansions, direct(),
+ * ewald() and dipole_correction() address a single system and return
+ * EXAFMM_ERR_STATE for a batch; set_bodies() returns to a single system. */
+EXAFMM_API int exafmm_b200_set_batch(exafmm_b200 *h, const double *bodies8, const int64_t *offsets, int nsys,
+                                     int where);
+
 /* Per-phase device times of the last evaluation in milliseconds, measured
  * with CUDA events on the handle's stream: tree, lists, upward, m2l, p2p,
  * downward, total (7 values). */

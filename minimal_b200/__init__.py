@@ -37,7 +37,7 @@ API = [
     "exafmm_b200_get_perm", "exafmm_b200_num_cells", "exafmm_b200_get_tree", "exafmm_b200_count_lists",
     "exafmm_b200_get_lists", "exafmm_b200_get_expansions", "exafmm_b200_direct", "exafmm_b200_get_timings",
     "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak", "exafmm_b200_direct_static",
-    "exafmm_b200_dipole_correction", "exafmm_b200_ewald",
+    "exafmm_b200_dipole_correction", "exafmm_b200_ewald", "exafmm_b200_set_batch",
 ]
 
 PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
@@ -94,6 +94,7 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_direct_static": (i, [vp, i64, vp, i64, vp]),
         "exafmm_b200_dipole_correction": (i, [vp]),
         "exafmm_b200_ewald": (i, [vp, i, d, d, d, vp, i64, i]),
+        "exafmm_b200_set_batch": (i, [vp, vp, vp, i, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -164,6 +165,27 @@ class FMM:
         """Body records already in device memory (e.g. a torch tensor's data_ptr())."""
         self.n = int(n)
         self._check(self.lib.exafmm_b200_set_bodies(self.h, ctypes.c_void_p(ptr), self.n, DEVICE))
+
+    def set_batch(self, systems):
+        """A batch of independent systems: a list of N_q x 4 (or x 8) arrays.
+        evaluate() runs each phase once over all of them; bodies() returns
+        every system's bodies in its own tree order, one system after the
+        other (split with self.offsets)."""
+        recs = [as_records(x) for x in systems]
+        offsets = np.zeros(len(recs) + 1, dtype=np.int64)
+        offsets[1:] = np.cumsum([len(r) for r in recs])
+        rec = np.ascontiguousarray(np.concatenate(recs))
+        self.n = len(rec)
+        self.offsets = offsets
+        self._check(self.lib.exafmm_b200_set_batch(self.h, _p(rec), _p(offsets), len(recs), HOST))
+
+    def set_batch_device(self, ptr, offsets):
+        """Batch whose Body records are already in device memory; offsets on the host."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        self.n = int(offsets[-1])
+        self.offsets = offsets
+        self._check(self.lib.exafmm_b200_set_batch(self.h, ctypes.c_void_p(ptr), _p(offsets), len(offsets) - 1,
+                                                   DEVICE))
 
     # ---- phases (3d/fmm.cxx:40-53)
     def build_tree(self):

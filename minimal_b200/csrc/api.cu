@@ -100,6 +100,12 @@ void need_tree(Handle &h) {
   if (!h.have_tree) throw Error{EXAFMM_ERR_STATE, "build_tree() has not run on the current bodies"};
 }
 
+// Tree and list exports, direct sums and the periodic tools address one
+// system; a batch only evaluates and returns bodies.
+void need_single(Handle &h, const char *what) {
+  if (h.nsys > 1) throw Error{EXAFMM_ERR_STATE, std::string(what) + " is not available for a batch of systems"};
+}
+
 void do_tree(Handle &h) {
   if (h.n <= 0) throw Error{EXAFMM_ERR_STATE, "no bodies loaded"};
   Timer t(h, PH_TREE);
@@ -242,6 +248,8 @@ int exafmm_b200_set_params(exafmm_b200 *H, const exafmm_params *params) {
   return guarded(H, [&](Handle &h) {
     if (!params) throw Error{EXAFMM_ERR_ARG, "null params"};
     check_params(*params);
+    if (h.nsys > 1 && params->images != 0)
+      throw Error{EXAFMM_ERR_STATE, "batches of systems are free-space only (images = 0)"};
     if (params->device != h.prm.device) throw Error{EXAFMM_ERR_ARG, "a handle stays on its device"};
     h.prm = *params;
     h.nterm = nterm_of(params->P);
@@ -274,6 +282,39 @@ int exafmm_b200_set_bodies(exafmm_b200 *H, const double *rec, int64_t n, int whe
     FMM_CUDA(cudaStreamSynchronize(h.stream));
     if (hb) throw Error{EXAFMM_ERR_ARG, "non-finite body position or charge"};
     h.have_tree = h.have_lists = h.have_up = h.have_horiz = h.have_down = false;
+    h.nsys = 1;
+    h.sys_off_host.clear();
+  });
+}
+
+int exafmm_b200_set_batch(exafmm_b200 *H, const double *rec, const int64_t *offsets, int nsys, int where) {
+  if (!H) return EXAFMM_ERR_ARG;
+  if (!offsets || nsys < 1 || nsys > (1 << 20)) {
+    H->h.err = "need offsets for 1 <= nsys <= 2^20 systems";
+    return EXAFMM_ERR_ARG;
+  }
+  if (offsets[0] != 0) {
+    H->h.err = "offsets[0] must be 0";
+    return EXAFMM_ERR_ARG;
+  }
+  for (int q = 0; q < nsys; q++)
+    if (offsets[q + 1] <= offsets[q]) {
+      H->h.err = "every system needs at least one body (offsets strictly increasing)";
+      return EXAFMM_ERR_ARG;
+    }
+  if (H->h.prm.images != 0) {
+    H->h.err = "batches of systems are free-space only (images = 0)";
+    return EXAFMM_ERR_STATE;
+  }
+  const int rc = exafmm_b200_set_bodies(H, rec, offsets[nsys], where);
+  if (rc != EXAFMM_OK) return rc;
+  return guarded(H, [&](Handle &h) {
+    h.sys_off.need((size_t)(nsys + 1) * sizeof(long long));
+    FMM_CUDA(cudaMemcpyAsync(h.sys_off.p, offsets, (nsys + 1) * sizeof(long long), cudaMemcpyHostToDevice,
+                             h.stream));
+    h.sys_off_host.assign(offsets, offsets + nsys + 1);
+    h.nsys = nsys;
+    h.key_levels = 0;
   });
 }
 
@@ -338,6 +379,7 @@ int64_t exafmm_b200_num_cells(exafmm_b200 *H) { return H && H->h.have_tree ? H->
 int exafmm_b200_get_tree(exafmm_b200 *H, int *nchild, int *child, int *body, int *nbody, int *level, double *xr) {
   return guarded(H, [&](Handle &h) {
     need_tree(h);
+    need_single(h, "get_tree()");
     const int C = h.ncells;
     std::vector<int> nc(C), ch(C), bg(C), ct(C), lv(C), rf(C);
     std::vector<double4> x(C);
@@ -372,6 +414,7 @@ int exafmm_b200_count_lists(exafmm_b200 *H, int64_t *a, int64_t *b) {
 int exafmm_b200_get_lists(exafmm_b200 *H, int *mo, int *ms, int *mi, int *po, int *ps, int *pi) {
   return guarded(H, [&](Handle &h) {
     if (!h.have_lists) throw Error{EXAFMM_ERR_STATE, "lists not built"};
+    need_single(h, "get_lists()");
     if (!mo || !ms || !mi || !po || !ps || !pi) throw Error{EXAFMM_ERR_ARG, "null output"};
     export_lists(h, mo, ms, mi, po, ps, pi);
   });
@@ -380,6 +423,7 @@ int exafmm_b200_get_lists(exafmm_b200 *H, int *mo, int *ms, int *mi, int *po, in
 int exafmm_b200_get_expansions(exafmm_b200 *H, double *M, double *L) {
   return guarded(H, [&](Handle &h) {
     if (!h.have_up) throw Error{EXAFMM_ERR_STATE, "upward() has not run"};
+    need_single(h, "get_expansions()");
     const int C = h.ncells, nt = h.nterm;
     std::vector<int> rf(C);
     std::vector<double2> m((size_t)C * nt), l((size_t)C * nt);
@@ -398,6 +442,7 @@ int exafmm_b200_get_expansions(exafmm_b200 *H, double *M, double *L) {
 int exafmm_b200_direct(exafmm_b200 *H, double *targets, int64_t nt, int where) {
   return guarded(H, [&](Handle &h) {
     need_tree(h);
+    need_single(h, "direct()");
     if (!targets || nt <= 0) throw Error{EXAFMM_ERR_ARG, "need targets"};
     Buf rec, xq, pf;
     rec.need(nt * 64);
@@ -421,6 +466,7 @@ int exafmm_b200_direct(exafmm_b200 *H, double *targets, int64_t nt, int where) {
 
 int exafmm_b200_dipole_correction(exafmm_b200 *H) {
   return guarded(H, [&](Handle &h) {
+    need_single(h, "dipole_correction()");
     if (!h.have_down) throw Error{EXAFMM_ERR_STATE, "dipole_correction() needs the results of evaluate()"};
     if (h.prm.images <= 0) throw Error{EXAFMM_ERR_STATE, "dipole_correction() is for periodic systems (images > 0)"};
     dipole_correction(h);
@@ -431,6 +477,7 @@ int exafmm_b200_ewald(exafmm_b200 *H, int ksize, double alpha, double sigma, dou
                       int64_t nt, int where) {
   return guarded(H, [&](Handle &h) {
     need_tree(h);
+    need_single(h, "ewald()");
     if (!targets || nt <= 0) throw Error{EXAFMM_ERR_ARG, "need targets"};
     if (ksize < 1 || ksize > 64 || !(alpha > 0) || !(sigma > 0) || !(cutoff > 0))
       throw Error{EXAFMM_ERR_ARG, "ewald: ksize in [1, 64] and positive alpha, sigma, cutoff required"};

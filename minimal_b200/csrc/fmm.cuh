@@ -91,8 +91,12 @@ struct Handle {
   cudaStream_t stream = nullptr;
   int64_t launches = 0;
 
-  // bodies
+  // bodies; a batch holds nsys independent systems, system q owning input
+  // bodies [sys_off[q], sys_off[q+1])
   int64_t n = 0;
+  int nsys = 1;
+  Buf sys_off;                        // long long [nsys + 1] (device)
+  std::vector<int64_t> sys_off_host;
   Buf in;      // double4 (x,y,z,q), caller order
   Buf src;     // double4 (x,y,z,q), tree order
   Buf out;     // double4 (p,Fx,Fy,Fz), tree order

@@ -122,10 +122,13 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
   }
 }
 
-__global__ void k_seed(int2 *f, unsigned long long *n, int images) {
-  const int t = threadIdx.x;
+// Root pairs of the walk: (root, root) of every system of a batch (the roots
+// are the first nsys cells), or the 27 image pairs of a periodic system.
+__global__ void k_seed(int2 *f, unsigned long long *n, int images, int nsys) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (images == 0) {
-    if (t == 0) { f[0] = make_int2(0 | (13 << IMG_SHIFT), 0); *n = 1; }
+    if (t < nsys) f[t] = make_int2(t | (13 << IMG_SHIFT), t);
+    if (t == 0) *n = (unsigned long long)nsys;
   } else if (t < 27) {
     // image loop order of the reference: x outermost, z innermost; img is
     // periodic1D = (x+1) + 3(y+1) + 9(z+1)
@@ -234,7 +237,8 @@ void build_lists(Handle &h) {
     h.p2p_raw.need(h.p2p_cap * sizeof(int2));
     FMM_CUDA(cudaMemsetAsync(&ctr->n_m2l, 0, sizeof(unsigned long long) * 4, s));
     FMM_CUDA(cudaMemsetAsync(&ctr->list_overflow, 0, sizeof(int), s));
-    k_seed<<<1, 32, 0, s>>>(h.frontier[0].as<int2>(), &ctr->frontier[0], images);
+    k_seed<<<grid_for(std::max(h.nsys, 32), 256), 256, 0, s>>>(h.frontier[0].as<int2>(), &ctr->frontier[0], images,
+                                                                h.nsys);
     h.launches++;
     CellView cv{h.c_xr.as<double4>(), h.c_child.as<int>(), h.c_nchild.as<int>()};
     const int steps = 2 * h.depth + 3;

@@ -24,6 +24,12 @@
 //      stable partition never reorders bodies of one leaf).
 // The key holds 3 bits per level for the first `key_levels` levels; if a cell
 // at that depth still needs splitting the build is repeated with all 21.
+//
+// Batches of independent systems build one forest: every system gets its own
+// bounds and root geometry, the system index sits above the octant digits in
+// the sort key (so it is the level-0 prefix), each system's root always exists,
+// and nothing else changes -- every system's cells and body order come out as
+// if it were built alone, one after the other.
 #include <cmath>
 
 #include "fmm.cuh"
@@ -83,14 +89,54 @@ __global__ void k_bounds_final(const double *part, int nb, RootGeom *g) {
   g->R0 = __dmul_rn(R0, 1.00001);
 }
 
-// Octant digits of each body, level by level, against the exact centres.
-__global__ void k_keys(const double4 *in, long n, const RootGeom *g, int D, u64 *keys, u32 *vals) {
+// Bounds of every system of a batch: one block per system, then the same
+// getBounds arithmetic as k_bounds_final.
+__global__ void k_bounds_systems(const double4 *in, const long long *off, RootGeom *geom) {
+  __shared__ double s[TB][6];
+  const long b0 = off[blockIdx.x], b1 = off[blockIdx.x + 1];
+  double lo[3] = {in[b0].x, in[b0].y, in[b0].z}, hi[3] = {lo[0], lo[1], lo[2]};
+  for (long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const double4 b = in[i];
+    lo[0] = dmin(b.x, lo[0]); lo[1] = dmin(b.y, lo[1]); lo[2] = dmin(b.z, lo[2]);
+    hi[0] = dmax(b.x, hi[0]); hi[1] = dmax(b.y, hi[1]); hi[2] = dmax(b.z, hi[2]);
+  }
+  for (int d = 0; d < 3; d++) { s[threadIdx.x][d] = lo[d]; s[threadIdx.x][3 + d] = hi[d]; }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  for (int k = 1; k < blockDim.x; k++)
+    for (int d = 0; d < 3; d++) { lo[d] = dmin(s[k][d], lo[d]); hi[d] = dmax(s[k][3 + d], hi[d]); }
+  RootGeom *g = geom + blockIdx.x;
+  double R0 = 0;
+  for (int d = 0; d < 3; d++) {
+    g->X0[d] = __ddiv_rn(__dadd_rn(hi[d], lo[d]), 2.0);
+    R0 = dmax(__dadd_rn(g->X0[d], -lo[d]), R0);
+    R0 = dmax(__dadd_rn(hi[d], -g->X0[d]), R0);
+  }
+  g->R0 = __dmul_rn(R0, 1.00001);
+}
+
+// System of body i: the last s with off[s] <= i (off: nsys+1 offsets).
+__device__ __forceinline__ int system_of(const long long *off, int nsys, long i) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Octant digits of each body, level by level, against the exact centres of
+// its system's cells; the system index above them.
+__global__ void k_keys(const double4 *in, long n, const RootGeom *geom, const long long *sys_off, int nsys, int D,
+                       u64 *keys, u32 *vals) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 b = in[i];
+  const int sys = nsys > 1 ? system_of(sys_off, nsys, i) : 0;
+  const RootGeom *g = geom + sys;
   double cx = g->X0[0], cy = g->X0[1], cz = g->X0[2];
   const double R0 = g->R0;
-  u64 key = 0;
+  u64 key = (u64)sys;
   for (int l = 0; l < D; l++) {
     const int ox = b.x > cx, oy = b.y > cy, oz = b.z > cz;
     key = (key << 3) | (u64)(ox | (oy << 1) | (oz << 2));
@@ -103,7 +149,8 @@ __global__ void k_keys(const double4 *in, long n, const RootGeom *g, int D, u64 
   vals[i] = (u32)i;
 }
 
-__device__ __forceinline__ u64 prefix_of(u64 key, int D, int l) { return l == 0 ? 0ull : key >> (3 * (D - l)); }
+// Level-l prefix of a key: the system index and the first l octant digits.
+__device__ __forceinline__ u64 prefix_of(u64 key, int D, int l) { return key >> (3 * (D - l)); }
 
 // First index in [lo, hi) whose level-l prefix exceeds p (keys sorted).
 __device__ long upper_run(const u64 *keys, long lo, long hi, int D, int l, u64 p) {
@@ -128,7 +175,8 @@ __device__ __forceinline__ int first_level(const u64 *keys, long i, int D) {
   const u64 x = keys[i] ^ keys[i - 1];
   if (x == 0) return D + 1;
   const int h = 63 - __clzll((long long)x);
-  return D - 1 - h / 3 + 1;
+  if (h >= 3 * D) return 0;  // another system: its root starts here
+  return D - h / 3;
 }
 
 // Number of cells whose first body is sorted position i (a chain of nested
@@ -143,8 +191,8 @@ __global__ void k_chain(const u64 *keys, long n, int D, int ncrit, int *lfirst, 
     const u64 key = keys[i];
     long end;
     bool parent_splits = true;
-    if (lf == 0) {
-      end = n;
+    if (lf == 0) {  // a system's root: always a cell
+      end = upper_run(keys, i, n, D, 0, prefix_of(key, D, 0));
     } else {
       const u64 pp = prefix_of(key, D, lf - 1);
       const long b0 = lower_run(keys, 0, i, D, lf - 1, pp);
@@ -154,7 +202,7 @@ __global__ void k_chain(const u64 *keys, long n, int D, int ncrit, int *lfirst, 
     }
     if (parent_splits) {
       for (int l = lf; l <= D; l++) {
-        const long e = l == 0 ? n : upper_run(keys, i, end, D, l, prefix_of(key, D, l));
+        const long e = upper_run(keys, i, end, D, l, prefix_of(key, D, l));
         len++;
         if (e - i <= ncrit) break;
         if (l == D) { ctr->overflow = 1; break; }
@@ -179,8 +227,9 @@ __global__ void k_cells(const u64 *keys, long n, int D, int ncrit, const int *lf
   if (len == 0) return;
   const int lf = lfirst[i];
   const u64 key = keys[i];
-  const double R0 = g->R0;
-  double cx = g->X0[0], cy = g->X0[1], cz = g->X0[2];
+  const RootGeom *gs = g + (long)(key >> (3 * D));  // the body's system
+  const double R0 = gs->R0;
+  double cx = gs->X0[0], cy = gs->X0[1], cz = gs->X0[2];
   for (int l = 0; l < lf; l++) {  // centre of the level-lf cell holding body i
     const int o = (int)((key >> (3 * (D - 1 - l))) & 7);
     const double r = __ddiv_rn(R0, (double)(1 << (l + 1)));
@@ -190,7 +239,7 @@ __global__ void k_cells(const u64 *keys, long n, int D, int ncrit, const int *lf
   }
   const int p0 = prebase[i];
   int parent = -1;
-  long end = n;
+  long end = upper_run(keys, i, n, D, 0, prefix_of(key, D, 0));  // the system's bodies
   if (lf > 0) {
     const u64 pp = prefix_of(key, D, lf - 1);
     const long b0 = lower_run(keys, 0, i, D, lf - 1, pp);
@@ -199,7 +248,7 @@ __global__ void k_cells(const u64 *keys, long n, int D, int ncrit, const int *lf
   }
   for (int k = 0; k < len; k++) {
     const int l = lf + k, p = p0 + k;
-    const long e = l == 0 ? n : upper_run(keys, i, end, D, l, prefix_of(key, D, l));
+    const long e = upper_run(keys, i, end, D, l, prefix_of(key, D, l));
     t.begin[p] = (int)i;
     t.count[p] = (int)(e - i);
     t.level[p] = l;
@@ -297,33 +346,50 @@ __global__ void k_zero_counters(DevCounters *c) {
 void build_tree(Handle &h) {
   const long n = h.n;
   cudaStream_t s = h.stream;
-  h.geom.need(sizeof(RootGeom));
+  const int nsys = h.nsys;
+  h.geom.need((size_t)nsys * sizeof(RootGeom));
   h.counters.need(sizeof(DevCounters));
   DevCounters *ctr = h.counters.as<DevCounters>();
   RootGeom *g = h.geom.as<RootGeom>();
+  const long long *sys_off = nsys > 1 ? h.sys_off.as<long long>() : nullptr;
 
   // 1. bounds
-  const int nbp = (int)std::min<long>(4 * 148, (n + TB - 1) / TB);
-  h.hist.need((size_t)nbp * 6 * sizeof(double));
-  k_bounds_partial<<<nbp, TB, 0, s>>>(h.in.as<double4>(), n, h.hist.as<double>());
-  k_bounds_final<<<1, TB, 0, s>>>(h.hist.as<double>(), nbp, g);
-  h.launches += 2;
+  if (nsys > 1) {
+    k_bounds_systems<<<nsys, TB, 0, s>>>(h.in.as<double4>(), sys_off, g);
+    h.launches++;
+  } else {
+    const int nbp = (int)std::min<long>(4 * 148, (n + TB - 1) / TB);
+    h.hist.need((size_t)nbp * 6 * sizeof(double));
+    k_bounds_partial<<<nbp, TB, 0, s>>>(h.in.as<double4>(), n, h.hist.as<double>());
+    k_bounds_final<<<1, TB, 0, s>>>(h.hist.as<double>(), nbp, g);
+    h.launches += 2;
+  }
   FMM_LAUNCH();
 
+  // the system index takes the key bits above the octant digits
+  int sys_bits = 0;
+  while ((1ll << sys_bits) < nsys) sys_bits++;
+  const int max_levels = std::min(EXAFMM_MAX_LEVEL, (64 - sys_bits) / 3);
   int D = h.key_levels;
   if (D <= 0) {
-    double ratio = (double)n / (double)(h.prm.ncrit > 0 ? h.prm.ncrit : 1);
+    long nmax = n;
+    if (nsys > 1) {
+      nmax = 0;
+      for (int q = 0; q < nsys; q++) nmax = std::max<long>(nmax, (long)(h.sys_off_host[q + 1] - h.sys_off_host[q]));
+    }
+    double ratio = (double)nmax / (double)(h.prm.ncrit > 0 ? h.prm.ncrit : 1);
     D = (int)std::ceil(std::log(std::max(ratio, 1.0)) / std::log(8.0)) + 3;
-    D = std::min(std::max(D, 2), EXAFMM_MAX_LEVEL);
+    D = std::min(std::max(D, 2), max_levels);
   }
+  D = std::min(D, max_levels);
   for (h.keys[0].need(n * 8), h.keys[1].need(n * 8), h.vals[0].need(n * 4), h.vals[1].need(n * 4);;) {
     k_zero_counters<<<1, 256, 0, s>>>(ctr);
     u64 *k = h.keys[0].as<u64>(), *k2 = h.keys[1].as<u64>();
     u32 *v = h.vals[0].as<u32>(), *v2 = h.vals[1].as<u32>();
-    k_keys<<<grid_for(n, TB), TB, 0, s>>>(h.in.as<double4>(), n, g, D, k, v);
+    k_keys<<<grid_for(n, TB), TB, 0, s>>>(h.in.as<double4>(), n, g, sys_off, nsys, D, k, v);
     h.launches += 2;
     FMM_LAUNCH();
-    radix_sort_pairs(h, k, v, k2, v2, n, 0, 3 * D);
+    radix_sort_pairs(h, k, v, k2, v2, n, 0, 3 * D + sys_bits);
     h.lfirst.need(n * 4);
     h.chain.need(n * 4);
     h.prebase.need((n + 1) * 4);
@@ -334,10 +400,10 @@ void build_tree(Handle &h) {
     FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
     FMM_CUDA(cudaStreamSynchronize(s));
     if (h.hc.overflow) {
-      if (D == EXAFMM_MAX_LEVEL)
+      if (D == max_levels)
         throw Error{EXAFMM_ERR_DEPTH, "more than ncrit bodies share a cell at the deepest level (" +
-                                          std::to_string(EXAFMM_MAX_LEVEL) + "): coincident bodies?"};
-      D = EXAFMM_MAX_LEVEL;
+                                          std::to_string(max_levels) + "): coincident bodies?"};
+      D = max_levels;
       continue;
     }
     const long C = h.hc.ncells;
