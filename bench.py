@@ -1,27 +1,33 @@
 """Benchmark: FMM evaluations per second on one B200 (or N replicas).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 1048576] [--P 10] [--precision fp64|mixed]
+                    [--n 1048576] [--P 10] [--precision mixed|fp64] [--quick]
 
-Workload (default): 3D free-space Laplace FMM, N = 1,048,576 bodies uniform
-in [-pi, pi]^3 with charges uniform in [-0.5, 0.5] (neutralised), generated
+Headline workload: 3D free-space Laplace FMM, N = 1,048,576 bodies uniform in
+[-pi, pi]^3 with charges uniform in [-0.5, 0.5] (neutralised), generated
 exactly like the reference driver (srand48(0)/drand48), P = 10, theta = 0.4,
-ncrit = 64.  One step is one complete evaluation -- tree build, interaction
-lists, upward pass, M2L + P2P, downward pass -- from the unsorted bodies
-already resident in HBM.  Between timed steps the L2 is flushed by writing a
-256 MB buffer (outside the timed events).
+ncrit = 64, in the mixed-precision form (FP32 near field with compensated
+sums, tensor-core M2L).  One step is one complete evaluation -- tree build,
+interaction lists, upward pass, M2L + P2P, downward pass -- from the unsorted
+bodies already resident in HBM.  Between timed steps the L2 is flushed by
+writing a 256 MB buffer (outside the timed events).
 
-Printed: one JSON line (rank 0) with the driver's keys plus the e2e number
-(Body records in pinned host memory -> set_bodies -> evaluate -> get_bodies
-back to host, per step), the roofline of the dominant kernel, the reference's
-own CPU build timed on this host's cores, per-phase times and the error of
-the result against FP64 direct summation on 1000 sampled bodies.
+Printed: one JSON line (rank 0) with the driver's keys; the e2e number (Body
+records in pinned host memory -> set_bodies -> evaluate -> get_bodies back to
+host, per step); the roofline of the dominant kernel (the FP32 near field)
+and of the tensor-core M2L; the reference's own CPU build timed on this
+host's cores; per-phase times; the error against FP64 direct summation on
+1000 sampled bodies; and, beside the headline, the same workload in the FP64
+form (the ratio the metric names), the P = 12 point (where 1e-5 force error
+is reachable), the batched form (2048 uneven systems, batched vs one system
+at a time) and the periodic form (1M bodies, 3 image layers, checked against
+the GPU Ewald sum).  --quick skips the P = 12, batched and periodic legs.
 
 --impl reference times the reference itself (its own headers compiled by
 oracle/Makefile into oracle/_ref, lazy traversal, OpenMP on all host cores)
 on the same workload and prints the same line with "impl": "reference".
 
-Multi-GPU: the evaluation does not shard across GPUs in this build; with
+Multi-GPU: one evaluation does not shard across GPUs in this build; with
 --gpus N (under torchrun) every rank evaluates its own independent system of
 the same size ("replicas"), so value = N / max-over-ranks time per step.
 """
@@ -44,14 +50,15 @@ METRIC = "FMM evals/s at 1M bodies P=10: mixed vs FP64 GPU at ≤1e-5 rel. force
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--P", type=int, default=10)
     ap.add_argument("--theta", type=float, default=0.4)
     ap.add_argument("--ncrit", type=int, default=64)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--quick", action="store_true", help="headline and FP64 legs only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=40.0, help="seconds of reference CPU work at most")
     return ap.parse_args()
@@ -179,6 +186,146 @@ def run_reference(a, rank, world):
 
 
 # ---------------------------------------------------------------- our arm
+def timed_steps(fmm, steps, flush, torch):
+    """Per-phase device times (library CUDA events) of `steps` evaluations,
+    each after an L2 flush; returns (phase lists, kernel launches)."""
+    import minimal_b200
+
+    phase = {k: [] for k in minimal_b200.PHASES}
+    launches = 0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        fmm.evaluate()
+        launches += fmm.last_launches()
+        for k, v in fmm.timings().items():
+            phase[k].append(v)
+    return phase, launches
+
+
+def errors_vs_direct(fmm, n, out=None):
+    """Relative L2 error of p and F on 1000 stride-sampled tree positions
+    against FP64 direct summation on the GPU."""
+    out = fmm.bodies() if out is None else out
+    sample = np.arange(0, n, max(1, n // 1000))[:1000]
+    tgt = out[sample].copy()
+    res = tgt.copy()
+    tgt[:, 4:] = 0
+    d = fmm.direct(tgt)
+    ep = float(np.sqrt(((res[:, 4] - d[:, 4]) ** 2).sum() / (d[:, 4] ** 2).sum()))
+    ef = float(np.sqrt(((res[:, 5:] - d[:, 5:]) ** 2).sum() / (d[:, 5:] ** 2).sum()))
+    return {"p": ep, "F": ef, "targets": len(sample)}
+
+
+def form_leg(FMM, d_rec, n, P, a, precision, flush, torch, local_rank, steps=3, warmup=2):
+    fmm = FMM(P=P, ncrit=a.ncrit, theta=a.theta, precision=precision, device=local_rank)
+    fmm.set_bodies_device(d_rec.data_ptr(), n)
+    for _ in range(warmup):
+        fmm.evaluate()
+    phase, _ = timed_steps(fmm, steps, flush, torch)
+    ms = statistics.mean(phase["total"])
+    err = errors_vs_direct(fmm, n)
+    fmm.close()
+    return {"evals_per_s": 1e3 / ms, "ms_per_eval": ms, "error_vs_direct": err,
+            "phases_ms": {k: statistics.mean(v) for k, v in phase.items()}}
+
+
+def batched_leg(FMM, torch, dev, local_rank, nsys=2048):
+    """Batched configuration: 2048 independent systems, sizes log-uniform in
+    [1000, 65536] (seeded), each uniform in [-pi, pi]^3, P=6, theta=0.5,
+    mixed; one batched evaluation vs the same systems one at a time."""
+    from minimal_b200.bodies import uniform_bodies
+
+    rng = np.random.default_rng(2048)
+    sizes = np.exp(rng.uniform(np.log(1000), np.log(65536), nsys)).astype(np.int64)
+    offs = np.zeros(nsys + 1, np.int64)
+    offs[1:] = np.cumsum(sizes)
+    N = int(offs[-1])
+    rec = np.zeros((N, 8))
+    for q in range(nsys):
+        rec[offs[q]:offs[q + 1], :4] = uniform_bodies(int(sizes[q]), q)
+    d = torch.from_numpy(rec).to(dev)
+    f = FMM(P=6, ncrit=64, theta=0.5, precision="mixed", device=local_rank)
+    f.set_batch_device(d.data_ptr(), offs)
+    f.evaluate()
+    tb = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        f.set_batch_device(d.data_ptr(), offs)
+        f.evaluate()
+        torch.cuda.synchronize()
+        tb.append(time.perf_counter() - t)
+    phases = f.timings()
+    # spot check: one system of the batch against its own evaluation
+    out = f.bodies()
+    q = int(np.argmax(sizes))
+    f.close()
+    g = FMM(P=6, ncrit=64, theta=0.5, precision="mixed", device=local_rank)
+    g.set_bodies_device(d[offs[q]:].data_ptr(), int(sizes[q]))
+    g.evaluate()
+    alone = g.bodies()
+    mine = out[offs[q]:offs[q + 1]]
+    same_order = bool(np.array_equal(mine[:, :4], alone[:, :4]))
+    dev_f = float(np.sqrt(((mine[:, 5:] - alone[:, 5:]) ** 2).sum() / (alone[:, 5:] ** 2).sum()))
+    for k in range(8):  # warm the one-at-a-time path
+        g.set_bodies_device(d[offs[k]:].data_ptr(), int(sizes[k]))
+        g.evaluate()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for k in range(nsys):
+        g.set_bodies_device(d[offs[k]:].data_ptr(), int(sizes[k]))
+        g.evaluate()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter() - t
+    g.close()
+    t_b = min(tb)
+    return {"workload": f"{nsys} systems, sizes log-uniform in [1000, 65536] (seeded), {N} bodies, "
+                        "uniform in [-pi,pi]^3, P=6, theta=0.5, ncrit=64, mixed",
+            "bodies": N, "batched_ms": t_b * 1e3, "batched_bodies_per_s": N / t_b,
+            "one_at_a_time_ms": t1 * 1e3, "one_at_a_time_bodies_per_s": N / t1, "speedup": t1 / t_b,
+            "batched_phases_ms": phases,
+            "check_largest_system": {"same_tree_order": same_order, "rel_force_diff_vs_alone": dev_f}}
+
+
+def periodic_leg(FMM, torch, dev, local_rank, n):
+    """Periodic configuration: N bodies uniform in a cube of side 2 pi
+    (neutralised), P=10, theta=0.4, ncrit=64, 3 image layers, mixed form
+    (root images in FP64); after the dipole correction, checked against the
+    GPU FP64 Ewald sum (ksize=11, alpha=ksize/cycle, cutoff=cycle/2) on 1000
+    sampled bodies, by the reference's measures (energy sum, force L2)."""
+    from minimal_b200 import drand48_bodies
+
+    cyc = 2 * np.pi
+    xq = drand48_bodies(n, 0, "3dp", cyc)
+    rec = np.zeros((n, 8))
+    rec[:, :4] = xq
+    d = torch.from_numpy(rec).to(dev)
+    res = {}
+    for prec in ("mixed", "fp64"):
+        f = FMM(P=10, ncrit=64, theta=0.4, images=3, cycle=cyc, precision=prec, device=local_rank)
+        f.set_bodies_device(d.data_ptr(), n)
+        f.evaluate()
+        ts = []
+        for _ in range(3):
+            f.evaluate()
+            ts.append(f.timings()["total"])
+        f.dipole_correction()
+        out = f.bodies()
+        sample = np.arange(0, n, max(1, n // 1000))[:1000]
+        tgt = out[sample].copy()
+        tgt[:, 4:] = 0
+        ew = f.ewald(tgt, ksize=11)
+        o = out[sample]
+        ep = abs((o[:, 4] * o[:, 3]).sum() - (ew[:, 4] * ew[:, 3]).sum()) / abs((ew[:, 4] * ew[:, 3]).sum())
+        ef = float(np.sqrt(((o[:, 5:] - ew[:, 5:]) ** 2).sum() / (ew[:, 5:] ** 2).sum()))
+        res[prec] = {"ms_per_eval": statistics.mean(ts), "evals_per_s": 1e3 / statistics.mean(ts),
+                     "energy_rel_err_vs_ewald": float(ep), "force_rel_l2_vs_ewald": ef}
+        f.close()
+    res["workload"] = f"{n} bodies uniform in a cube of side 2 pi, P=10, theta=0.4, ncrit=64, images=3"
+    return res
+
+
 def run_ours(a, rank, world, local_rank):
     import torch
 
@@ -191,7 +338,7 @@ def run_ours(a, rank, world, local_rank):
 
         import torch.distributed as td
 
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
 
@@ -218,8 +365,6 @@ def run_ours(a, rank, world, local_rank):
         fmm.evaluate()
 
     clocks = Clocks(local_rank)
-    phase = {k: [] for k in minimal_b200.PHASES}
-    launches = 0
     torch.cuda.synchronize()
     if dist:
         import torch.distributed as td
@@ -227,13 +372,7 @@ def run_ours(a, rank, world, local_rank):
         td.barrier()
     clocks.start()
     t0 = time.perf_counter()
-    for _ in range(a.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        fmm.evaluate()
-        launches += fmm.last_launches()
-        for k, v in fmm.timings().items():
-            phase[k].append(v)
+    phase, launches = timed_steps(fmm, a.steps, flush, torch)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     if dist:
@@ -262,42 +401,65 @@ def run_ours(a, rank, world, local_rank):
     if rank != 0:
         fmm.close()
         if dist:
+            td.barrier()
             td.destroy_process_group()
         return
 
-    # accuracy on 1000 sampled tree positions vs FP64 direct summation
-    out = h_out.numpy().copy()
-    sample = np.arange(0, a.n, max(1, a.n // 1000))[:1000]
-    tgt = out[sample].copy()
-    res = tgt.copy()
-    tgt[:, 4:] = 0
-    d = fmm.direct(tgt)
-    err_p = float(np.sqrt(((res[:, 4] - d[:, 4]) ** 2).sum() / (d[:, 4] ** 2).sum()))
-    err_f = float(np.sqrt(((res[:, 5:] - d[:, 5:]) ** 2).sum() / (d[:, 5:] ** 2).sum()))
+    err = errors_vs_direct(fmm, a.n, h_out.numpy().copy())
 
-    # roofline of the dominant kernel (one launch per phase for m2l and p2p)
+    # roofline: the near field (FP32 pipe in the mixed form, FP64 in the
+    # plain form) dominates; the tensor-core M2L is reported beside it
     pairs, n_m2l = pair_count(fmm)
-    peak64 = fmm.fma_peak("fp64")
+    mixed = a.precision == "mixed"
+    peak_fma = fmm.fma_peak("mixed" if mixed else "fp64")
     m2l_ms = statistics.mean(phase["m2l"])
     p2p_ms = statistics.mean(phase["p2p"])
-    m2l_tf = n_m2l * m2l_flops_per_pair(a.P) / (m2l_ms * 1e-3) / 1e12
-    p2p_tf = pairs * 20 / (p2p_ms * 1e-3) / 1e12
-    if m2l_ms >= p2p_ms:
-        dom = {"kernel": "k_m2l (M2L, FP64)", "achieved": m2l_tf, "flops_per_launch": n_m2l * m2l_flops_per_pair(a.P)}
-    else:
-        dom = {"kernel": "k_p2p (P2P, FP64)", "achieved": p2p_tf, "flops_per_launch": pairs * 20}
-    traffic = None
+    p2p_flops = pairs * 20
+    m2l_flops = n_m2l * m2l_flops_per_pair(a.P)
+    p2p_tf = p2p_flops / (p2p_ms * 1e-3) / 1e12
+    m2l_tf = m2l_flops / (m2l_ms * 1e-3) / 1e12
+    peaks = {}
+    ppath = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(ppath):
+        peaks = json.load(open(ppath))
+    traffic = {}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(dom["kernel"].split()[0])
-    roof = {"bound": "fp64", "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": peak64,
-            "unit": "TFLOP/s", "frac": dom["achieved"] / peak64, "traffic": traffic,
-            "peak_source": "measured FP64 FMA-pipe microbenchmark on this GPU (exafmm_b200_fma_peak)",
-            "flops_per_launch": dom["flops_per_launch"],
-            "other": {"k_m2l_tflops": m2l_tf, "k_p2p_tflops": p2p_tf}}
+        traffic = json.load(open(tpath))
+    kern = "k_p2p_cta<1>" if mixed else "k_p2p_cta<0>"
+    roof = {"bound": "fp32" if mixed else "fp64", "kernel": kern + " (P2P near field)", "achieved": p2p_tf,
+            "peak": peak_fma, "unit": "TFLOP/s", "frac": p2p_tf / peak_fma,
+            "traffic": traffic.get(kern, {}).get("bytes_per_launch_1M"),
+            "peak_source": ("measured FP32" if mixed else "measured FP64") +
+                           " FMA-pipe peak on this GPU (dependent-chain microbenchmark, exafmm_b200_fma_peak); "
+                           "the pool's MEASURED_PEAKS.json has no FP32/FP64 figure",
+            "flops_per_launch": p2p_flops, "flops_per_unit": "20 per body pair (3d/kernel.h:133-142)",
+            "time": "P2P phase events (source conversion + near-field kernel)"}
+    roof_m2l = None
+    if mixed and peaks.get("bf16_tflops"):
+        roof_m2l = {"bound": "tensor", "kernel": "k_m2l_tc (grouped M2L, tcgen05 split-FP16) + grouping",
+                    "achieved": m2l_tf, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                    "frac": m2l_tf / peaks["bf16_tflops"], "peak_source": "MEASURED_PEAKS.json bf16 burst",
+                    "flops_per_launch": m2l_flops,
+                    "flops_per_unit": f"{m2l_flops_per_pair(a.P)} per M2L pair (dense realified, truncated)",
+                    "time": "M2L phase events (grouping kernels + contraction + residual)",
+                    "traffic": traffic.get("k_m2l_tc", {}).get("bytes_per_launch_1M")}
+
+    extra = {}
+    other = "fp64" if mixed else "mixed"
+    extra[f"{other}_same_workload"] = form_leg(FMM, d_rec, a.n, a.P, a, other, flush, torch, local_rank)
+    if mixed:
+        extra["mixed_over_fp64_speedup"] = extra["fp64_same_workload"]["ms_per_eval"] / ms_dev
+    if not a.quick and world == 1:  # the side legs run at N = 1 only
+        extra["p12"] = {prec: form_leg(FMM, d_rec, a.n, 12, a, prec, flush, torch, local_rank)
+                        for prec in ("mixed", "fp64")}
+        extra["p12"]["mixed_over_fp64_speedup"] = (extra["p12"]["fp64"]["ms_per_eval"] /
+                                                   extra["p12"]["mixed"]["ms_per_eval"])
+        extra["batched"] = batched_leg(FMM, torch, dev, local_rank)
+        extra["periodic"] = periodic_leg(FMM, torch, dev, local_rank, a.n)
 
     cpu = None
-    if not a.no_cpu_baseline:
+    if not a.no_cpu_baseline and world == 1:
         try:
             cpu = cpu_baseline(xq, a)
         except Exception as e:  # the reference build missing is reported, not hidden
@@ -305,20 +467,21 @@ def run_ours(a, rank, world, local_rank):
 
     line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "mixed",
+            "vs_baseline": None, "dtype": "f32+f16x3 tensor (mixed), f64 root/coefficients" if mixed else "f64",
             "data": "synthetic (drand48, the reference driver's generator; seed = rank)",
             "config": dict(workload(a), parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                            precision=a.precision),
             "e2e": {"value": world * 1e3 / e2e_ms, "unit": "evals/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": a.n * 64, "d2h_bytes_per_step": a.n * 64},
-            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-            "phases_ms": {k: statistics.mean(v) for k, v in phase.items()},
-            "wall_ms_per_step": wall * 1e3 / a.steps,
-            "error_vs_direct": {"p": err_p, "F": err_f, "targets": len(sample)},
+            "gpu_launches": launches, "roofline": roof, "roofline_m2l": roof_m2l, "cpu_baseline": cpu,
+            "clocks": clk, "phases_ms": {k: statistics.mean(v) for k, v in phase.items()},
+            "wall_ms_per_step": wall * 1e3 / a.steps, "error_vs_direct": err,
             "work": {"cells": fmm.num_cells(), "m2l_pairs": n_m2l, "p2p_body_pairs": pairs}}
+    line.update(extra)
     print(json.dumps(line), flush=True)
     fmm.close()
     if dist:
+        td.barrier()
         td.destroy_process_group()
 
 
