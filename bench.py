@@ -1,7 +1,7 @@
 """Benchmark: FMM evaluations per second on one B200 (or N replicas).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 1048576] [--P 10] [--precision mixed|fp64] [--quick]
+                    [--n 1048576] [--P 10] [--precision mixed|fp64] [--legs all|fp64|none]
 
 Headline workload: 3D free-space Laplace FMM, N = 1,048,576 bodies uniform in
 [-pi, pi]^3 with charges uniform in [-0.5, 0.5] (neutralised), generated
@@ -21,7 +21,8 @@ host's cores; per-phase times; the error against FP64 direct summation on
 form (the ratio the metric names), the P = 12 point (where 1e-5 force error
 is reachable), the batched form (2048 uneven systems, batched vs one system
 at a time) and the periodic form (1M bodies, 3 image layers, checked against
-the GPU Ewald sum).  --quick skips the P = 12, batched and periodic legs.
+the GPU Ewald sum).  --legs fp64 keeps only the FP64 leg, --legs none only
+the headline (for profiling).
 
 --impl reference times the reference itself (its own headers compiled by
 oracle/Makefile into oracle/_ref, lazy traversal, OpenMP on all host cores)
@@ -58,7 +59,8 @@ def parse():
     ap.add_argument("--theta", type=float, default=0.4)
     ap.add_argument("--ncrit", type=int, default=64)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--quick", action="store_true", help="headline and FP64 legs only")
+    ap.add_argument("--legs", default="all", choices=["all", "fp64", "none"],
+                    help="side legs: all (FP64, P=12, batched, periodic), fp64 only, or none (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=40.0, help="seconds of reference CPU work at most")
     return ap.parse_args()
@@ -447,10 +449,11 @@ def run_ours(a, rank, world, local_rank):
 
     extra = {}
     other = "fp64" if mixed else "mixed"
-    extra[f"{other}_same_workload"] = form_leg(FMM, d_rec, a.n, a.P, a, other, flush, torch, local_rank)
-    if mixed:
-        extra["mixed_over_fp64_speedup"] = extra["fp64_same_workload"]["ms_per_eval"] / ms_dev
-    if not a.quick and world == 1:  # the side legs run at N = 1 only
+    if a.legs != "none":
+        extra[f"{other}_same_workload"] = form_leg(FMM, d_rec, a.n, a.P, a, other, flush, torch, local_rank)
+        if mixed:
+            extra["mixed_over_fp64_speedup"] = extra["fp64_same_workload"]["ms_per_eval"] / ms_dev
+    if a.legs == "all" and world == 1:  # the side legs run at N = 1 only
         extra["p12"] = {prec: form_leg(FMM, d_rec, a.n, 12, a, prec, flush, torch, local_rank)
                         for prec in ("mixed", "fp64")}
         extra["p12"]["mixed_over_fp64_speedup"] = (extra["p12"]["fp64"]["ms_per_eval"] /

@@ -231,9 +231,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int n
 // order at the end.  Leaves are limited to 64 bodies (ncrit <= 64); larger
 // leaves use the warp kernels above.
 constexpr int CT = 128;           // threads per CTA
-constexpr int CT_LEAVES = 32;     // source leaves staged at once
+// source leaves staged at once: FP32 24 (7 CTAs per SM, register-bound),
+// FP64 16 (5 CTAs per SM); tuned on B200 at 1M bodies
+template <bool F32>
+constexpr int ct_leaves() { return F32 ? 24 : 16; }
 constexpr int CT_MAXLEAF = 64;    // bodies per leaf the staging buffer allows
 constexpr int CT_TPT = 2;         // targets per thread (register blocking)
+constexpr int CT_BLOCK = 64;      // sources summed in FP32 before one compensated addition
 
 template <bool F32>
 struct NearBody;
@@ -249,16 +253,18 @@ struct NearBody<true> {
 };
 
 template <bool F32>
-__global__ void __launch_bounds__(CT) k_p2p_cta(const int *leaves, const int *begin, const int *count,
+__global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, const int *begin, const int *count,
                                                 const int *off, const u32 *ent, const double4 *xr,
                                                 const typename NearBody<F32>::T *bodies, double4 *out,
                                                 double cycle) {
   typedef typename NearBody<F32>::T BT;
   typedef typename NearBody<F32>::R RT;
+  constexpr int CT_LEAVES = ct_leaves<F32>();
+  static_assert(CT_LEAVES <= 32, "one warp computes the staging offsets");
   extern __shared__ __align__(16) unsigned char stage_raw[];  // CT_LEAVES * CT_MAXLEAF bodies
   BT *stage = (BT *)stage_raw;
-  __shared__ int soff[CT_LEAVES + 1];
-  __shared__ double red[CT * CT_TPT * 4];
+  __shared__ int soff[32 + 1];  // warp 0 scans 32 lanes (CT_LEAVES <= 32)
+  double *red = (double *)stage_raw;  // after the last chunk: CT * CT_TPT * 4 partial sums
   const int c = leaves[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31;
   const int tb = begin[c], tn = count[c];
@@ -320,40 +326,43 @@ __global__ void __launch_bounds__(CT) k_p2p_cta(const int *leaves, const int *be
     }
     __syncthreads();
     if (act) {
-      for (int b0 = g; b0 < T; b0 += 32 * G) {
+      // sources g, g+G, g+2G, ... of the staged chunk, CT_BLOCK at a time
+      // (FP32: one compensated addition per block), four per iteration
+      const int nsrc = g < T ? (T - g + G - 1) / G : 0;
+      const BT *sp = stage + g;
+      for (int c0 = 0; c0 < nsrc; c0 += CT_BLOCK) {
         RT p[CT_TPT][4];
 #pragma unroll
         for (int u = 0; u < CT_TPT; u++)
 #pragma unroll
           for (int q = 0; q < 4; q++) p[u][q] = 0;
-        const int bend = min(T, b0 + 32 * G);
-        int b = b0;
-        for (; b + G < bend; b += 2 * G) {
-          const BT s0 = stage[b], s1 = stage[b + G];
+        const int cend = min(nsrc, c0 + CT_BLOCK);
+        int c = c0;
+        auto acc_pair = [&](const BT &sv) {
 #pragma unroll
           for (int u = 0; u < CT_TPT; u++) {
-            if constexpr (F32) {
-              pair_f32(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
-              pair_f32(A[u].x, A[u].y, A[u].z, s1, p[u][0], p[u][1], p[u][2], p[u][3]);
-            } else {
-              pair(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
-              pair(A[u].x, A[u].y, A[u].z, s1, p[u][0], p[u][1], p[u][2], p[u][3]);
-            }
+            if constexpr (F32) pair_f32(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
+            else pair(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
           }
+        };
+        for (; c + 4 <= cend; c += 4) {
+          const BT s0 = sp[0], s1 = sp[G], s2 = sp[2 * G], s3 = sp[3 * G];
+          sp += 4 * G;
+          acc_pair(s0);
+          acc_pair(s1);
+          acc_pair(s2);
+          acc_pair(s3);
         }
-        if (b < bend) {
-          const BT s0 = stage[b];
-#pragma unroll
-          for (int u = 0; u < CT_TPT; u++) {
-            if constexpr (F32) pair_f32(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
-            else pair(A[u].x, A[u].y, A[u].z, s0, p[u][0], p[u][1], p[u][2], p[u][3]);
-          }
+        for (; c < cend; c++) {
+          const BT s0 = sp[0];
+          sp += G;
+          acc_pair(s0);
         }
 #pragma unroll
         for (int u = 0; u < CT_TPT; u++)
 #pragma unroll
           for (int q = 0; q < 4; q++) {
-            if constexpr (F32) two_sum_acc(sacc[u][q], eacc[u][q], p[u][q]);  // compensated per 32 sources
+            if constexpr (F32) two_sum_acc(sacc[u][q], eacc[u][q], p[u][q]);  // compensated per block
             else sacc[u][q] += p[u][q];
           }
       }
@@ -380,9 +389,9 @@ __global__ void __launch_bounds__(CT) k_p2p_cta(const int *leaves, const int *be
 
 void p2p_set_attributes() {
   cudaFuncSetAttribute(k_p2p_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       CT_LEAVES * CT_MAXLEAF * (int)sizeof(double4));
+                       ct_leaves<false>() * CT_MAXLEAF * (int)sizeof(double4));
   cudaFuncSetAttribute(k_p2p_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       CT_LEAVES * CT_MAXLEAF * (int)sizeof(float4));
+                       ct_leaves<true>() * CT_MAXLEAF * (int)sizeof(float4));
 }
 
 void p2p_pass(Handle &h) {
@@ -395,7 +404,7 @@ void p2p_pass(Handle &h) {
         h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
         h.src.as<double4>(), h.srcf.as<float4>());
     if (cta)
-      k_p2p_cta<true><<<h.nleaves, CT, CT_LEAVES * CT_MAXLEAF * sizeof(float4), h.stream>>>(
+      k_p2p_cta<true><<<h.nleaves, CT, ct_leaves<true>() * CT_MAXLEAF * sizeof(float4), h.stream>>>(
           h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
           h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
     else
@@ -407,7 +416,7 @@ void p2p_pass(Handle &h) {
     return;
   }
   if (cta)
-    k_p2p_cta<false><<<h.nleaves, CT, CT_LEAVES * CT_MAXLEAF * sizeof(double4), h.stream>>>(
+    k_p2p_cta<false><<<h.nleaves, CT, ct_leaves<false>() * CT_MAXLEAF * sizeof(double4), h.stream>>>(
         h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
         h.c_xr.as<double4>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
   else
