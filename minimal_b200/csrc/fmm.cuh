@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/exafmm_b200.h"
@@ -136,7 +137,12 @@ struct Handle {
   int m2l_units_P = -1;
 
   // grouped M2L (m2l_group.cu)
-  Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg, g_m16;
+  Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg, g_m16, g_slot;
+  // operator cache: group key -> slot in g_ops, for order op_P and layout
+  // op_layout (0: FP64 row blocks, 1: tensor-core FP16 images)
+  std::unordered_map<int, int> op_slot;
+  int op_P = -1, op_layout = -1;
+  std::vector<int> op_host_keys, op_host_slots, op_host_new_keys, op_host_new_slots;
   int g_ntiles = 0, g_ngroups = 0, g_nseg = 0;
   bool g_used_tc = false;
   bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only

@@ -17,15 +17,17 @@
 //   scan       group ids of the occupied keys;
 //   k_gops     the realified operator of every group (FP64);
 //   tiles      targets with grouped entries sorted by (level, child rank) and
-//              cut into tiles of 32; every grouped entry gets the sort key
-//              (tile, group) and one radix sort yields the (tile, group)
-//              segments, each with the source cell of every tile slot;
+//              cut into tiles (32 targets for DMMA, 128 for tcgen05); the
+//              (tile, group) pairs that hold entries are marked, scanned into
+//              segment ids and filled with the source cell of every tile slot;
 //   k_gemm64   one CTA (8 warps) per tile: for each group of the tile, stage
 //              the operator and the 32 gathered scaled multipoles in shared
 //              memory and accumulate with FP64 DMMA (mma.m8n8k4) in registers;
 //              then reduce the warps' pieces, unscale and store L.
 #include <map>
 #include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include "fmm.cuh"
 #include "harmonics.cuh"
@@ -45,8 +47,6 @@ constexpr int KEY_DL = 4;   // level difference lt - ls in [-4, 3]
 constexpr int KEY_V = 32;   // offset components in [-32, 31]
 constexpr int KEY_SPACE = 8 << 18;
 constexpr int XS = 36;      // padded row stride of the staged multipoles (doubles)
-constexpr int SLOT_SHIFT = 25;  // sorted entry value = tile slot << 25 | source cell
-constexpr u32 SLOT_MASK = (1u << SLOT_SHIFT) - 1;
 constexpr int TC_TILE = 128;    // targets per tile on the tensor core (MMA M)
 constexpr int TC_EPI_WARPS = 4; // warps 0-3: epilogue (warp w owns TMEM lanes 32w..32w+31)
 constexpr int TC_LOAD_WARP = 4; // first of the producer warps
@@ -72,8 +72,8 @@ __global__ void k_gkeys(int ncells, const int *off, const u32 *ent, const double
     if (img == 13) {
       const double4 Y = xr[s];
       const int dl = lt - level[s];
-      const double rf = fmin(X.w, Y.w);
-      const double vx = rint((X.x - Y.x) / rf), vy = rint((X.y - Y.y) / rf), vz = rint((X.z - Y.z) / rf);
+      const double inv = 1.0 / fmin(X.w, Y.w);  // the quotients are integers up to rounding
+      const double vx = rint((X.x - Y.x) * inv), vy = rint((X.y - Y.y) * inv), vz = rint((X.z - Y.z) * inv);
       if (dl >= -KEY_DL && dl < KEY_DL && vx >= -KEY_V && vx < KEY_V && vy >= -KEY_V && vy < KEY_V &&
           vz >= -KEY_V && vz < KEY_V) {
         key = ((dl + KEY_DL) << 18) | (((int)vx + KEY_V) << 12) | (((int)vy + KEY_V) << 6) | ((int)vz + KEY_V);
@@ -154,11 +154,10 @@ __device__ double op_value(int row, int col, int P, int NT, int dl, const double
 }
 
 // One CTA per group: the realified, scaled operator in row-block layout.
-__global__ void k_gops(const int *key_of, PlanDev pd, double *ops) {
+__global__ void k_gops(const int *keys, const int *slots, PlanDev pd, double *ops) {
   extern __shared__ double2 Zsh[];  // NT irregular harmonics of v
-  const int g = blockIdx.x;
-  const int dl = group_harmonics(key_of[g], pd.P, Zsh);
-  double *W = ops + (size_t)g * pd.wsize;
+  const int dl = group_harmonics(keys[blockIdx.x], pd.P, Zsh);
+  double *W = ops + (size_t)slots[blockIdx.x] * pd.wsize;
   for (int i = threadIdx.x; i < pd.wsize; i += blockDim.x) {
     int rb = 0;
     while (pd.woff[rb + 1] <= i) rb++;
@@ -203,12 +202,12 @@ TcPlan make_tc_plan(int P, int KP) {
 
 // One CTA per group: the operator split into FP16 hi + lo parts, written as
 // the byte image the MMA reads from shared memory (hi image, then lo image).
-__global__ void k_gops16(const int *key_of, int P, TcPlan pl, __half *ops16) {
+__global__ void k_gops16(const int *keys, const int *slots, int P, TcPlan pl, __half *ops16) {
   extern __shared__ double2 Zsh[];
-  const int g = blockIdx.x, NT = tri(P);
-  const int dl = group_harmonics(key_of[g], P, Zsh);
+  const int NT = tri(P);
+  const int dl = group_harmonics(keys[blockIdx.x], P, Zsh);
   const int nh = pl.bimg / 2;  // halves per image
-  __half *Wh = ops16 + (size_t)g * 2 * nh, *Wl = Wh + nh;
+  __half *Wh = ops16 + (size_t)slots[blockIdx.x] * 2 * nh, *Wl = Wh + nh;
   for (int e = threadIdx.x; e < nh; e += blockDim.x) {
     const int byte = 2 * e;
     int b = 0;
@@ -278,53 +277,46 @@ __global__ void k_tiles(int ntiles, int tile_n, int nflag, const u32 *sorted, in
   }
 }
 
-__global__ void k_gentries(int ncells, const int *off, const u32 *ent, const int *ekey, const int *gidx,
-                           const int *gcount, const int *tslot, int tile_n, int gbits, unsigned long long *fill,
-                           u64 *keys, u32 *vals) {
+// (tile, group) segments without sorting: mark every (tile, group) pair
+// that holds a grouped entry, scan the marks into segment ids (tiles in
+// order, groups in order within a tile), then write each entry's source into
+// its segment's slot.  A target has at most one entry per group, so every
+// (segment, slot) is written once.
+__global__ void k_gmark(int ncells, const int *off, const int *ekey, const int *gidx, const int *gcount,
+                        const int *tslot, int tile_n, int ngroups, int *mark) {
   const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (c >= ncells || gcount[c] == 0) return;
-  unsigned long long base = 0;
-  if (lane == 0) base = atomicAdd(fill, (unsigned long long)gcount[c]);
-  base = __shfl_sync(0xffffffffu, base, 0);
+  const long row = (long)(tslot[c] / tile_n) * ngroups;
+  for (int e = off[c] + lane; e < off[c + 1]; e += 32)
+    if (ekey[e] >= 0) mark[row + gidx[ekey[e]]] = 1;
+}
+
+__global__ void k_gfill(int ncells, const int *off, const u32 *ent, const int *ekey, const int *gidx,
+                        const int *gcount, const int *tslot, int tile_n, int ngroups, const int *segid,
+                        const int *slot_of_gid, int *tg_gid, int *tg_src) {
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (c >= ncells || gcount[c] == 0) return;
   const int ts = tslot[c];
-  const u64 tile = (u64)(ts / tile_n);
-  const u32 slot = (u32)(ts % tile_n);
-  int pos = 0;
-  for (int e0 = off[c]; e0 < off[c + 1]; e0 += 32) {
-    const int e = e0 + lane;
-    const bool ok = e < off[c + 1] && ekey[e] >= 0;
-    const unsigned b = __ballot_sync(0xffffffffu, ok);
-    if (ok) {
-      const int r = pos + __popc(b & ((1u << lane) - 1));
-      keys[base + r] = (tile << gbits) | (u64)gidx[ekey[e]];
-      vals[base + r] = (slot << SLOT_SHIFT) | (ent[e] & IDX_MASK);
-    }
-    pos += __popc(b);
+  const long row = (long)(ts / tile_n) * ngroups;
+  const int slot = ts % tile_n;
+  for (int e = off[c] + lane; e < off[c + 1]; e += 32) {
+    if (ekey[e] < 0) continue;
+    const int gid = gidx[ekey[e]];
+    const int sg = segid[row + gid];
+    tg_gid[sg] = slot_of_gid[gid];  // the group's operator slot in the cache
+    tg_src[(long)sg * tile_n + slot] = (int)(ent[e] & IDX_MASK);
   }
 }
 
-__global__ void k_segflags(const u64 *keys, long n, int gbits, int *flag) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) flag[i] = i == 0 || keys[i] != keys[i - 1];
+// First segment of every tile (the exclusive scan at the tile's first
+// group), and the end.
+__global__ void k_tg_off(int ntiles, int ngroups, const int *segid, const int *nseg, int *tg_off) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < ntiles) tg_off[t] = segid[(long)t * ngroups];
+  if (t == ntiles) tg_off[t] = *nseg;
 }
 
-__global__ void k_segments(const u64 *keys, const u32 *vals, long n, int tile_n, int gbits, const int *segid,
-                           int *tg_gid, int *tg_src, int *tg_off) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const u64 k = keys[i];
-  const bool first = i == 0 || k != keys[i - 1];
-  // segid is the exclusive scan of the segment-start flags: it already counts
-  // the start of this entry's own segment unless the entry is that start
-  const int s = segid[i] - (first ? 0 : 1);
-  if (first) tg_gid[s] = (int)(k & ((1ull << gbits) - 1));
-  const u32 v = vals[i];
-  tg_src[(long)s * tile_n + (v >> SLOT_SHIFT)] = (int)(v & SLOT_MASK);
-  const u64 tile = k >> gbits;
-  if (i == 0 || (keys[i - 1] >> gbits) != tile) tg_off[tile] = s;
-}
 
-__global__ void k_set_int(int *p, const int *v) { *p = *v; }
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -729,12 +721,6 @@ size_t gemm64_smem(const GroupPlan &g) {
   return std::max(stage, red) * sizeof(double);
 }
 
-int bits_for(long v) {
-  int b = 1;
-  while ((1l << b) < v) b++;
-  return b;
-}
-
 constexpr size_t TC_SMEM_MAX = 227 * 1024;  // opt-in shared memory per CTA on sm_100
 
 int tc_kp(int P) { return (P * (P + 1) + 15) / 16 * 16; }
@@ -811,15 +797,64 @@ void m2l_grouped_pass(Handle &h) {
     // operators
     h.g_keyof.need(ngroups * sizeof(int));
     k_key_of_gid<<<grid_for(KEY_SPACE, TB), TB, 0, s>>>(occ, gidx, h.g_keyof.as<int>());
+    // operators: cached per handle by group key (they depend only on the key
+    // and P); only keys not seen before are built
+    const int layout = tcore ? 1 : 0;
+    if (h.op_P != P || h.op_layout != layout) {
+      h.op_slot.clear();
+      h.op_P = P;
+      h.op_layout = layout;
+    }
+    const size_t op_bytes = tcore ? (size_t)2 * tp.bimg : (size_t)gp.wsize * sizeof(double);
+    std::vector<int> &key_of = h.op_host_keys;
+    key_of.resize(ngroups);
+    FMM_CUDA(cudaMemcpyAsync(key_of.data(), h.g_keyof.p, (size_t)ngroups * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> &slot_of = h.op_host_slots, &new_keys = h.op_host_new_keys, &new_slots = h.op_host_new_slots;
+    slot_of.resize(ngroups);
+    new_keys.clear();
+    new_slots.clear();
+    for (int g = 0; g < ngroups; g++) {
+      auto it = h.op_slot.find(key_of[g]);
+      if (it == h.op_slot.end()) {
+        const int sl = (int)h.op_slot.size();
+        it = h.op_slot.emplace(key_of[g], sl).first;
+        new_keys.push_back(key_of[g]);
+        new_slots.push_back(sl);
+      }
+      slot_of[g] = it->second;
+    }
+    const size_t nslots = h.op_slot.size();
+    if (nslots * op_bytes > h.g_ops.bytes) {  // grow, keeping the operators built so far
+      Buf grown;
+      grown.need(std::max(nslots, (size_t)64) * op_bytes * 2);
+      if (h.g_ops.p && nslots > new_keys.size())
+        FMM_CUDA(cudaMemcpyAsync(grown.p, h.g_ops.p, (nslots - new_keys.size()) * op_bytes, cudaMemcpyDeviceToDevice,
+                                 s));
+      FMM_CUDA(cudaStreamSynchronize(s));
+      h.g_ops.release();
+      h.g_ops = grown;
+    }
+    h.g_slot.need((size_t)(ngroups + 2 * new_keys.size() + 2) * sizeof(int));
+    int *d_slot_of = h.g_slot.as<int>(), *d_new_keys = d_slot_of + ngroups,
+        *d_new_slots = d_new_keys + new_keys.size();
+    FMM_CUDA(cudaMemcpyAsync(d_slot_of, slot_of.data(), (size_t)ngroups * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (!new_keys.empty()) {
+      FMM_CUDA(cudaMemcpyAsync(d_new_keys, new_keys.data(), new_keys.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+      FMM_CUDA(cudaMemcpyAsync(d_new_slots, new_slots.data(), new_slots.size() * sizeof(int), cudaMemcpyHostToDevice,
+                               s));
+      if (tcore)
+        k_gops16<<<(int)new_keys.size(), 256, NT * sizeof(double2), s>>>(d_new_keys, d_new_slots, P, tp,
+                                                                          h.g_ops.as<__half>());
+      else
+        k_gops<<<(int)new_keys.size(), 128, NT * sizeof(double2), s>>>(d_new_keys, d_new_slots, pd,
+                                                                        h.g_ops.as<double>());
+      h.launches++;
+    }
     if (tcore) {
-      h.g_ops.need((size_t)ngroups * 2 * tp.bimg);
-      k_gops16<<<ngroups, 256, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), P, tp, h.g_ops.as<__half>());
       h.g_m16.need((size_t)C * 2 * KP16 * sizeof(__half));
       k_msplit16<<<grid_for((long)C * KP16, TB), TB, 0, s>>>((long)C * KP16, KP16, h.g_mt.as<double>(),
                                                              h.g_m16.as<__half>());
-    } else {
-      h.g_ops.need((size_t)ngroups * gp.wsize * sizeof(double));
-      k_gops<<<ngroups, 128, NT * sizeof(double2), s>>>(h.g_keyof.as<int>(), pd, h.g_ops.as<double>());
     }
     // tiles of targets
     const int ntiles = (nflag + tile_n - 1) / tile_n;
@@ -832,21 +867,13 @@ void m2l_grouped_pass(Handle &h) {
     h.g_tile.need((size_t)ntiles * tile_n * sizeof(int) + 64);
     k_tiles<<<grid_for((long)ntiles * tile_n, TB), TB, 0, s>>>(ntiles, tile_n, nflag, tv, h.g_tile.as<int>(), tslot);
     // (tile, group) segments
-    const long ngent = nent - nres;
-    const int gbits = bits_for(ngroups), tbits = bits_for(ntiles + 1);
-    h.keys[0].need(ngent * 8); h.keys[1].need(ngent * 8);
-    h.vals[0].need(ngent * 4); h.vals[1].need(ngent * 4);
-    u64 *ek = h.keys[0].as<u64>(), *ek2 = h.keys[1].as<u64>();
-    u32 *ev = h.vals[0].as<u32>(), *ev2 = h.vals[1].as<u32>();
-    FMM_CUDA(cudaMemsetAsync(&ctr->gfill, 0, sizeof(unsigned long long), s));
-    k_gentries<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
-                                                        h.g_ekey.as<int>(), gidx, gcount, tslot, tile_n, gbits,
-                                                        &ctr->gfill, ek, ev);
-    radix_sort_pairs(h, ek, ev, ek2, ev2, ngent, 0, gbits + tbits);
-    h.g_seg.need((ngent + 1) * sizeof(int) * 2);
-    int *flag = h.g_seg.as<int>(), *segid = flag + ngent + 1;
-    k_segflags<<<grid_for(ngent, TB), TB, 0, s>>>(ek, ngent, gbits, flag);
-    scan_exclusive_int(h, flag, segid, ngent, &counts[3]);
+    const long nmark = (long)ntiles * ngroups;
+    h.g_seg.need((size_t)(nmark + 1) * sizeof(int) * 2);
+    int *mark = h.g_seg.as<int>(), *segid = mark + nmark + 1;
+    FMM_CUDA(cudaMemsetAsync(mark, 0, (size_t)nmark * sizeof(int), s));
+    k_gmark<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.g_ekey.as<int>(), gidx, gcount, tslot,
+                                                     tile_n, ngroups, mark);
+    scan_exclusive_int(h, mark, segid, nmark, &counts[3]);
     FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
     FMM_CUDA(cudaStreamSynchronize(s));
     const int nseg = h.hc.gcounts[3];
@@ -854,8 +881,10 @@ void m2l_grouped_pass(Handle &h) {
     // tg_src first: its rows of tile_n slots stay 16-byte aligned
     int *tg_src = h.g_tg.as<int>(), *tg_gid = tg_src + (size_t)nseg * tile_n, *tg_off = tg_gid + nseg;
     FMM_CUDA(cudaMemsetAsync(tg_src, 0xff, (size_t)nseg * tile_n * sizeof(int), s));
-    k_segments<<<grid_for(ngent, TB), TB, 0, s>>>(ek, ev, ngent, tile_n, gbits, segid, tg_gid, tg_src, tg_off);
-    k_set_int<<<1, 1, 0, s>>>(tg_off + ntiles, &counts[3]);
+    k_gfill<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(), h.g_ekey.as<int>(),
+                                                     gidx, gcount, tslot, tile_n, ngroups, segid, d_slot_of, tg_gid,
+                                                     tg_src);
+    k_tg_off<<<grid_for(ntiles + 1, TB), TB, 0, s>>>(ntiles, ngroups, segid, &counts[3], tg_off);
     // contraction
     if (tcore) {
       FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
