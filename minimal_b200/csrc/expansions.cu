@@ -8,6 +8,9 @@
 // and L2L take one thread per (cell, output coefficient (j,k)); the offset
 // harmonics they need depend only on level and octant and come from a
 // table built once per upward pass.
+#include <algorithm>
+#include <vector>
+
 #include "fmm.cuh"
 #include "harmonics.cuh"
 #include "translations.cuh"
@@ -124,8 +127,16 @@ __device__ void stage_tables(double2 *Y, const double2 *ytab, int dir, double rh
 
 // M2M of one level: thread (oct, o) translates the child in octant oct (if
 // any); the eight contributions are summed in octant order.
+// Term table of one translation for order P: output slot r computes
+// output perm[r] from terms[off[r], off[r+1]); slots sorted by descending
+// term count so the lanes of a warp do similar work.
+struct TermTable {
+  const int *perm, *off;
+  const unsigned *terms;
+};
+
 __global__ void __launch_bounds__(SH_T) k_m2m(int c0, const int *child, const int *nchild, const double4 *xr,
-                                             const double2 *ytab, double2 *M, int P) {
+                                             const double2 *ytab, TermTable tab, double2 *M, int P) {
   extern __shared__ double2 sm2[];  // Y[8][nt], Mc[8][nt], part[8][nt]
   __shared__ int cho[8];
   const int nt = tri(P), c = c0 + blockIdx.x;
@@ -147,9 +158,11 @@ __global__ void __launch_bounds__(SH_T) k_m2m(int c0, const int *child, const in
   }
   __syncthreads();
   const int oct = threadIdx.x / SH_O;
-  for (int o = threadIdx.x % SH_O; o < nt; o += SH_O) {
-    const int j = order_of(o), k = o - tri(j);
-    part[oct * nt + o] = cho[oct] >= 0 ? m2m_coeff(j, k, Mc + oct * nt, Y + oct * nt) : make_double2(0, 0);
+  for (int r = threadIdx.x % SH_O; r < nt; r += SH_O) {  // outputs by descending term count
+    const int o = tab.perm[r];
+    part[oct * nt + o] = cho[oct] >= 0 ? apply_terms(tab.terms + tab.off[r], tab.off[r + 1] - tab.off[r],
+                                                     Mc + oct * nt, Y + oct * nt)
+                                       : make_double2(0, 0);
   }
   __syncthreads();
   for (int o = threadIdx.x; o < nt; o += SH_T) {
@@ -165,7 +178,7 @@ __global__ void __launch_bounds__(SH_T) k_m2m(int c0, const int *child, const in
 // L2L of one level of parents: thread (oct, o) adds the parent's local,
 // shifted, into output o of its child in octant oct.
 __global__ void __launch_bounds__(SH_T) k_l2l(int c0, const int *child, const int *nchild, const double4 *xr,
-                                             const double2 *ytab, double2 *L, int P) {
+                                             const double2 *ytab, TermTable tab, double2 *L, int P) {
   extern __shared__ double2 sm2[];  // Y[8][nt], Lp[nt]
   __shared__ int cho[8];
   const int nt = tri(P), c = c0 + blockIdx.x;
@@ -184,9 +197,9 @@ __global__ void __launch_bounds__(SH_T) k_l2l(int c0, const int *child, const in
   __syncthreads();
   const int oct = threadIdx.x / SH_O, q = cho[oct];
   if (q < 0) return;
-  for (int o = threadIdx.x % SH_O; o < nt; o += SH_O) {
-    const int j = order_of(o), k = o - tri(j);
-    const double2 v = l2l_coeff(j, k, P, Lp, Y + oct * nt);
+  for (int r = threadIdx.x % SH_O; r < nt; r += SH_O) {  // outputs by descending term count
+    const int o = tab.perm[r];
+    const double2 v = apply_terms(tab.terms + tab.off[r], tab.off[r + 1] - tab.off[r], Lp, Y + oct * nt);
     double2 &d = L[(long)q * nt + o];
     d.x += v.x;
     d.y += v.y;
@@ -262,7 +275,46 @@ void expansions_set_attributes() {
   cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
-// Unit offset harmonics for order P (cached per handle).
+// Term tables of M2M and L2L for order P, built on the host from the same
+// enumerators the formulas use.  Layout (ints): per direction perm[nt],
+// off[nt + 1], terms[...].
+std::vector<int> term_tables(int P, size_t *l2l_at) {
+  const int nt = tri(P);
+  std::vector<int> out;
+  for (int dir = 0; dir < 2; dir++) {
+    if (dir == 1) *l2l_at = out.size();
+    std::vector<std::vector<unsigned>> per(nt);
+    for (int j = 0; j < P; j++)
+      for (int k = 0; k <= j; k++) {
+        auto emit = [&](int ia, bool ca, int n, int o, int f) { per[tri(j) + k].push_back(pack_term(ia, ca, n, o, f)); };
+        if (dir == 0) m2m_terms(j, k, emit);
+        else l2l_terms(j, k, P, emit);
+      }
+    std::vector<int> perm(nt);
+    for (int o = 0; o < nt; o++) perm[o] = o;
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return per[a].size() > per[b].size(); });
+    const size_t base = out.size();
+    out.resize(base + 2 * nt + 1);
+    int acc = 0;
+    for (int r = 0; r < nt; r++) {
+      out[base + r] = perm[r];
+      out[base + nt + r] = acc;
+      acc += (int)per[perm[r]].size();
+    }
+    out[base + 2 * nt] = acc;
+    for (int r = 0; r < nt; r++)
+      for (unsigned t : per[perm[r]]) out.push_back((int)t);
+  }
+  return out;
+}
+
+TermTable table_view(const Handle &h, int P, int dir) {
+  const int nt = tri(P);
+  const int *b = h.shift_terms.as<int>() + (dir ? h.shift_l2l_at : 0);
+  return TermTable{b, b + nt, (const unsigned *)(b + 2 * nt + 1)};
+}
+
+// Unit offset harmonics and term tables for order P (cached per handle).
 void unit_tables(Handle &h) {
   const int P = h.prm.P;
   if (h.shift_P == P) return;
@@ -270,6 +322,11 @@ void unit_tables(Handle &h) {
   k_unit_tables<<<16, 32, 0, h.stream>>>(P, h.shift_ops.as<double2>());
   h.launches++;
   FMM_LAUNCH();
+  size_t at = 0;
+  const std::vector<int> t = term_tables(P, &at);
+  h.shift_terms.need(t.size() * sizeof(int));
+  FMM_CUDA(cudaMemcpy(h.shift_terms.p, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
+  h.shift_l2l_at = at;
   h.shift_P = P;
 }
 
@@ -289,7 +346,7 @@ void upward_pass(Handle &h) {
     if (c1 <= c0) continue;
     k_m2m<<<c1 - c0, SH_T, 24 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
                                                           h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
-                                                          h.M.as<double2>(), P);
+                                                          table_view(h, P, 0), h.M.as<double2>(), P);
     h.launches++;
     FMM_LAUNCH();
   }
@@ -304,7 +361,7 @@ void downward_pass(Handle &h) {
     if (c1 <= c0) continue;
     k_l2l<<<c1 - c0, SH_T, 9 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
                                                          h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
-                                                         h.L.as<double2>(), P);
+                                                         table_view(h, P, 1), h.L.as<double2>(), P);
     h.launches++;
     FMM_LAUNCH();
   }
