@@ -128,6 +128,7 @@ struct Handle {
   size_t m2l_cap = 0, p2p_cap = 0;
   Buf m2l_off, m2l_ent, p2p_off, p2p_ent, fill;
   int64_t n_m2l = 0, n_p2p = 0;
+  bool m2l_ordered = false;  // M2L entries of each target in the reference's recording order
 
   // expansions
   Buf M, L;   // double2 [ncells][nterm]
@@ -170,6 +171,7 @@ void build_tree(Handle &h);
 // lists.cu
 void build_lists(Handle &h);
 void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img);
+void order_m2l_lists(Handle &h);
 // expansions.cu
 void upward_pass(Handle &h);
 void downward_pass(Handle &h);

@@ -201,7 +201,12 @@ __global__ void __launch_bounds__(SEG_WARPS * 32) k_order_segments(const int *of
 
 }  // namespace
 
-static void bucket(Handle &h, const int2 *raw, unsigned long long *n_dev, int64_t n, Buf &off_b, Buf &ent_b) {
+// CSR by target from the raw (target, source) pairs.  With `order` the
+// entries of each target are put in the reference's recording order;
+// without it they stay in arrival order (not deterministic) until
+// order_m2l_lists() runs.
+static void bucket(Handle &h, const int2 *raw, unsigned long long *n_dev, int64_t n, Buf &off_b, Buf &ent_b,
+                   bool order) {
   cudaStream_t s = h.stream;
   const int C = h.ncells;
   off_b.need((size_t)(C + 1) * 4);
@@ -214,11 +219,28 @@ static void bucket(Handle &h, const int2 *raw, unsigned long long *n_dev, int64_
   scan_exclusive_int(h, cnt, off_b.as<int>(), C + 1, nullptr);
   FMM_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(C + 1) * 4, s));
   u32 *tmp = ent_b.as<u32>() + (n > 0 ? n : 1);
-  k_bucket<<<g, TB, 0, s>>>(raw, n_dev, (u64)n, off_b.as<int>(), cnt, tmp);
-  k_order_segments<<<grid_for(C, SEG_WARPS), SEG_WARPS * 32, 0, s>>>(off_b.as<int>(), C, tmp, ent_b.as<u32>(),
-                                                                    h.c_pre.as<int>());
-  h.launches += 3;
+  k_bucket<<<g, TB, 0, s>>>(raw, n_dev, (u64)n, off_b.as<int>(), cnt, order ? tmp : ent_b.as<u32>());
+  h.launches += 2;
+  if (order) {
+    k_order_segments<<<grid_for(C, SEG_WARPS), SEG_WARPS * 32, 0, s>>>(off_b.as<int>(), C, tmp, ent_b.as<u32>(),
+                                                                      h.c_pre.as<int>());
+    h.launches++;
+  }
   FMM_LAUNCH();
+}
+
+void order_m2l_lists(Handle &h) {
+  if (h.m2l_ordered) return;
+  const int64_t n = h.n_m2l;
+  if (n > 0) {
+    u32 *ent = h.m2l_ent.as<u32>(), *tmp = ent + n;
+    FMM_CUDA(cudaMemcpyAsync(tmp, ent, n * sizeof(u32), cudaMemcpyDeviceToDevice, h.stream));
+    k_order_segments<<<grid_for(h.ncells, SEG_WARPS), SEG_WARPS * 32, 0, h.stream>>>(h.m2l_off.as<int>(), h.ncells,
+                                                                                     tmp, ent, h.c_pre.as<int>());
+    h.launches++;
+    FMM_LAUNCH();
+  }
+  h.m2l_ordered = true;
 }
 
 void build_lists(Handle &h) {
@@ -269,12 +291,20 @@ void build_lists(Handle &h) {
   }
   h.n_m2l = (int64_t)h.hc.n_m2l;
   h.n_p2p = (int64_t)h.hc.n_p2p;
-  bucket(h, h.m2l_raw.as<int2>(), &ctr->n_m2l, h.n_m2l, h.m2l_off, h.m2l_ent);
-  bucket(h, h.p2p_raw.as<int2>(), &ctr->n_p2p, h.n_p2p, h.p2p_off, h.p2p_ent);
+  // The grouped M2L does not depend on the order of a target's entries, so
+  // the M2L lists are put in the reference's order only when something reads
+  // that order: an export, the direct-form kernel, or residual entries.  The
+  // P2P lists are ordered always: their order is the near field's summation
+  // order, which keeps results reproducible.
+  const bool order_m2l = images > 0 || h.force_direct_m2l;
+  bucket(h, h.m2l_raw.as<int2>(), &ctr->n_m2l, h.n_m2l, h.m2l_off, h.m2l_ent, order_m2l);
+  h.m2l_ordered = order_m2l;
+  bucket(h, h.p2p_raw.as<int2>(), &ctr->n_p2p, h.n_p2p, h.p2p_off, h.p2p_ent, true);
 }
 
 // Lists in the reference's cell numbering (host arrays, CSR over ref index).
 void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img) {
+  order_m2l_lists(h);
   const int C = h.ncells;
   std::vector<int> ref(C), moff(C + 1), poff(C + 1);
   std::vector<u32> ment(h.n_m2l > 0 ? h.n_m2l : 1), pent(h.n_p2p > 0 ? h.n_p2p : 1);

@@ -98,8 +98,12 @@ void m2l_residual(Handle &h, const int *ekey) { launch_direct_form(h, ekey); }
 
 void m2l_pass(Handle &h) {
   h.L.need((size_t)h.ncells * tri(h.prm.P) * sizeof(double2));
-  if (!h.force_direct_m2l && m2l_grouped_available(h.prm.P)) m2l_grouped_pass(h);
-  else launch_direct_form(h, nullptr);
+  if (!h.force_direct_m2l && m2l_grouped_available(h.prm.P)) {
+    m2l_grouped_pass(h);
+  } else {
+    order_m2l_lists(h);  // the direct form sums each target's entries in list order
+    launch_direct_form(h, nullptr);
+  }
 }
 
 void m2l_set_attributes() {

@@ -793,6 +793,11 @@ void m2l_grouped_pass(Handle &h) {
   FMM_CUDA(cudaStreamSynchronize(s));
   const int nres = h.hc.gcounts[0], nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
   h.launches += 3;
+  if (nres > 0 && !h.m2l_ordered) {  // residual entries are summed in list order: order, then start over
+    order_m2l_lists(h);
+    m2l_grouped_pass(h);
+    return;
+  }
   if (ngroups > 0) {
     // operators
     h.g_keyof.need(ngroups * sizeof(int));
