@@ -9,7 +9,7 @@
 //   else both leaves                                 -> P2P entry
 //   else Cj leaf or (Ri >= Rj and Ci not a leaf)     -> (children of Ci, Cj)
 //   else                                             -> (Ci, children of Cj)
-// Emission uses warp-aggregated atomics.  The entries are then bucketed per
+// Emission uses one warp scan and one atomic per list per warp.  The entries are then bucketed per
 // target cell (CSR) and each target's entries are ordered as the recursion
 // would have recorded them: image-loop order first (x outermost), then the
 // source's depth-first pre-order rank (a depth-first walk meets the sources
@@ -34,22 +34,6 @@ __device__ __forceinline__ void img3(int img, int &x, int &y, int &z) {
   x = img % 3 - 1;
   y = (img / 3) % 3 - 1;
   z = img / 9 - 1;
-}
-
-// Warp-aggregated append of k items: returns this lane's first slot.
-__device__ __forceinline__ unsigned long long warp_append(unsigned long long *ctr, int k) {
-  const int lane = threadIdx.x & 31;
-  int incl = k;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
-  }
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  unsigned long long base = 0;
-  if (lane == 31 && total) base = atomicAdd(ctr, (unsigned long long)total);
-  base = __shfl_sync(0xffffffffu, base, 31);
-  return base + (unsigned long long)(incl - k);
 }
 
 __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const unsigned long long *nin_p,
@@ -97,23 +81,35 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
       }
     }
     const int packed_i = i | (img << IMG_SHIFT);
-    {
-      const unsigned long long s = warp_append(nm2l, kind == 0);
-      if (kind == 0) {
-        if (s < mcap) m2l[s] = make_int2(packed_i, j); else *overflow = 1;
-      }
+    // one warp scan for the three appends: M2L count in bits 0-5, P2P in
+    // 6-11, frontier pairs in 12-20 (at most 32, 32 and 256 per warp)
+    const int lane = threadIdx.x & 31;
+    const int mine = (kind == 0) | ((kind == 1) << 6) | (nk << 12);
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
     }
-    {
-      const unsigned long long s = warp_append(np2p, kind == 1);
-      if (kind == 1) {
-        if (s < pcap) p2p[s] = make_int2(packed_i, j); else *overflow = 1;
-      }
-    }
-    {
-      const unsigned long long s = warp_append(nout, nk);
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - mine;
+    unsigned long long res = 0;  // lanes 0, 1, 2 reserve the M2L, P2P and frontier ranges
+    if (lane == 0 && (total & 63)) res = atomicAdd(nm2l, (unsigned long long)(total & 63));
+    if (lane == 1 && ((total >> 6) & 63)) res = atomicAdd(np2p, (unsigned long long)((total >> 6) & 63));
+    if (lane == 2 && (total >> 12)) res = atomicAdd(nout, (unsigned long long)(total >> 12));
+    const unsigned long long bm = __shfl_sync(0xffffffffu, res, 0), bp = __shfl_sync(0xffffffffu, res, 1),
+                             bf = __shfl_sync(0xffffffffu, res, 2);
+    if (kind == 0) {
+      const unsigned long long sl = bm + (excl & 63);
+      if (sl < mcap) m2l[sl] = make_int2(packed_i, j); else *overflow = 1;
+    } else if (kind == 1) {
+      const unsigned long long sl = bp + ((excl >> 6) & 63);
+      if (sl < pcap) p2p[sl] = make_int2(packed_i, j); else *overflow = 1;
+    } else if (nk > 0) {
+      const unsigned long long sl = bf + (excl >> 12);
       for (int c = 0; c < nk; c++) {
-        if (s + c < fcap) {
-          fout[s + c] = kind == 2 ? make_int2((first + c) | (img << IMG_SHIFT), j) : make_int2(packed_i, first + c);
+        if (sl + c < fcap) {
+          fout[sl + c] = kind == 2 ? make_int2((first + c) | (img << IMG_SHIFT), j) : make_int2(packed_i, first + c);
         } else {
           *overflow = 1;
         }
