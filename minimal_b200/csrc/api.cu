@@ -111,6 +111,7 @@ void do_tree(Handle &h) {
   Timer t(h, PH_TREE);
   build_tree(h);
   h.have_tree = true;
+  h.srcf_ready = false;
   h.have_lists = h.have_up = h.have_horiz = h.have_down = false;
 }
 

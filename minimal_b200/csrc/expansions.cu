@@ -89,6 +89,157 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m(const int *leaves, int nleav
 }
 
 // M2M (3d/kernel.h:204-231), one warp per parent at one level.
+// ---- mixed form: P2M and L2P in FP32 (bodies relative to their leaf centre,
+// the FP32 copy the near field uses), same lock-step generator in float;
+// expansions stay FP64 in memory.
+__constant__ float c_recip_f[2 * EXAFMM_MAX_P + 4];
+
+struct SphF {
+  float r, c, s, inv_s;
+  float2 e;
+};
+
+__device__ __forceinline__ SphF sph_of_f(float dx, float dy, float dz) {
+  SphF o;
+  const float rxy2 = dx * dx + dy * dy;
+  o.r = sqrtf(rxy2 + dz * dz);
+  const float rxy = sqrtf(rxy2);
+  if (o.r == 0.f) {
+    o.c = 1.f;
+    o.s = 0.f;
+  } else {
+    o.c = dz / o.r;
+    o.s = rxy / o.r;
+  }
+  o.inv_s = o.s == 0.f ? 0.f : 1.f / o.s;
+  if (rxy == 0.f) o.e = make_float2(1.f, 0.f);
+  else o.e = make_float2(dx / rxy, dy / rxy);
+  return o;
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+template <bool WITH_DY, class F>
+__device__ __forceinline__ void regular_all_f(int P, const SphF &g, float2 e1, F f) {
+  float2 em = make_float2(1.f, 0.f);
+  float pmm = 1.f, odd = 1.f, cm = 1.f;
+  for (int m = 0; m < P; m++) {
+    float p = pmm, p1 = 0.f, cn = cm;
+    for (int n = m; n < P; n++) {
+      const float pn1 =
+          n == m ? g.c * (2 * m + 1) * p : (g.c * (2 * n + 1) * p - (n + m) * p1) * c_recip_f[n - m + 1];
+      const float2 Y = make_float2(em.x * cn * p, em.y * cn * p);
+      float2 dY = make_float2(0.f, 0.f);
+      if (WITH_DY) {
+        const float d = cn * ((n - m + 1) * pn1 - (n + 1) * g.c * p) * g.inv_s;
+        dY = make_float2(em.x * d, em.y * d);
+      }
+      f(n, m, Y, dY);
+      p1 = p;
+      p = pn1;
+      cn *= -g.r * c_recip_f[n + 1 + m];
+    }
+    cm *= -g.r * c_recip_f[2 * m + 2] * c_recip_f[2 * m + 1];
+    pmm = -pmm * odd * g.s;
+    odd += 2.f;
+    em = cmulf(em, e1);
+  }
+}
+
+// P2M in FP32: lane per body, each coefficient reduced over the warp by a
+// float butterfly, chunks of 32 bodies summed in FP64.
+__global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int nleaves, const int *begin,
+                                                        const int *count, const float4 *srcf, double2 *M, int P) {
+  extern __shared__ double2 sh[];
+  const int nt = tri(P);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * WARPS + wid;
+  if (w >= nleaves) return;
+  double2 *acc = sh + wid * nt;
+  for (int k = lane; k < nt; k += 32) acc[k] = make_double2(0, 0);
+  __syncwarp();
+  const int c = leaves[w];
+  const int b0 = begin[c], nb = count[c];
+  for (int t = 0; t < nb; t += 32) {
+    const bool ok = t + lane < nb;
+    const float4 B = ok ? srcf[b0 + t + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const SphF g = sph_of_f(B.x, B.y, B.z);
+    regular_all_f<false>(P, g, make_float2(g.e.x, -g.e.y), [&](int n, int m, float2 Y, float2) {
+      float x = B.w * Y.x, y = B.w * Y.y;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+      }
+      if (lane == 0) {
+        acc[tri(n) + m].x += (double)x;
+        acc[tri(n) + m].y += (double)y;
+      }
+    });
+  }
+  __syncwarp();
+  for (int k = lane; k < nt; k += 32) M[(long)c * nt + k] = acc[k];
+}
+
+// L2P in FP32: lane per body, the leaf's local expansion broadcast from
+// shared memory as float; p and F added to the FP64 results.
+__global__ void __launch_bounds__(WARPS * 32) k_l2p_f32(const int *leaves, int nleaves, const int *begin,
+                                                        const int *count, const float4 *srcf, const double2 *L,
+                                                        double4 *out, int P) {
+  extern __shared__ float2 shf[];
+  const int nt = tri(P);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * WARPS + wid;
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  float2 *Lc = shf + wid * nt;
+  for (int k = lane; k < nt; k += 32) {
+    const double2 l = L[(long)c * nt + k];
+    Lc[k] = make_float2((float)l.x, (float)l.y);
+  }
+  __syncwarp();
+  const int b0 = begin[c], nb = count[c];
+  for (int t = 0; t < nb; t += 32) {
+    const int b = b0 + t + lane;
+    const bool ok = t + lane < nb;
+    const float4 B = ok ? srcf[b] : make_float4(1.f, 0.f, 0.f, 0.f);
+    const SphF g = sph_of_f(B.x, B.y, B.z);
+    float pot = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    regular_all_f<true>(P, g, g.e, [&](int n, int m, float2 Y, float2 dY) {
+      const float2 l = Lc[tri(n) + m];
+      const float w2 = m == 0 ? 1.f : 2.f;
+      const float re = l.x * Y.x - l.y * Y.y;
+      const float red = l.x * dY.x - l.y * dY.y;
+      const float rei = -(l.x * Y.y + l.y * Y.x);
+      pot += w2 * re;
+      s0 += w2 * re * n;
+      s1 += w2 * red;
+      s2 += w2 * rei * m;
+    });
+    s0 = g.r != 0.f ? s0 / g.r : 0.f;
+    if (ok) {
+      const float st = g.s, ct = g.c, cp = g.e.x, sp = g.e.y, r = g.r;
+      float fx = st * cp * s0, fy = st * sp * s0, fz = ct * s0;
+      if (r != 0.f) {
+        fx += ct * cp / r * s1;
+        fy += ct * sp / r * s1;
+        fz -= st / r * s1;
+        if (st != 0.f) {
+          fx -= sp / r / st * s2;
+          fy += cp / r / st * s2;
+        }
+      }
+      double4 &d = out[b];
+      d.x += pot;
+      d.y += fx;
+      d.z += fy;
+      d.w += fz;
+    }
+  }
+}
+
 // M2M and L2L.  A child sits at its parent's centre +-R_child on every
 // axis, so the offset harmonics depend only on the octant and, through
 // rho = R_child, on the level: Y_n = rho^n Yhat_n with Yhat the harmonics of
@@ -269,8 +420,13 @@ void expansions_set_attributes() {
   rc[0] = 0;
   for (int k = 1; k < 2 * EXAFMM_MAX_P + 4; k++) rc[k] = 1.0 / k;
   FMM_CUDA(cudaMemcpyToSymbol(c_recip, rc, sizeof(rc)));
+  float rf[2 * EXAFMM_MAX_P + 4];
+  for (int k = 0; k < 2 * EXAFMM_MAX_P + 4; k++) rf[k] = (float)rc[k];
+  FMM_CUDA(cudaMemcpyToSymbol(c_recip_f, rf, sizeof(rf)));
   cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2p, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_p2m_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_l2p_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
@@ -335,9 +491,16 @@ void upward_pass(Handle &h) {
   const int P = h.prm.P, nt = tri(P);
   h.M.need((size_t)h.ncells * nt * sizeof(double2));
   h.L.need((size_t)h.ncells * nt * sizeof(double2));
-  k_p2m<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
-      h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
-      h.src.as<double4>(), h.M.as<double2>(), P);
+  if (h.prm.precision == EXAFMM_MIXED) {
+    make_srcf(h);
+    k_p2m_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
+        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.srcf.as<float4>(),
+        h.M.as<double2>(), P);
+  } else {
+    k_p2m<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
+        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
+        h.src.as<double4>(), h.M.as<double2>(), P);
+  }
   h.launches++;
   FMM_LAUNCH();
   unit_tables(h);
@@ -365,9 +528,16 @@ void downward_pass(Handle &h) {
     h.launches++;
     FMM_LAUNCH();
   }
-  k_l2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
-      h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
-      h.src.as<double4>(), h.L.as<double2>(), h.out.as<double4>(), P);
+  if (h.prm.precision == EXAFMM_MIXED) {
+    make_srcf(h);
+    k_l2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(float2), s>>>(
+        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.srcf.as<float4>(),
+        h.L.as<double2>(), h.out.as<double4>(), P);
+  } else {
+    k_l2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
+        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
+        h.src.as<double4>(), h.L.as<double2>(), h.out.as<double4>(), P);
+  }
   h.launches++;
   FMM_LAUNCH();
 }

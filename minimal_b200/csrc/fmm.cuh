@@ -103,6 +103,7 @@ struct Handle {
   Buf out;     // double4 (p,Fx,Fy,Fz), tree order
   Buf perm;    // int, tree position -> input index
   Buf srcf;    // float4 (x,y,z rel. to leaf centre, q), tree order (mixed form)
+  bool srcf_ready = false;  // srcf matches the current tree
   Buf stage;   // staging for Body records crossing the boundary
 
   // tree build scratch
@@ -179,6 +180,7 @@ void downward_pass(Handle &h);
 void m2l_pass(Handle &h);
 // p2p.cu
 void p2p_pass(Handle &h);
+void make_srcf(Handle &h);
 void direct_sum(Handle &h, double4 *targets_pq /*x,y,z,q*/, double4 *out, long nt);
 // periodic.cu
 void periodic_set_attributes();

@@ -387,6 +387,18 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
 
 }  // namespace
 
+// The FP32 leaf-relative copy of the bodies (mixed form), once per tree.
+void make_srcf(Handle &h) {
+  if (h.srcf_ready) return;
+  h.srcf.need((size_t)h.n * sizeof(float4));
+  k_make_srcf<<<grid_for((long)h.nleaves * 32, 256), 256, 0, h.stream>>>(
+      h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
+      h.src.as<double4>(), h.srcf.as<float4>());
+  h.launches++;
+  FMM_LAUNCH();
+  h.srcf_ready = true;
+}
+
 void p2p_set_attributes() {
   cudaFuncSetAttribute(k_p2p_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        ct_leaves<false>() * CT_MAXLEAF * (int)sizeof(double4));
@@ -399,10 +411,7 @@ void p2p_pass(Handle &h) {
   const double cyc = h.prm.images ? h.prm.cycle : 0.0;
   const bool cta = h.prm.ncrit <= CT_MAXLEAF;  // every leaf fits the staging layout
   if (h.prm.precision == EXAFMM_MIXED) {
-    h.srcf.need((size_t)h.n * sizeof(float4));
-    k_make_srcf<<<grid_for((long)h.nleaves * 32, 256), 256, 0, h.stream>>>(
-        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
-        h.src.as<double4>(), h.srcf.as<float4>());
+    make_srcf(h);
     if (cta)
       k_p2p_cta<true><<<h.nleaves, CT, ct_leaves<true>() * CT_MAXLEAF * sizeof(float4), h.stream>>>(
           h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
@@ -411,7 +420,7 @@ void p2p_pass(Handle &h) {
       k_p2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
           h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
           h.p2p_ent.as<u32>(), h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
-    h.launches += 2;
+    h.launches++;
     FMM_LAUNCH();
     return;
   }
