@@ -639,7 +639,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         ok = tc::mbar_wait(&full[st], parity(k), spin) && tc::mbar_wait(&bful[st], parity(k), spin);
         if (ok && k % flush_every == 0 && w >= 2) ok = tc::mbar_wait(&acce[a], (uint32_t)((w >> 1) - 1) & 1u, spin);
         if (!ok) break;
-        tc::fence_async_smem();  // the producers' cp.async writes -> the tensor core's reads
         tc::fence_after();
         const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
         const uint64_t dA = tc::smem_desc_sw128(sA), dB = tc::smem_desc_sw128(sB);
