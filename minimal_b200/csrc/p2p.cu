@@ -228,14 +228,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int n
 // source starting at g = t / H, G = floor(128/H): for leaves of 20-64 bodies
 // nearly all 128 threads are busy, and each staged source is read once per
 // two pairs.  Partial sums of the G source groups are combined in a fixed
-// order at the end.  Leaves are limited to 64 bodies (ncrit <= 64); larger
-// leaves use the warp kernels above.
+// order at the end.  A chunk stages as many whole source leaves (up to 32)
+// as fit in the buffer; target leaves up to 256 bodies (ncrit <= 256) use
+// this kernel, larger ones the warp kernels above.
 constexpr int CT = 128;           // threads per CTA
-// source leaves staged at once: FP32 24 (7 CTAs per SM, register-bound),
-// FP64 16 (5 CTAs per SM); tuned on B200 at 1M bodies
+// bodies staged at once: FP32 1536 (7 CTAs per SM, register-bound), FP64
+// 1024 (5 CTAs per SM); tuned on B200 at 1M bodies
 template <bool F32>
-constexpr int ct_leaves() { return F32 ? 24 : 16; }
-constexpr int CT_MAXLEAF = 64;    // bodies per leaf the staging buffer allows
+constexpr int ct_cap() { return F32 ? 1536 : 1024; }
+constexpr int CT_MAXTGT = 256;    // target-leaf bodies: two per thread
 constexpr int CT_TPT = 2;         // targets per thread (register blocking)
 constexpr int CT_BLOCK = 64;      // sources summed in FP32 before one compensated addition
 
@@ -259,11 +260,11 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
                                                 double cycle) {
   typedef typename NearBody<F32>::T BT;
   typedef typename NearBody<F32>::R RT;
-  constexpr int CT_LEAVES = ct_leaves<F32>();
-  static_assert(CT_LEAVES <= 32, "one warp computes the staging offsets");
-  extern __shared__ __align__(16) unsigned char stage_raw[];  // CT_LEAVES * CT_MAXLEAF bodies
+  constexpr int CAP = ct_cap<F32>();
+  extern __shared__ __align__(16) unsigned char stage_raw[];  // CAP bodies
   BT *stage = (BT *)stage_raw;
-  __shared__ int soff[32 + 1];  // warp 0 scans 32 lanes (CT_LEAVES <= 32)
+  __shared__ int soff[32 + 1];  // staging offsets of the chunk's leaves (warp 0 scans up to 32)
+  __shared__ int s_nl;          // leaves in the chunk
   double *red = (double *)stage_raw;  // after the last chunk: CT * CT_TPT * 4 partial sums
   const int c = leaves[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31;
@@ -282,11 +283,11 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
 #pragma unroll
     for (int q = 0; q < 4; q++) sacc[u][q] = eacc[u][q] = 0;
   const int eb = off[c], ee = off[c + 1];
-  for (int e0i = eb; e0i < ee; e0i += CT_LEAVES) {
-    const int nl = min(CT_LEAVES, ee - e0i);
+  for (int e0i = eb; e0i < ee;) {
     __syncthreads();
-    if (tid < 32) {  // offsets of the chunk's leaves in the staging buffer
-      const int n = lane < nl ? count[ent[e0i + lane] & IDX_MASK] : 0;
+    if (tid < 32) {  // offsets of the next leaves in the staging buffer; take those that fit
+      const int cand = min(32, ee - e0i);
+      const int n = lane < cand ? count[ent[e0i + lane] & IDX_MASK] : 0;
       int inc = n;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -295,9 +296,13 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
       }
       soff[lane + 1] = inc;
       if (lane == 0) soff[0] = 0;
+      // the running sums grow, so the leaves that fit are a prefix (at least
+      // one: no leaf exceeds the buffer)
+      const unsigned fit = __ballot_sync(0xffffffffu, lane < cand && inc <= CAP);
+      if (lane == 0) s_nl = __popc(fit);
     }
     __syncthreads();
-    const int T = soff[nl];
+    const int nl = s_nl, T = soff[nl];
     for (int k = tid >> 5; k < nl; k += CT / 32) {
       const u32 en = ent[e0i + k];
       const int sc = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
@@ -367,6 +372,7 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
           }
       }
     }
+    e0i += nl;
   }
   __syncthreads();
   if (act) {
@@ -401,19 +407,19 @@ void make_srcf(Handle &h) {
 
 void p2p_set_attributes() {
   cudaFuncSetAttribute(k_p2p_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       ct_leaves<false>() * CT_MAXLEAF * (int)sizeof(double4));
+                       ct_cap<false>() * (int)sizeof(double4));
   cudaFuncSetAttribute(k_p2p_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       ct_leaves<true>() * CT_MAXLEAF * (int)sizeof(float4));
+                       ct_cap<true>() * (int)sizeof(float4));
 }
 
 void p2p_pass(Handle &h) {
   h.out.need((size_t)h.n * sizeof(double4));
   const double cyc = h.prm.images ? h.prm.cycle : 0.0;
-  const bool cta = h.prm.ncrit <= CT_MAXLEAF;  // every leaf fits the staging layout
+  const bool cta = h.prm.ncrit <= CT_MAXTGT;  // every leaf fits two targets per thread and the buffer
   if (h.prm.precision == EXAFMM_MIXED) {
     make_srcf(h);
     if (cta)
-      k_p2p_cta<true><<<h.nleaves, CT, ct_leaves<true>() * CT_MAXLEAF * sizeof(float4), h.stream>>>(
+      k_p2p_cta<true><<<h.nleaves, CT, ct_cap<true>() * sizeof(float4), h.stream>>>(
           h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
           h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
     else
@@ -425,7 +431,7 @@ void p2p_pass(Handle &h) {
     return;
   }
   if (cta)
-    k_p2p_cta<false><<<h.nleaves, CT, ct_leaves<false>() * CT_MAXLEAF * sizeof(double4), h.stream>>>(
+    k_p2p_cta<false><<<h.nleaves, CT, ct_cap<false>() * sizeof(double4), h.stream>>>(
         h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
         h.c_xr.as<double4>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
   else
