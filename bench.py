@@ -235,7 +235,8 @@ def form_leg(FMM, d_rec, n, P, a, precision, flush, torch, local_rank, steps=3, 
 def batched_leg(FMM, torch, dev, local_rank, nsys=2048):
     """Batched configuration: 2048 independent systems, sizes log-uniform in
     [1000, 65536] (seeded), each uniform in [-pi, pi]^3, P=6, theta=0.5,
-    mixed; one batched evaluation vs the same systems one at a time."""
+    mixed, ncrit picked by the autotuner; one batched evaluation vs the same
+    systems one at a time (same ncrit), host clock around each."""
     from minimal_b200.bodies import uniform_bodies
 
     rng = np.random.default_rng(2048)
@@ -250,6 +251,11 @@ def batched_leg(FMM, torch, dev, local_rank, nsys=2048):
     f = FMM(P=6, ncrit=64, theta=0.5, precision="mixed", device=local_rank)
     f.set_batch_device(d.data_ptr(), offs)
     f.evaluate()
+    t64 = []
+    for _ in range(2):
+        f.evaluate()
+        t64.append(f.timings()["total"])
+    ncrit, tuned_ms = f.autotune(repeats=2)  # the project's autotuner over the leaf size
     tb = []
     for _ in range(3):
         torch.cuda.synchronize()
@@ -263,7 +269,7 @@ def batched_leg(FMM, torch, dev, local_rank, nsys=2048):
     out = f.bodies()
     q = int(np.argmax(sizes))
     f.close()
-    g = FMM(P=6, ncrit=64, theta=0.5, precision="mixed", device=local_rank)
+    g = FMM(P=6, ncrit=ncrit, theta=0.5, precision="mixed", device=local_rank)
     g.set_bodies_device(d[offs[q]:].data_ptr(), int(sizes[q]))
     g.evaluate()
     alone = g.bodies()
@@ -283,7 +289,8 @@ def batched_leg(FMM, torch, dev, local_rank, nsys=2048):
     g.close()
     t_b = min(tb)
     return {"workload": f"{nsys} systems, sizes log-uniform in [1000, 65536] (seeded), {N} bodies, "
-                        "uniform in [-pi,pi]^3, P=6, theta=0.5, ncrit=64, mixed",
+                        f"uniform in [-pi,pi]^3, P=6, theta=0.5, mixed, ncrit autotuned -> {ncrit}",
+            "autotune": {"ncrit": ncrit, "tuned_device_ms": tuned_ms, "device_ms_at_ncrit_64": min(t64)},
             "bodies": N, "batched_ms": t_b * 1e3, "batched_bodies_per_s": N / t_b,
             "one_at_a_time_ms": t1 * 1e3, "one_at_a_time_bodies_per_s": N / t1, "speedup": t1 / t_b,
             "batched_phases_ms": phases,

@@ -155,6 +155,16 @@ EXAFMM_API int exafmm_b200_ewald(exafmm_b200 *h, int ksize, double alpha, double
 EXAFMM_API int exafmm_b200_set_batch(exafmm_b200 *h, const double *bodies8, const int64_t *offsets, int nsys,
                                      int where);
 
+/* Autotuner (no reference counterpart: the reference hard-codes ncrit,
+ * 3d/fmm.cxx:14).  Times evaluate() on the bodies now loaded (one system or a
+ * batch) for each candidate leaf size ncrit (NULL = 32, 48, 64, 96, 128,
+ * 192, 256), `repeats` timed runs each after one warm-up, keeps the fastest
+ * in the handle's parameters and leaves its results in the handle.  ncrit
+ * shapes the tree, so results after tuning are those of the chosen ncrit,
+ * not of the reference's; the plain drop-in configuration keeps ncrit = 64. */
+EXAFMM_API int exafmm_b200_autotune(exafmm_b200 *h, const int *ncrit_candidates, int ncand, int repeats,
+                                    int *best_ncrit, double *best_ms);
+
 /* Per-phase device times of the last evaluation in milliseconds, measured
  * with CUDA events on the handle's stream: tree, lists, upward, m2l, p2p,
  * downward, total (7 values). */

@@ -37,7 +37,7 @@ API = [
     "exafmm_b200_get_perm", "exafmm_b200_num_cells", "exafmm_b200_get_tree", "exafmm_b200_count_lists",
     "exafmm_b200_get_lists", "exafmm_b200_get_expansions", "exafmm_b200_direct", "exafmm_b200_get_timings",
     "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak", "exafmm_b200_direct_static",
-    "exafmm_b200_dipole_correction", "exafmm_b200_ewald", "exafmm_b200_set_batch",
+    "exafmm_b200_dipole_correction", "exafmm_b200_ewald", "exafmm_b200_set_batch", "exafmm_b200_autotune",
 ]
 
 PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
@@ -95,6 +95,7 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_dipole_correction": (i, [vp]),
         "exafmm_b200_ewald": (i, [vp, i, d, d, d, vp, i64, i]),
         "exafmm_b200_set_batch": (i, [vp, vp, vp, i, i]),
+        "exafmm_b200_autotune": (i, [vp, vp, i, i, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -271,6 +272,20 @@ class FMM:
         self._check(self.lib.exafmm_b200_ewald(self.h, int(ksize), float(alpha), float(sigma), float(cutoff), _p(t),
                                                len(t), HOST))
         return t
+
+    def autotune(self, candidates=None, repeats=2):
+        """Pick the fastest leaf size ncrit for the loaded bodies (one system or
+        a batch); returns (ncrit, ms per evaluation) and keeps it."""
+        best = np.zeros(1, dtype=np.int32)
+        ms = np.zeros(1)
+        if candidates is None:
+            cand_p, nc = None, 0
+        else:
+            cand = np.ascontiguousarray(candidates, dtype=np.int32)
+            cand_p, nc = _p(cand), len(cand)
+        self._check(self.lib.exafmm_b200_autotune(self.h, cand_p, nc, int(repeats), _p(best), _p(ms)))
+        self.params.ncrit = int(best[0])
+        return int(best[0]), float(ms[0])
 
     def timings(self):
         t = np.zeros(7)

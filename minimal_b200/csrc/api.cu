@@ -4,6 +4,8 @@
 #include <cstring>
 #include <new>
 
+#include <algorithm>
+
 #include "fmm.cuh"
 
 namespace fmm {
@@ -344,6 +346,50 @@ int exafmm_b200_evaluate(exafmm_b200 *H) {
     do_horiz(h);
     do_down(h);
     sync(h);
+  });
+}
+
+int exafmm_b200_autotune(exafmm_b200 *H, const int *candidates, int ncand, int repeats, int *best_ncrit,
+                         double *best_ms) {
+  return guarded(H, [&](Handle &h) {
+    if (h.n <= 0) throw Error{EXAFMM_ERR_STATE, "autotune() needs bodies (set_bodies or set_batch)"};
+    static const int defaults[] = {32, 48, 64, 96, 128, 192, 256};
+    if (!candidates) {
+      candidates = defaults;
+      ncand = (int)(sizeof(defaults) / sizeof(defaults[0]));
+    }
+    if (ncand < 1 || ncand > 64) throw Error{EXAFMM_ERR_ARG, "autotune(): 1 to 64 candidates"};
+    for (int k = 0; k < ncand; k++)
+      if (candidates[k] < 1) throw Error{EXAFMM_ERR_ARG, "autotune(): ncrit candidates must be >= 1"};
+    if (repeats < 1 || repeats > 100) throw Error{EXAFMM_ERR_ARG, "autotune(): repeats in [1, 100]"};
+    auto run = [&]() {
+      h.launches = 0;
+      do_tree(h);
+      do_lists(h);
+      do_up(h);
+      do_horiz(h);
+      do_down(h);
+      sync(h);
+      return (double)h.ms[PH_COUNT];
+    };
+    int best = -1;
+    double tbest = 0;
+    for (int k = 0; k < ncand; k++) {
+      h.prm.ncrit = candidates[k];
+      h.key_levels = 0;  // the key depth follows ncrit
+      run();             // warm-up: buffers grow to this tree's size
+      double t = run();
+      for (int r = 1; r < repeats; r++) t = std::min(t, run());
+      if (best < 0 || t < tbest) {
+        best = candidates[k];
+        tbest = t;
+      }
+    }
+    h.prm.ncrit = best;
+    h.key_levels = 0;
+    run();  // leave the results of the chosen setting
+    if (best_ncrit) *best_ncrit = best;
+    if (best_ms) *best_ms = tbest;
   });
 }
 

@@ -113,3 +113,25 @@ def test_batch_errors():
     f.set_bodies(sys_[0])  # back to a single system
     f.evaluate()
     assert len(f.tree()["nchild"]) >= 1
+
+
+def test_autotune_picks_a_candidate_and_keeps_it():
+    """The autotuner times the loaded batch for each candidate ncrit, keeps the
+    fastest, and leaves exactly the results of that setting."""
+    from minimal_b200 import FMM, FMMError
+
+    sys_ = systems([3000, 20000, 500, 9000], 500)
+    f = FMM(P=6, ncrit=64, theta=0.5, precision="mixed")
+    f.set_batch(sys_)
+    best, ms = f.autotune([32, 64, 128], repeats=2)
+    assert best in (32, 64, 128) and ms > 0
+    tuned = f.bodies()
+    g = FMM(P=6, ncrit=best, theta=0.5, precision="mixed")
+    g.set_batch(sys_)
+    g.evaluate()
+    ref = g.bodies()
+    assert np.array_equal(tuned[:, :4], ref[:, :4])
+    assert rel_l2(tuned[:, 5:], ref[:, 5:]) < 1e-6
+    with pytest.raises(FMMError) as e:
+        f.autotune([0, 64])
+    assert e.value.code == -1
