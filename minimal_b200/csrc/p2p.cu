@@ -220,17 +220,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int n
 }
 
 // ------------------------------------------------ CTA-per-leaf near field
-// One CTA per target leaf.  The bodies of up to 32 source leaves at a time
-// are staged in shared memory already shifted into the target's frame (warp
-// w copies source leaves w, w+4, ...; the shift is computed once per leaf),
-// so the inner loop is a plain (target, source) sweep.  Thread t takes the
-// targets i and i+H with i = t % H, H = ceil(tn/2), and every G-th staged
-// source starting at g = t / H, G = floor(128/H): for leaves of 20-64 bodies
-// nearly all 128 threads are busy, and each staged source is read once per
-// two pairs.  Partial sums of the G source groups are combined in a fixed
-// order at the end.  A chunk stages as many whole source leaves (up to 32)
-// as fit in the buffer; target leaves up to 256 bodies (ncrit <= 256) use
-// this kernel, larger ones the warp kernels above.
+// One CTA per target leaf.  The P2P list is taken in chunks of whole source
+// leaves (up to 32) that fit the staging buffer.  Every warp reads the
+// metadata of the chunk's leaves lane-parallel (lane k: leaf k's first body,
+// size and shift into the target frame) and scans the sizes; the warps then
+// copy the chunk's bodies into shared memory, already shifted into the
+// target's frame, in 32-body blocks (a body finds its leaf with two warp
+// votes), so the inner loop is a plain (target, source) sweep.  Thread t
+// takes the targets i and i+H with i = t % H, H = ceil(tn/2), and the G-th
+// part of the staged sources, g = t / H, G = floor(128/H): for leaves of 20-64
+// bodies nearly all 128 threads are busy, and each staged source is read once
+// per two pairs.  Partial sums of the G source parts are combined in a fixed
+// order at the end.  Target leaves up to 256 bodies (ncrit <= 256) use this
+// kernel, larger ones the warp kernels above.
 constexpr int CT = 128;           // threads per CTA
 // bodies staged at once: FP32 1536 (7 CTAs per SM, register-bound), FP64
 // 1024 (5 CTAs per SM); tuned on B200 at 1M bodies
@@ -239,6 +241,9 @@ constexpr int ct_cap() { return F32 ? 1536 : 1024; }
 constexpr int CT_MAXTGT = 256;    // target-leaf bodies: two per thread
 constexpr int CT_TPT = 2;         // targets per thread (register blocking)
 constexpr int CT_BLOCK = 64;      // sources summed in FP32 before one compensated addition
+// 32-body blocks a warp loads before storing them (register-bound)
+template <bool F32>
+constexpr int ct_unroll() { return F32 ? 3 : 1; }
 
 template <bool F32>
 struct NearBody;
@@ -260,14 +265,13 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
                                                 double cycle) {
   typedef typename NearBody<F32>::T BT;
   typedef typename NearBody<F32>::R RT;
-  constexpr int CAP = ct_cap<F32>();
+  constexpr int CAP = ct_cap<F32>(), CT_UNROLL = ct_unroll<F32>();
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char stage_raw[];  // CAP bodies
   BT *stage = (BT *)stage_raw;
-  __shared__ int soff[32 + 1];  // staging offsets of the chunk's leaves (warp 0 scans up to 32)
-  __shared__ int s_nl;          // leaves in the chunk
   double *red = (double *)stage_raw;  // after the last chunk: CT * CT_TPT * 4 partial sums
   const int c = leaves[blockIdx.x];
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int tb = begin[c], tn = count[c];
   const int H = (tn + CT_TPT - 1) / CT_TPT, G = CT / H;
   const int i = tid % H, g = tid / H;
@@ -284,65 +288,94 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
     for (int q = 0; q < 4; q++) sacc[u][q] = eacc[u][q] = 0;
   const int eb = off[c], ee = off[c + 1];
   for (int e0i = eb; e0i < ee;) {
-    __syncthreads();
-    if (tid < 32) {  // offsets of the next leaves in the staging buffer; take those that fit
-      const int cand = min(32, ee - e0i);
-      const int n = lane < cand ? count[ent[e0i + lane] & IDX_MASK] : 0;
-      int inc = n;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
-      }
-      soff[lane + 1] = inc;
-      if (lane == 0) soff[0] = 0;
-      // the running sums grow, so the leaves that fit are a prefix (at least
-      // one: no leaf exceeds the buffer)
-      const unsigned fit = __ballot_sync(0xffffffffu, lane < cand && inc <= CAP);
-      if (lane == 0) s_nl = __popc(fit);
-    }
-    __syncthreads();
-    const int nl = s_nl, T = soff[nl];
-    for (int k = tid >> 5; k < nl; k += CT / 32) {
-      const u32 en = ent[e0i + k];
-      const int sc = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
-      const int sb = begin[sc], sn = count[sc], so = soff[k];
-      const double sx = (img % 3 - 1) * cycle, sy = ((img / 3) % 3 - 1) * cycle, sz = (img / 9 - 1) * cycle;
-      RT ox, oy, oz;
-      if constexpr (F32) {  // source relative to its leaf -> relative to the target leaf
+    // lane k: source leaf k of the chunk candidates
+    const int cand = min(32, ee - e0i);
+    // FP32: the shift (ox, oy, oz) from the source leaf's frame into the
+    // target leaf's; FP64: absolute positions, shifted by the periodic image
+    // `img` (the shift is formed per body from it)
+    int n = 0, base = 0, img = 13;
+    float ox = 0, oy = 0, oz = 0;
+    if (lane < cand) {
+      const u32 en = ent[e0i + lane];
+      const int sc = (int)(en & IDX_MASK);
+      img = (int)(en >> IMG_SHIFT);
+      n = count[sc];
+      base = begin[sc];
+      if constexpr (F32) {
+        const double sx = (img % 3 - 1) * cycle, sy = ((img / 3) % 3 - 1) * cycle, sz = (img / 9 - 1) * cycle;
         const double4 CB = xr[sc];
         ox = (float)(CA.x - CB.x - sx);
         oy = (float)(CA.y - CB.y - sy);
         oz = (float)(CA.z - CB.z - sz);
-      } else {
-        ox = -sx;
-        oy = -sy;
-        oz = -sz;
       }
-      for (int b = lane; b < sn; b += 32) {
-        const BT s = bodies[sb + b];
-        BT t;
-        t.x = s.x - ox;
-        t.y = s.y - oy;
-        t.z = s.z - oz;
-        t.w = s.w;
-        stage[so + b] = t;
+    }
+    int inc = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += t;
+    }
+    // the running sums grow, so the leaves that fit are a prefix (at least
+    // one: no leaf exceeds the buffer)
+    const int nl = __popc(__ballot_sync(FULL, lane < cand && inc <= CAP));
+    const int T = __shfl_sync(FULL, inc, nl - 1);
+    const int start = inc - n;  // first staging slot of leaf `lane`
+    base -= start;              // body index = base + staging slot
+    const bool inchunk = lane < nl;
+    __syncthreads();  // the previous chunk's sweep is done with the buffer
+    for (int j0 = wid * 32; j0 < T; j0 += CT * CT_UNROLL) {
+      BT v[CT_UNROLL];
+      int kk[CT_UNROLL];
+#pragma unroll
+      for (int u = 0; u < CT_UNROLL; u++) {
+        const int jb = j0 + u * CT, j = jb + lane;
+        // leaf of slot j: the last leaf starting at or before jb, plus the
+        // leaves starting in (jb, j]
+        const int k0 = __popc(__ballot_sync(FULL, inchunk && start <= jb)) - 1;
+        const unsigned st = __reduce_or_sync(FULL, inchunk && start > jb && start < jb + 32 ? 1u << (start - jb) : 0u);
+        const int k = k0 + __popc(st & (FULL >> (31 - lane)));
+        kk[u] = k;
+        const int bk = __shfl_sync(FULL, base, k);
+        if (j < T) v[u] = bodies[bk + j];
+      }
+#pragma unroll
+      for (int u = 0; u < CT_UNROLL; u++) {
+        const int j = j0 + u * CT + lane;
+        RT sx, sy, sz;
+        if constexpr (F32) {
+          sx = __shfl_sync(FULL, ox, kk[u]);
+          sy = __shfl_sync(FULL, oy, kk[u]);
+          sz = __shfl_sync(FULL, oz, kk[u]);
+        } else {
+          const int im = __shfl_sync(FULL, img, kk[u]);
+          sx = -(im % 3 - 1) * cycle;
+          sy = -((im / 3) % 3 - 1) * cycle;
+          sz = -(im / 9 - 1) * cycle;
+        }
+        if (j < T) {
+          BT t;
+          t.x = v[u].x - sx;
+          t.y = v[u].y - sy;
+          t.z = v[u].z - sz;
+          t.w = v[u].w;
+          stage[j] = t;
+        }
       }
     }
     __syncthreads();
     if (act) {
-      // sources g, g+G, g+2G, ... of the staged chunk, CT_BLOCK at a time
-      // (FP32: one compensated addition per block), four per iteration
-      const int nsrc = g < T ? (T - g + G - 1) / G : 0;
-      const BT *sp = stage + g;
-      for (int c0 = 0; c0 < nsrc; c0 += CT_BLOCK) {
+      // sources [lo, hi) of the staged chunk, CT_BLOCK at a time (FP32: one
+      // compensated addition per block), four per iteration
+      const int lo = g * T / G, hi = (g + 1) * T / G;
+      const BT *sp = stage + lo;
+      for (int c0 = lo; c0 < hi; c0 += CT_BLOCK) {
         RT p[CT_TPT][4];
 #pragma unroll
         for (int u = 0; u < CT_TPT; u++)
 #pragma unroll
           for (int q = 0; q < 4; q++) p[u][q] = 0;
-        const int cend = min(nsrc, c0 + CT_BLOCK);
-        int c = c0;
+        const int cend = min(hi, c0 + CT_BLOCK);
+        int cs = c0;
         auto acc_pair = [&](const BT &sv) {
 #pragma unroll
           for (int u = 0; u < CT_TPT; u++) {
@@ -350,17 +383,17 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
             else pair(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
           }
         };
-        for (; c + 4 <= cend; c += 4) {
-          const BT s0 = sp[0], s1 = sp[G], s2 = sp[2 * G], s3 = sp[3 * G];
-          sp += 4 * G;
+        for (; cs + 4 <= cend; cs += 4) {
+          const BT s0 = sp[0], s1 = sp[1], s2 = sp[2], s3 = sp[3];
+          sp += 4;
           acc_pair(s0);
           acc_pair(s1);
           acc_pair(s2);
           acc_pair(s3);
         }
-        for (; c < cend; c++) {
+        for (; cs < cend; cs++) {
           const BT s0 = sp[0];
-          sp += G;
+          sp += 1;
           acc_pair(s0);
         }
 #pragma unroll
