@@ -7,6 +7,8 @@
 // lanes then read the same body: a broadcast).  Pairs at distance zero are
 // skipped as in the reference.  P2P is the first writer of the outputs, so it
 // stores p and F; L2P adds to them later.
+#include <type_traits>
+
 #include "fmm.cuh"
 
 namespace fmm {
@@ -143,11 +145,27 @@ __device__ __forceinline__ float rsqrt_or_zero(float r2) {
   return y;
 }
 
+// r2 floor of the unchecked pair, in units where the target leaf's radius is
+// in [1, 2): 2^-64, far below the FP32 resolution of that frame (~2^-20), so
+// it changes no resolved pair; two distinct bodies whose FP32 offsets
+// coincide get 1/r = 2^32 instead of an infinity, and q / r^3 stays finite
+// for |q| < 2^32.
+constexpr float NEAR_TINY = 5.421010862427522e-20f;  // 2^-64
+
+// CHECK: pairs at distance zero contribute nothing (3d/kernel.h:131); the
+// unchecked form serves source leaves other than the target's own, where a
+// zero offset can only come from FP32 rounding.
+template <bool CHECK = true>
 __device__ __forceinline__ void pair_f32(float xi, float yi, float zi, const float4 s, float &pot, float &ax,
                                          float &ay, float &az) {
   const float dx = xi - s.x, dy = yi - s.y, dz = zi - s.z;
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float ir = rsqrt_or_zero(r2);
+  float ir;
+  if constexpr (CHECK) {
+    ir = rsqrt_or_zero(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+  } else {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, NEAR_TINY)));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ir) : "f"(r2));
+  }
   const float qir = s.w * ir;
   const float qir3 = qir * ir * ir;
   pot += qir;
@@ -233,6 +251,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int n
 // per two pairs.  Partial sums of the G source parts are combined in a fixed
 // order at the end.  Target leaves up to 256 bodies (ncrit <= 256) use this
 // kernel, larger ones the warp kernels above.
+//
+// FP32 form: coordinates are scaled by a power of two (exact) so that the
+// target leaf's radius is in [1, 2); the target leaf's own bodies (its list
+// always holds it: the acceptance test never accepts a cell with itself) go
+// first, in slots [0, tn) of the first chunk, and only they are swept with
+// the zero-distance check; every group takes its share of both parts, so the
+// warps stay converged.  FP64 form: list order, every pair checked.
 constexpr int CT = 128;           // threads per CTA
 // bodies staged at once: FP32 1536 (7 CTAs per SM, register-bound), FP64
 // 1024 (5 CTAs per SM); tuned on B200 at 1M bodies
@@ -243,7 +268,7 @@ constexpr int CT_TPT = 2;         // targets per thread (register blocking)
 constexpr int CT_BLOCK = 64;      // sources summed in FP32 before one compensated addition
 // 32-body blocks a warp loads before storing them (register-bound)
 template <bool F32>
-constexpr int ct_unroll() { return F32 ? 3 : 1; }
+constexpr int ct_unroll() { return F32 ? 2 : 1; }
 
 template <bool F32>
 struct NearBody;
@@ -276,10 +301,19 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
   const int H = (tn + CT_TPT - 1) / CT_TPT, G = CT / H;
   const int i = tid % H, g = tid / H;
   const bool act = g < G;
+  const double4 CA = xr[c];
+  const int sexp = CA.w > 0 ? max(-100, min(100, ilogb(CA.w))) : 0;
+  const float scale = F32 ? exp2f((float)-sexp) : 1.0f;  // FP32: R * scale in [1, 2)
   BT A[CT_TPT];
 #pragma unroll
-  for (int u = 0; u < CT_TPT; u++) A[u] = act && i + u * H < tn ? bodies[tb + i + u * H] : BT{};
-  const double4 CA = xr[c];
+  for (int u = 0; u < CT_TPT; u++) {
+    A[u] = act && i + u * H < tn ? bodies[tb + i + u * H] : BT{};
+    if constexpr (F32) {
+      A[u].x *= scale;
+      A[u].y *= scale;
+      A[u].z *= scale;
+    }
+  }
   // accumulators: FP64 form plain; FP32 form compensated (s, e) per quantity
   RT sacc[CT_TPT][4], eacc[CT_TPT][4];
 #pragma unroll
@@ -287,13 +321,15 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
 #pragma unroll
     for (int q = 0; q < 4; q++) sacc[u][q] = eacc[u][q] = 0;
   const int eb = off[c], ee = off[c + 1];
+  int pre = F32 ? tn : 0;  // slots [0, pre) of this chunk: the target leaf itself (FP32, first chunk)
   for (int e0i = eb; e0i < ee;) {
     // lane k: source leaf k of the chunk candidates
     const int cand = min(32, ee - e0i);
     // FP32: the shift (ox, oy, oz) from the source leaf's frame into the
-    // target leaf's; FP64: absolute positions, shifted by the periodic image
-    // `img` (the shift is formed per body from it)
+    // target leaf's, scaled; FP64: absolute positions, shifted by the
+    // periodic image `img` (the shift is formed per body from it)
     int n = 0, base = 0, img = 13;
+    bool self = false;  // FP32: the target leaf's own entry (staged first, so here of size 0)
     float ox = 0, oy = 0, oz = 0;
     if (lane < cand) {
       const u32 en = ent[e0i + lane];
@@ -302,11 +338,13 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
       n = count[sc];
       base = begin[sc];
       if constexpr (F32) {
+        self = sc == c && img == 13;
+        if (self) n = 0;
         const double sx = (img % 3 - 1) * cycle, sy = ((img / 3) % 3 - 1) * cycle, sz = (img / 9 - 1) * cycle;
         const double4 CB = xr[sc];
-        ox = (float)(CA.x - CB.x - sx);
-        oy = (float)(CA.y - CB.y - sy);
-        oz = (float)(CA.z - CB.z - sz);
+        ox = (float)(CA.x - CB.x - sx) * scale;  // exact: scale is a power of two
+        oy = (float)(CA.y - CB.y - sy) * scale;
+        oz = (float)(CA.z - CB.z - sz) * scale;
       }
     }
     int inc = n;
@@ -315,25 +353,39 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
       const int t = __shfl_up_sync(FULL, inc, o);
       if (lane >= o) inc += t;
     }
+    inc += pre;
     // the running sums grow, so the leaves that fit are a prefix (at least
-    // one: no leaf exceeds the buffer)
+    // one: no leaf exceeds the buffer less the target leaf)
     const int nl = __popc(__ballot_sync(FULL, lane < cand && inc <= CAP));
     const int T = __shfl_sync(FULL, inc, nl - 1);
     const int start = inc - n;  // first staging slot of leaf `lane`
     base -= start;              // body index = base + staging slot
     const bool inchunk = lane < nl;
+    // the size-0 self entry shares its start with the next leaf
+    const unsigned zm = __ballot_sync(FULL, inchunk && self);
+    const int zs = zm ? __shfl_sync(FULL, start, __ffs(zm) - 1) : -1;
     __syncthreads();  // the previous chunk's sweep is done with the buffer
-    for (int j0 = wid * 32; j0 < T; j0 += CT * CT_UNROLL) {
+    if constexpr (F32) {
+      for (int j = tid; j < pre; j += CT) {  // the target leaf, in slots [0, tn)
+        BT t = bodies[tb + j];
+        t.x *= scale;
+        t.y *= scale;
+        t.z *= scale;
+        stage[j] = t;
+      }
+    }
+    for (int j0 = pre + wid * 32; j0 < T; j0 += CT * CT_UNROLL) {
       BT v[CT_UNROLL];
       int kk[CT_UNROLL];
 #pragma unroll
       for (int u = 0; u < CT_UNROLL; u++) {
         const int jb = j0 + u * CT, j = jb + lane;
         // leaf of slot j: the last leaf starting at or before jb, plus the
-        // leaves starting in (jb, j]
+        // leaves starting in (jb, j] (a size-0 leaf counts as well: the
+        // leaf after it starts at the same slot)
         const int k0 = __popc(__ballot_sync(FULL, inchunk && start <= jb)) - 1;
         const unsigned st = __reduce_or_sync(FULL, inchunk && start > jb && start < jb + 32 ? 1u << (start - jb) : 0u);
-        const int k = k0 + __popc(st & (FULL >> (31 - lane)));
+        const int k = k0 + __popc(st & (FULL >> (31 - lane))) + (zs > jb && zs <= j);
         kk[u] = k;
         const int bk = __shfl_sync(FULL, base, k);
         if (j < T) v[u] = bodies[bk + j];
@@ -354,9 +406,15 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
         }
         if (j < T) {
           BT t;
-          t.x = v[u].x - sx;
-          t.y = v[u].y - sy;
-          t.z = v[u].z - sz;
+          if constexpr (F32) {  // into the target frame, scaled (exact)
+            t.x = fmaf(v[u].x, scale, -sx);
+            t.y = fmaf(v[u].y, scale, -sy);
+            t.z = fmaf(v[u].z, scale, -sz);
+          } else {
+            t.x = v[u].x - sx;
+            t.y = v[u].y - sy;
+            t.z = v[u].z - sz;
+          }
           t.w = v[u].w;
           stage[j] = t;
         }
@@ -364,48 +422,59 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
     }
     __syncthreads();
     if (act) {
-      // sources [lo, hi) of the staged chunk, CT_BLOCK at a time (FP32: one
-      // compensated addition per block), four per iteration
-      const int lo = g * T / G, hi = (g + 1) * T / G;
-      const BT *sp = stage + lo;
-      for (int c0 = lo; c0 < hi; c0 += CT_BLOCK) {
-        RT p[CT_TPT][4];
+      // a slot range, CT_BLOCK sources at a time (FP32: one compensated
+      // addition per block), four per iteration
+      auto sweep = [&](int from, int to, auto check) {
+        constexpr bool CHECK = decltype(check)::value;
+        const BT *sp = stage + from;
+        for (int c0 = from; c0 < to; c0 += CT_BLOCK) {
+          RT p[CT_TPT][4];
 #pragma unroll
-        for (int u = 0; u < CT_TPT; u++)
+          for (int u = 0; u < CT_TPT; u++)
 #pragma unroll
-          for (int q = 0; q < 4; q++) p[u][q] = 0;
-        const int cend = min(hi, c0 + CT_BLOCK);
-        int cs = c0;
-        auto acc_pair = [&](const BT &sv) {
+            for (int q = 0; q < 4; q++) p[u][q] = 0;
+          const int cend = min(to, c0 + CT_BLOCK);
+          int cs = c0;
+          auto acc = [&](const BT &sv) {
 #pragma unroll
-          for (int u = 0; u < CT_TPT; u++) {
-            if constexpr (F32) pair_f32(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
-            else pair(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
+            for (int u = 0; u < CT_TPT; u++) {
+              if constexpr (F32) pair_f32<CHECK>(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
+              else pair(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
+            }
+          };
+          for (; cs + 4 <= cend; cs += 4) {
+            const BT s0 = sp[0], s1 = sp[1], s2 = sp[2], s3 = sp[3];
+            sp += 4;
+            acc(s0);
+            acc(s1);
+            acc(s2);
+            acc(s3);
           }
-        };
-        for (; cs + 4 <= cend; cs += 4) {
-          const BT s0 = sp[0], s1 = sp[1], s2 = sp[2], s3 = sp[3];
-          sp += 4;
-          acc_pair(s0);
-          acc_pair(s1);
-          acc_pair(s2);
-          acc_pair(s3);
-        }
-        for (; cs < cend; cs++) {
-          const BT s0 = sp[0];
-          sp += 1;
-          acc_pair(s0);
-        }
-#pragma unroll
-        for (int u = 0; u < CT_TPT; u++)
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            if constexpr (F32) two_sum_acc(sacc[u][q], eacc[u][q], p[u][q]);  // compensated per block
-            else sacc[u][q] += p[u][q];
+          for (; cs < cend; cs++) {
+            const BT s0 = sp[0];
+            sp += 1;
+            acc(s0);
           }
+#pragma unroll
+          for (int u = 0; u < CT_TPT; u++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              if constexpr (F32) two_sum_acc(sacc[u][q], eacc[u][q], p[u][q]);  // compensated per block
+              else sacc[u][q] += p[u][q];
+            }
+        }
+      };
+      if constexpr (F32) {
+        // the target leaf with the zero-distance check, the others without
+        if (pre) sweep(g * pre / G, (g + 1) * pre / G, std::true_type{});
+        const int rest = T - pre;
+        sweep(pre + g * rest / G, pre + (g + 1) * rest / G, std::false_type{});
+      } else {
+        sweep(g * T / G, (g + 1) * T / G, std::true_type{});
       }
     }
     e0i += nl;
+    pre = 0;
   }
   __syncthreads();
   if (act) {
@@ -420,7 +489,8 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
     for (int gg = 0; gg < G; gg++)
 #pragma unroll
       for (int q = 0; q < 4; q++) r[q] += red[(gg * CT_TPT * H + tid) * 4 + q];
-    out[tb + tid] = make_double4(r[0], -r[1], -r[2], -r[3]);
+    const double s1 = scale, s2 = s1 * s1;  // back to the input units
+    out[tb + tid] = make_double4(r[0] * s1, -r[1] * s2, -r[2] * s2, -r[3] * s2);
   }
 }
 
