@@ -74,7 +74,7 @@ struct DevCounters {
   int overflow;        // a cell at the deepest key level still had > ncrit bodies
   int nleaves;
   unsigned long long n_m2l, n_p2p;  // emitted list entries (may exceed capacity)
-  unsigned long long frontier[2];   // BFS pair frontier sizes (ping-pong)
+  unsigned long long frontier[3];   // BFS pair frontier sizes (rotating over the steps)
   int list_overflow;   // an emission or the frontier exceeded its capacity
   int max_m2l_seg, max_p2p_seg;
   int gcounts[4];      // grouped M2L: residual entries, flagged targets, groups, segments
@@ -129,7 +129,7 @@ struct Handle {
   size_t m2l_cap = 0, p2p_cap = 0;
   Buf m2l_off, m2l_ent, p2p_off, p2p_ent, fill;
   int64_t n_m2l = 0, n_p2p = 0;
-  bool m2l_ordered = false;  // M2L entries of each target in the reference's recording order
+  bool m2l_ordered = false;  // m2l_off/m2l_ent built: per-target CSR in the reference's recording order
 
   // expansions
   Buf M, L;   // double2 [ncells][nterm]
@@ -141,7 +141,7 @@ struct Handle {
   int m2l_units_P = -1;
 
   // grouped M2L (m2l_group.cu)
-  Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg, g_m16, g_slot;
+  Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg, g_m16, g_slot, g_pairs;
   // operator cache: group key -> slot in g_ops, for order op_P and layout
   // op_layout (0: FP64 row blocks, 1: tensor-core FP16 images)
   std::unordered_map<int, int> op_slot;

@@ -37,15 +37,21 @@ __device__ __forceinline__ void img3(int img, int &x, int &y, int &z) {
 }
 
 __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const unsigned long long *nin_p,
-                                            int2 *fout, unsigned long long *nout, u64 fcap, int2 *m2l,
-                                            unsigned long long *nm2l, u64 mcap, int2 *p2p,
+                                            int2 *fout, unsigned long long *nout, unsigned long long *nnext,
+                                            u64 fcap, int2 *m2l, unsigned long long *nm2l, u64 mcap, int2 *p2p,
                                             unsigned long long *np2p, u64 pcap, double theta, double cycle,
                                             int *overflow) {
+  constexpr int NW = TB / 32;
+  __shared__ int s_tot[NW], s_totk[NW];    // every warp's packed list counts and frontier count
+  __shared__ unsigned long long s_base[3];  // the block's M2L, P2P and frontier ranges
   // the producer counts appends past its capacity (to size the retry); only
   // the stored entries may be read
   const u64 nin = min((u64)*nin_p, fcap);
+  // the counter the step after next appends to: nothing reads it any more
+  if (blockIdx.x == 0 && threadIdx.x == 0) *nnext = 0;
   const u64 stride = (u64)gridDim.x * blockDim.x;
-  // every lane of a warp iterates the same number of times (warp-wide appends)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // every thread of a block iterates the same number of times (block-wide appends)
   for (u64 base = (u64)blockIdx.x * blockDim.x; base < nin; base += stride) {
     const u64 idx = base + threadIdx.x;
     const bool act = idx < nin;
@@ -81,32 +87,47 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
       }
     }
     const int packed_i = i | (img << IMG_SHIFT);
-    // one warp scan for the three appends: M2L count in bits 0-5, P2P in
-    // 6-11, frontier pairs in 12-20 (at most 32, 32 and 256 per warp)
-    const int lane = threadIdx.x & 31;
-    const int mine = (kind == 0) | ((kind == 1) << 6) | (nk << 12);
-    int incl = mine;
+    // warp scans for the three appends: M2L count in bits 0-10 and P2P in
+    // 11-21 of one word (at most 256 each per block), frontier pairs in a
+    // second
+    const int mine = (kind == 0) | ((kind == 1) << 11);
+    int incl = mine, inck = nk;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
+      const int t = __shfl_up_sync(0xffffffffu, incl, o), tk = __shfl_up_sync(0xffffffffu, inck, o);
+      if (lane >= o) {
+        incl += t;
+        inck += tk;
+      }
     }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const int excl = incl - mine;
-    unsigned long long res = 0;  // lanes 0, 1, 2 reserve the M2L, P2P and frontier ranges
-    if (lane == 0 && (total & 63)) res = atomicAdd(nm2l, (unsigned long long)(total & 63));
-    if (lane == 1 && ((total >> 6) & 63)) res = atomicAdd(np2p, (unsigned long long)((total >> 6) & 63));
-    if (lane == 2 && (total >> 12)) res = atomicAdd(nout, (unsigned long long)(total >> 12));
-    const unsigned long long bm = __shfl_sync(0xffffffffu, res, 0), bp = __shfl_sync(0xffffffffu, res, 1),
-                             bf = __shfl_sync(0xffffffffu, res, 2);
+    __syncthreads();  // the previous iteration's block ranges are consumed
+    if (lane == 31) {
+      s_tot[wid] = incl;
+      s_totk[wid] = inck;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {  // threads 0, 1, 2 reserve the block's M2L, P2P and frontier ranges
+      int tot = 0;
+      for (int w = 0; w < NW; w++) tot += threadIdx.x == 2 ? s_totk[w] : s_tot[w];
+      const unsigned n = threadIdx.x == 0 ? (tot & 2047) : threadIdx.x == 1 ? ((tot >> 11) & 2047) : tot;
+      unsigned long long *ctr = threadIdx.x == 0 ? nm2l : threadIdx.x == 1 ? np2p : nout;
+      s_base[threadIdx.x] = n ? atomicAdd(ctr, (unsigned long long)n) : 0ull;
+    }
+    __syncthreads();
+    int wpre = 0, wprek = 0;  // earlier warps of the block
+    for (int w = 0; w < wid; w++) {
+      wpre += s_tot[w];
+      wprek += s_totk[w];
+    }
+    const int excl = wpre + incl - mine, exclk = wprek + inck - nk;
     if (kind == 0) {
-      const unsigned long long sl = bm + (excl & 63);
+      const unsigned long long sl = s_base[0] + (excl & 2047);
       if (sl < mcap) m2l[sl] = make_int2(packed_i, j); else *overflow = 1;
     } else if (kind == 1) {
-      const unsigned long long sl = bp + ((excl >> 6) & 63);
+      const unsigned long long sl = s_base[1] + ((excl >> 11) & 2047);
       if (sl < pcap) p2p[sl] = make_int2(packed_i, j); else *overflow = 1;
     } else if (nk > 0) {
-      const unsigned long long sl = bf + (excl >> 12);
+      const unsigned long long sl = s_base[2] + exclk;
       for (int c = 0; c < nk; c++) {
         if (sl + c < fcap) {
           fout[sl + c] = kind == 2 ? make_int2((first + c) | (img << IMG_SHIFT), j) : make_int2(packed_i, first + c);
@@ -135,22 +156,32 @@ __global__ void k_seed(int2 *f, unsigned long long *n, int images, int nsys) {
   }
 }
 
-__global__ void k_zero_u64(unsigned long long *p) { *p = 0; }
-
+// Entries of one target often arrive together (a split emits the children
+// of one cell side by side): lanes with the same target add once.
 __global__ void k_count_tgt(const int2 *e, const unsigned long long *n_p, u64 cap, int *cnt) {
   const u64 n = min((u64)*n_p, cap);
-  for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x)
-    atomicAdd(&cnt[e[k].x & (int)IDX_MASK], 1);
+  for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x) {
+    const int t = e[k].x & (int)IDX_MASK;
+    const unsigned peers = __match_any_sync(__activemask(), t);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&cnt[t], __popc(peers));
+  }
 }
 
 __global__ void k_bucket(const int2 *e, const unsigned long long *n_p, u64 cap, const int *off, int *fill,
                          u32 *ent) {
   const u64 n = min((u64)*n_p, cap);
+  const int lane = threadIdx.x & 31;
   for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x) {
     const int2 v = e[k];
     const int t = v.x & (int)IDX_MASK;
     const u32 img = (u32)v.x >> IMG_SHIFT;
-    const int pos = off[t] + atomicAdd(&fill[t], 1);
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, t);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&fill[t], __popc(peers));
+    base = __shfl_sync(act, base, leader);
+    const int pos = off[t] + base + __popc(peers & ((1u << lane) - 1));
     ent[pos] = (u32)v.y | (img << IMG_SHIFT);
   }
 }
@@ -225,17 +256,11 @@ static void bucket(Handle &h, const int2 *raw, unsigned long long *n_dev, int64_
   FMM_LAUNCH();
 }
 
+// The M2L lists as CSR by target in the reference's order, built from the
+// walk's raw entries when first needed.
 void order_m2l_lists(Handle &h) {
   if (h.m2l_ordered) return;
-  const int64_t n = h.n_m2l;
-  if (n > 0) {
-    u32 *ent = h.m2l_ent.as<u32>(), *tmp = ent + n;
-    FMM_CUDA(cudaMemcpyAsync(tmp, ent, n * sizeof(u32), cudaMemcpyDeviceToDevice, h.stream));
-    k_order_segments<<<grid_for(h.ncells, SEG_WARPS), SEG_WARPS * 32, 0, h.stream>>>(h.m2l_off.as<int>(), h.ncells,
-                                                                                     tmp, ent, h.c_pre.as<int>());
-    h.launches++;
-    FMM_LAUNCH();
-  }
+  bucket(h, h.m2l_raw.as<int2>(), &h.counters.as<DevCounters>()->n_m2l, h.n_m2l, h.m2l_off, h.m2l_ent, true);
   h.m2l_ordered = true;
 }
 
@@ -253,21 +278,23 @@ void build_lists(Handle &h) {
     h.frontier[1].need(h.frontier_cap * sizeof(int2));
     h.m2l_raw.need(h.m2l_cap * sizeof(int2));
     h.p2p_raw.need(h.p2p_cap * sizeof(int2));
-    FMM_CUDA(cudaMemsetAsync(&ctr->n_m2l, 0, sizeof(unsigned long long) * 4, s));
+    FMM_CUDA(cudaMemsetAsync(&ctr->n_m2l, 0, sizeof(unsigned long long) * 5, s));  // list and frontier counts
     FMM_CUDA(cudaMemsetAsync(&ctr->list_overflow, 0, sizeof(int), s));
     k_seed<<<grid_for(std::max(h.nsys, 32), 256), 256, 0, s>>>(h.frontier[0].as<int2>(), &ctr->frontier[0], images,
                                                                 h.nsys);
     h.launches++;
     CellView cv{h.c_xr.as<double4>(), h.c_child.as<int>(), h.c_nchild.as<int>()};
     const int steps = 2 * h.depth + 3;
+    // frontier counters rotate over three words: step st reads word st % 3,
+    // appends to (st + 1) % 3 (zeroed by step st - 1, or above) and zeroes
+    // (st + 2) % 3
     for (int st = 0; st < steps; st++) {
       const int a = st & 1, b = a ^ 1;
-      k_zero_u64<<<1, 1, 0, s>>>(&ctr->frontier[b]);
-      k_walk<<<148 * 8, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[a], h.frontier[b].as<int2>(),
-                                    &ctr->frontier[b], h.frontier_cap, h.m2l_raw.as<int2>(), &ctr->n_m2l, h.m2l_cap,
-                                    h.p2p_raw.as<int2>(), &ctr->n_p2p, h.p2p_cap, h.prm.theta,
-                                    images ? h.prm.cycle : 0.0, &ctr->list_overflow);
-      h.launches += 2;
+      k_walk<<<148 * 8, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[st % 3], h.frontier[b].as<int2>(),
+                                    &ctr->frontier[(st + 1) % 3], &ctr->frontier[(st + 2) % 3], h.frontier_cap,
+                                    h.m2l_raw.as<int2>(), &ctr->n_m2l, h.m2l_cap, h.p2p_raw.as<int2>(), &ctr->n_p2p,
+                                    h.p2p_cap, h.prm.theta, images ? h.prm.cycle : 0.0, &ctr->list_overflow);
+      h.launches++;
       FMM_LAUNCH();
     }
     FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
@@ -281,20 +308,19 @@ void build_lists(Handle &h) {
       h.frontier_cap *= 4;
       continue;
     }
-    if (h.hc.frontier[steps & 1] != 0)
+    if (h.hc.frontier[steps % 3] != 0)
       throw Error{EXAFMM_ERR_STATE, "dual-tree walk did not finish in 2*depth+3 steps"};
     break;
   }
   h.n_m2l = (int64_t)h.hc.n_m2l;
   h.n_p2p = (int64_t)h.hc.n_p2p;
-  // The grouped M2L does not depend on the order of a target's entries, so
-  // the M2L lists are put in the reference's order only when something reads
+  // The grouped M2L reads the raw entries in any order, so the M2L lists
+  // become per-target CSR in the reference's order only when something reads
   // that order: an export, the direct-form kernel, or residual entries.  The
   // P2P lists are ordered always: their order is the near field's summation
   // order, which keeps results reproducible.
-  const bool order_m2l = images > 0 || h.force_direct_m2l;
-  bucket(h, h.m2l_raw.as<int2>(), &ctr->n_m2l, h.n_m2l, h.m2l_off, h.m2l_ent, order_m2l);
-  h.m2l_ordered = order_m2l;
+  h.m2l_ordered = false;
+  if (images > 0 || h.force_direct_m2l) order_m2l_lists(h);
   bucket(h, h.p2p_raw.as<int2>(), &ctr->n_p2p, h.n_p2p, h.p2p_off, h.p2p_ent, true);
 }
 

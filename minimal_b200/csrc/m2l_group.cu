@@ -58,40 +58,46 @@ constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
 // the mixed form's potential error stays within a few percent of FP64's.
 constexpr int TC_FLUSH_EVERY = 16;
 
-__global__ void k_gkeys(int ncells, const int *off, const u32 *ent, const double4 *xr, const int *level, int *ekey,
-                        int *occ, int *gcount, int *counts /*[0] residual entries, [1] flagged targets*/) {
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (c >= ncells) return;
-  const double4 X = xr[c];
-  const int lt = level[c];
-  int grouped = 0, resid = 0;
-  for (int e = off[c] + lane; e < off[c + 1]; e += 32) {
-    const u32 en = ent[e];
-    const int s = (int)(en & IDX_MASK), img = (int)(en >> IMG_SHIFT);
-    int key = -1;
+// Group key of every M2L entry (pairs: the walk's raw (target | img << 26,
+// source) entries, or the CSR lists expanded in order): (level difference,
+// integer offset in units of the smaller radius); -1 for residual entries
+// (images, or outside the key space).  Marks the keys that occur and the
+// targets that have grouped entries.
+__global__ void k_gkeys(long n, const int2 *pairs, const double4 *xr, const int *level, int *ekey, int *occ,
+                        int *gflag, int *counts /*[0] residual entries*/) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int key = -1;
+  if (e < n) {
+    const int2 pr = pairs[e];
+    const int t = pr.x & (int)IDX_MASK, img = (int)((u32)pr.x >> IMG_SHIFT), s = pr.y;
     if (img == 13) {
-      const double4 Y = xr[s];
-      const int dl = lt - level[s];
+      const double4 X = xr[t], Y = xr[s];
+      const int dl = level[t] - level[s];
       const double inv = 1.0 / fmin(X.w, Y.w);  // the quotients are integers up to rounding
       const double vx = rint((X.x - Y.x) * inv), vy = rint((X.y - Y.y) * inv), vz = rint((X.z - Y.z) * inv);
       if (dl >= -KEY_DL && dl < KEY_DL && vx >= -KEY_V && vx < KEY_V && vy >= -KEY_V && vy < KEY_V &&
           vz >= -KEY_V && vz < KEY_V) {
         key = ((dl + KEY_DL) << 18) | (((int)vx + KEY_V) << 12) | (((int)vy + KEY_V) << 6) | ((int)vz + KEY_V);
-        occ[key] = 1;
+        // a few hundred keys (and every target) take many entries: store
+        // only what this SM has not seen set (the L1-cached reads keep the
+        // stores off the few hot L2 lines)
+        if (occ[key] == 0) occ[key] = 1;
+        if (gflag[t] == 0) gflag[t] = 1;
       }
     }
     ekey[e] = key;
-    grouped += key >= 0;
-    resid += key < 0;
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    grouped += __shfl_xor_sync(0xffffffffu, grouped, o);
-    resid += __shfl_xor_sync(0xffffffffu, resid, o);
-  }
-  if (lane == 0) {
-    gcount[c] = grouped;
-    if (resid) atomicAdd(&counts[0], resid);
-    if (grouped) atomicAdd(&counts[1], 1);
+  const int nres = __syncthreads_count(e < n && key < 0);  // one atomic per block
+  if (threadIdx.x == 0 && nres) atomicAdd(&counts[0], nres);
+}
+
+// CSR lists expanded to (target | img << 26, source) pairs in list order.
+__global__ void k_csr_pairs(int ncells, const int *off, const u32 *ent, int2 *pairs) {
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (c >= ncells) return;
+  for (int e = off[c] + lane; e < off[c + 1]; e += 32) {
+    const u32 en = ent[e];
+    pairs[e] = make_int2(c | (int)((en >> IMG_SHIFT) << IMG_SHIFT), (int)(en & IDX_MASK));
   }
 }
 
@@ -224,45 +230,54 @@ __global__ void k_gops16(const int *keys, const int *slots, int P, TcPlan pl, __
 }
 
 // Scaled multipoles split into FP16 hi + lo rows (KP values per cell each).
-__global__ void k_msplit16(long total, int KP, const double *Mt, __half *M16) {
+// Scaled, realified multipole entry k of cell c: M[c][n,m] / R_c^n, k = 2*(tri(n)+m)+{0,1}.
+__device__ __forceinline__ double mscaled(int c, int k, int NT, const double4 *xr, const double2 *M) {
+  if (k >= 2 * NT) return 0.0;
+  const int ci = k >> 1;
+  int n = 0;
+  while (tri(n + 1) <= ci) n++;
+  const double inv = 1.0 / xr[c].w;
+  double s = 1;
+  for (int q = 0; q < n; q++) s *= inv;
+  const double2 m = M[(long)c * NT + ci];
+  return (k & 1 ? m.y : m.x) * s;
+}
+
+// Scaled, realified multipoles: Mt[c][k] (FP64 form).
+__global__ void k_mscale(int ncells, int P, int KP, const double4 *xr, const double2 *M, double *Mt) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= total) return;
+  if (i >= (long)ncells * KP) return;
+  const int c = (int)(i / KP), k = (int)(i - (long)c * KP);
+  Mt[i] = mscaled(c, k, tri(P), xr, M);
+}
+
+// Mixed form: the scaled multipoles split into FP16 hi and lo parts
+// (M16[c][0..KP) hi, M16[c][KP..2KP) lo), written directly.
+__global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const double2 *M, __half *M16) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)ncells * KP) return;
   const long c = i / KP;
   const int k = (int)(i - c * KP);
-  const double v = Mt[i];
+  const double v = mscaled((int)c, k, tri(P), xr, M);
   const __half hi = __double2half(v);
   M16[c * 2 * KP + k] = hi;
   M16[c * 2 * KP + KP + k] = __double2half(v - (double)__half2float(hi));
 }
 
-// Scaled, realified multipoles: Mt[c][2*(tri(n)+m)+{0,1}] = M[c][n,m] / R_c^n.
-__global__ void k_mscale(int ncells, int P, int KP, const double4 *xr, const double2 *M, double *Mt) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int NT = tri(P);
-  if (i >= (long)ncells * KP) return;
-  const int c = (int)(i / KP), k = (int)(i - (long)c * KP);
-  double v = 0;
-  if (k < 2 * NT) {
-    const int ci = k >> 1;
-    int n = 0;
-    while (tri(n + 1) <= ci) n++;
-    const double inv = 1.0 / xr[c].w;
-    double s = 1;
-    for (int q = 0; q < n; q++) s *= inv;
-    const double2 m = M[(long)c * NT + ci];
-    v = (k & 1 ? m.y : m.x) * s;
-  }
-  Mt[i] = v;
-}
-
-__global__ void k_tkeys(int ncells, const int *gcount, const int *level, const int *parent, const int *child,
-                        u64 *keys, u32 *vals) {
+// Tile order of the flagged targets: by level, then child class; counts
+// them (counts[1]).
+__global__ void k_tkeys(int ncells, const int *gflag, const int *level, const int *parent, const int *child,
+                        u64 *keys, u32 *vals, int *counts) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
-  const int pa = parent[c];
-  const int cls = pa < 0 ? 0 : c - child[pa];
-  keys[c] = gcount[c] > 0 ? (u64)(level[c] * 8 + cls) : 255ull;
-  vals[c] = (u32)c;
+  const bool f = c < ncells && gflag[c];
+  if (c < ncells) {
+    const int pa = parent[c];
+    const int cls = pa < 0 ? 0 : c - child[pa];
+    keys[c] = f ? (u64)(level[c] * 8 + cls) : 255ull;
+    vals[c] = (u32)c;
+  }
+  const int nf = __syncthreads_count(f);
+  if (threadIdx.x == 0 && nf) atomicAdd(&counts[1], nf);
 }
 
 __global__ void k_tiles(int ntiles, int tile_n, int nflag, const u32 *sorted, int *tile_tgt, int *tslot) {
@@ -282,30 +297,29 @@ __global__ void k_tiles(int ntiles, int tile_n, int nflag, const u32 *sorted, in
 // order, groups in order within a tile), then write each entry's source into
 // its segment's slot.  A target has at most one entry per group, so every
 // (segment, slot) is written once.
-__global__ void k_gmark(int ncells, const int *off, const int *ekey, const int *gidx, const int *gcount,
-                        const int *tslot, int tile_n, int ngroups, int *mark) {
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (c >= ncells || gcount[c] == 0) return;
-  const long row = (long)(tslot[c] / tile_n) * ngroups;
-  for (int e = off[c] + lane; e < off[c + 1]; e += 32)
-    if (ekey[e] >= 0) mark[row + gidx[ekey[e]]] = 1;
+__global__ void k_gmark(long n, const int2 *pairs, const int *ekey, const int *gidx, const int *tslot, int tile_n,
+                        int ngroups, int *mark) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || ekey[e] < 0) return;
+  const int t = pairs[e].x & (int)IDX_MASK;
+  mark[(long)(tslot[t] / tile_n) * ngroups + gidx[ekey[e]]] = 1;
 }
 
-__global__ void k_gfill(int ncells, const int *off, const u32 *ent, const int *ekey, const int *gidx,
-                        const int *gcount, const int *tslot, int tile_n, int ngroups, const int *segid,
-                        const int *slot_of_gid, int *tg_gid, int *tg_src) {
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (c >= ncells || gcount[c] == 0) return;
-  const int ts = tslot[c];
-  const long row = (long)(ts / tile_n) * ngroups;
-  const int slot = ts % tile_n;
-  for (int e = off[c] + lane; e < off[c + 1]; e += 32) {
-    if (ekey[e] < 0) continue;
-    const int gid = gidx[ekey[e]];
-    const int sg = segid[row + gid];
-    tg_gid[sg] = slot_of_gid[gid];  // the group's operator slot in the cache
-    tg_src[(long)sg * tile_n + slot] = (int)(ent[e] & IDX_MASK);
-  }
+__global__ void k_gfill(long n, const int2 *pairs, const int *ekey, const int *gidx, const int *tslot, int tile_n,
+                        int ngroups, const int *segid, int *tg_src) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || ekey[e] < 0) return;
+  const int2 pr = pairs[e];
+  const int ts = tslot[pr.x & (int)IDX_MASK];
+  const int sg = segid[(long)(ts / tile_n) * ngroups + gidx[ekey[e]]];
+  tg_src[(long)sg * tile_n + ts % tile_n] = pr.y;
+}
+
+// Every marked (tile, group): its segment's operator slot in the cache.
+__global__ void k_seg_gid(long nmark, int ngroups, const int *mark, const int *segid, const int *slot_of_gid,
+                          int *tg_gid) {
+  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nmark && mark[r]) tg_gid[segid[r]] = slot_of_gid[(int)(r % ngroups)];
 }
 
 // First segment of every tile (the exclusive scan at the tile's first
@@ -771,27 +785,49 @@ void m2l_grouped_pass(Handle &h) {
   h.g_used_tc = false;
   if (nent == 0) return;
 
-  // scaled multipoles
-  h.g_mt.need((size_t)C * gp.KP * sizeof(double));
-  k_mscale<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>(C, P, gp.KP, h.c_xr.as<double4>(), h.M.as<double2>(),
-                                                        h.g_mt.as<double>());
-  // keys, occupancy, counts
+  // scaled multipoles: FP64 (DMMA) or FP16 hi/lo (tensor core)
+  if (tcore) {
+    h.g_m16.need((size_t)C * 2 * KP16 * sizeof(__half));
+    k_mscale16<<<grid_for((long)C * KP16, TB), TB, 0, s>>>(C, P, KP16, h.c_xr.as<double4>(), h.M.as<double2>(),
+                                                           h.g_m16.as<__half>());
+  } else {
+    h.g_mt.need((size_t)C * gp.KP * sizeof(double));
+    k_mscale<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>(C, P, gp.KP, h.c_xr.as<double4>(), h.M.as<double2>(),
+                                                          h.g_mt.as<double>());
+  }
+  // the entries: the walk's raw pairs, or the ordered CSR lists expanded
+  // (then the entry index is the CSR position the residual kernel reads)
+  const int2 *pairs = h.m2l_raw.as<int2>();
+  if (h.m2l_ordered) {
+    h.g_pairs.need(nent * sizeof(int2));
+    k_csr_pairs<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
+                                                          h.g_pairs.as<int2>());
+    h.launches++;
+    pairs = h.g_pairs.as<int2>();
+  }
+  // keys, occupancy, flagged targets and their tile order, counts
   h.g_ekey.need(nent * sizeof(int));
   h.g_occ.need((size_t)KEY_SPACE * sizeof(int) * 2 + 64);
   int *occ = h.g_occ.as<int>(), *gidx = occ + KEY_SPACE;
   h.g_cnt.need(C * sizeof(int) * 2 + 64);
-  int *gcount = h.g_cnt.as<int>(), *tslot = gcount + C;
+  int *gflag = h.g_cnt.as<int>(), *tslot = gflag + C;
   DevCounters *ctr = h.counters.as<DevCounters>();
   int *counts = ctr->gcounts;
   FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
+  FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
   FMM_CUDA(cudaMemsetAsync(counts, 0, 4 * sizeof(int), s));
-  k_gkeys<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(), h.c_xr.as<double4>(),
-                                                    h.c_level.as<int>(), h.g_ekey.as<int>(), occ, gcount, counts);
+  k_gkeys<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.c_xr.as<double4>(), h.c_level.as<int>(),
+                                            h.g_ekey.as<int>(), occ, gflag, counts);
   scan_exclusive_int(h, occ, gidx, KEY_SPACE, &counts[2]);
+  h.g_tk.need((size_t)C * 2 * (sizeof(u64) + sizeof(u32)) + 64);
+  u64 *tk = h.g_tk.as<u64>(), *tk2 = tk + C;
+  u32 *tv = (u32 *)(tk2 + C), *tv2 = tv + C;
+  k_tkeys<<<grid_for(C, TB), TB, 0, s>>>(C, gflag, h.c_level.as<int>(), h.c_parent.as<int>(), h.c_child.as<int>(),
+                                         tk, tv, counts);
   FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
   FMM_CUDA(cudaStreamSynchronize(s));
   const int nres = h.hc.gcounts[0], nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
-  h.launches += 3;
+  h.launches += 4;
   if (nres > 0 && !h.m2l_ordered) {  // residual entries are summed in list order: order, then start over
     order_m2l_lists(h);
     m2l_grouped_pass(h);
@@ -855,18 +891,8 @@ void m2l_grouped_pass(Handle &h) {
                                                                         h.g_ops.as<double>());
       h.launches++;
     }
-    if (tcore) {
-      h.g_m16.need((size_t)C * 2 * KP16 * sizeof(__half));
-      k_msplit16<<<grid_for((long)C * KP16, TB), TB, 0, s>>>((long)C * KP16, KP16, h.g_mt.as<double>(),
-                                                             h.g_m16.as<__half>());
-    }
     // tiles of targets
     const int ntiles = (nflag + tile_n - 1) / tile_n;
-    h.g_tk.need((size_t)C * 2 * (sizeof(u64) + sizeof(u32)) + 64);
-    u64 *tk = h.g_tk.as<u64>(), *tk2 = tk + C;
-    u32 *tv = (u32 *)(tk2 + C), *tv2 = tv + C;
-    k_tkeys<<<grid_for(C, TB), TB, 0, s>>>(C, gcount, h.c_level.as<int>(), h.c_parent.as<int>(), h.c_child.as<int>(),
-                                           tk, tv);
     radix_sort_pairs(h, tk, tv, tk2, tv2, C, 0, 8);
     h.g_tile.need((size_t)ntiles * tile_n * sizeof(int) + 64);
     k_tiles<<<grid_for((long)ntiles * tile_n, TB), TB, 0, s>>>(ntiles, tile_n, nflag, tv, h.g_tile.as<int>(), tslot);
@@ -875,8 +901,7 @@ void m2l_grouped_pass(Handle &h) {
     h.g_seg.need((size_t)(nmark + 1) * sizeof(int) * 2);
     int *mark = h.g_seg.as<int>(), *segid = mark + nmark + 1;
     FMM_CUDA(cudaMemsetAsync(mark, 0, (size_t)nmark * sizeof(int), s));
-    k_gmark<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.g_ekey.as<int>(), gidx, gcount, tslot,
-                                                     tile_n, ngroups, mark);
+    k_gmark<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.g_ekey.as<int>(), gidx, tslot, tile_n, ngroups, mark);
     scan_exclusive_int(h, mark, segid, nmark, &counts[3]);
     FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
     FMM_CUDA(cudaStreamSynchronize(s));
@@ -885,9 +910,9 @@ void m2l_grouped_pass(Handle &h) {
     // tg_src first: its rows of tile_n slots stay 16-byte aligned
     int *tg_src = h.g_tg.as<int>(), *tg_gid = tg_src + (size_t)nseg * tile_n, *tg_off = tg_gid + nseg;
     FMM_CUDA(cudaMemsetAsync(tg_src, 0xff, (size_t)nseg * tile_n * sizeof(int), s));
-    k_gfill<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(), h.g_ekey.as<int>(),
-                                                     gidx, gcount, tslot, tile_n, ngroups, segid, d_slot_of, tg_gid,
-                                                     tg_src);
+    k_gfill<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.g_ekey.as<int>(), gidx, tslot, tile_n, ngroups, segid,
+                                              tg_src);
+    k_seg_gid<<<grid_for(nmark, TB), TB, 0, s>>>(nmark, ngroups, mark, segid, d_slot_of, tg_gid);
     k_tg_off<<<grid_for(ntiles + 1, TB), TB, 0, s>>>(ntiles, ngroups, segid, &counts[3], tg_off);
     // contraction
     if (tcore) {
@@ -906,7 +931,7 @@ void m2l_grouped_pass(Handle &h) {
                                                               h.g_ops.as<double>(), h.g_mt.as<double>(),
                                                               h.c_xr.as<double4>(), h.L.as<double2>(), pd);
     }
-    h.launches += 10;
+    h.launches += 11;
     h.g_ntiles = ntiles;
     h.g_ngroups = ngroups;
     h.g_nseg = nseg;
