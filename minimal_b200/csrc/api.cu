@@ -229,7 +229,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
                  &h.lfirst, &h.chain, &h.prebase, &h.scan_tmp, &h.hist, &h.c_begin, &h.c_count, &h.c_child,
                  &h.c_nchild, &h.c_parent, &h.c_level, &h.c_xr, &h.c_pre, &h.c_ref, &h.c_leaf_of_body,
                  &h.leaves, &h.pre_tmp, &h.ctmp, &h.geom, &h.counters, &h.frontier[0], &h.frontier[1],
-                 &h.m2l_raw, &h.p2p_raw, &h.m2l_off, &h.m2l_ent, &h.p2p_off, &h.p2p_ent, &h.fill, &h.M, &h.L,
+                 &h.m2l_raw, &h.m2l_key, &h.p2p_raw, &h.m2l_off, &h.m2l_ent, &h.p2p_off, &h.p2p_ent, &h.fill, &h.M, &h.L,
                  &h.m2l_units, &h.stage, &h.g_mt, &h.g_ekey, &h.g_occ, &h.g_cnt, &h.g_keyof, &h.g_ops,
                  &h.g_tk, &h.g_tile, &h.g_seg, &h.g_tg, &h.g_m16, &h.g_slot, &h.g_pairs, &h.shift_ops, &h.shift_terms};
   for (Buf *b : bufs) b->release();
@@ -238,6 +238,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
       for (int k = 0; k < 2; k++) cudaEventDestroy(h.ev[p][k]);
   if (h.stream) cudaStreamDestroy(h.stream);
   if (h.flags_host) cudaFreeHost(h.flags_host);
+  if (h.keys_host) cudaFreeHost(h.keys_host);
   delete H;
   return EXAFMM_OK;
 }

@@ -76,6 +76,7 @@ struct DevCounters {
   unsigned long long n_m2l, n_p2p;  // emitted list entries (may exceed capacity)
   unsigned long long frontier[3];   // BFS pair frontier sizes (rotating over the steps)
   int list_overflow;   // an emission or the frontier exceeded its capacity
+  int walk_resid;      // M2L entries the walk found without a group key
   int max_m2l_seg, max_p2p_seg;
   int gcounts[4];      // grouped M2L: residual entries, flagged targets, groups, segments
   unsigned long long gfill;
@@ -126,6 +127,7 @@ struct Handle {
   Buf frontier[2];
   size_t frontier_cap = 0;
   Buf m2l_raw, p2p_raw;  // emitted (tgt, src|img) pairs
+  Buf m2l_key;           // group key of each raw M2L entry (-1: none)
   size_t m2l_cap = 0, p2p_cap = 0;
   Buf m2l_off, m2l_ent, p2p_off, p2p_ent, fill;
   int64_t n_m2l = 0, n_p2p = 0;
@@ -147,6 +149,7 @@ struct Handle {
   std::unordered_map<int, int> op_slot;
   int op_P = -1, op_layout = -1;
   std::vector<int> op_host_keys, op_host_slots, op_host_new_keys, op_host_new_slots;
+  int *keys_host = nullptr;  // pinned: the group keys read with the counts
   int g_ntiles = 0, g_ngroups = 0, g_nseg = 0;
   bool g_used_tc = false;
   bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only

@@ -15,13 +15,14 @@
 // source's depth-first pre-order rank (a depth-first walk meets the sources
 // of one target in pre-order, because a target-side split never reorders
 // them).  The result equals getList's per-cell lists entry for entry.
-#include "fmm.cuh"
+#include "group_key.cuh"
 
 namespace fmm {
 
 namespace {
 
 constexpr int TB = 256;
+constexpr int WALK_BLOCKS_PER_SM = 6;    // one wave of the walk (register-bound: 40 per thread)
 constexpr int IMG_SHIFT = 26;             // entry = src | img << 26
 constexpr u32 IDX_MASK = (1u << IMG_SHIFT) - 1;
 
@@ -40,10 +41,13 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
                                             int2 *fout, unsigned long long *nout, unsigned long long *nnext,
                                             u64 fcap, int2 *m2l, unsigned long long *nm2l, u64 mcap, int2 *p2p,
                                             unsigned long long *np2p, u64 pcap, double theta, double cycle,
-                                            int *overflow) {
+                                            int *overflow, int *m2l_key, int *occ, int *gflag, int *nres) {
   constexpr int NW = TB / 32;
   __shared__ int s_tot[NW], s_totk[NW];    // every warp's packed list counts and frontier count
   __shared__ unsigned long long s_base[3];  // the block's M2L, P2P and frontier ranges
+  __shared__ int s_res;                     // M2L entries without a group key
+  if (threadIdx.x == 0) s_res = 0;
+  int res = 0;
   // the producer counts appends past its capacity (to size the retry); only
   // the stored entries may be read
   const u64 nin = min((u64)*nin_p, fcap);
@@ -56,7 +60,7 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
     const u64 idx = base + threadIdx.x;
     const bool act = idx < nin;
     int i = 0, j = 0, img = 13, kind = -1;  // 0 m2l, 1 p2p, 2 split i, 3 split j
-    int nk = 0, first = 0;
+    int nk = 0, first = 0, key = -1;
     if (act) {
       const int2 pr = fin[idx];
       i = pr.x & (int)IDX_MASK;
@@ -74,6 +78,11 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
       const int ci = cv.nchild[i], cj = cv.nchild[j];
       if (R2 > __dmul_rn(rs, rs)) {
         kind = 0;
+        // the group key of the grouped M2L (radii are R0 / 2^level exactly,
+        // so their exponents give the level difference)
+        if (img == 13) key = m2l_group_key(a, b, ilogb(b.w) - ilogb(a.w));
+        if (key >= 0) m2l_mark_key(key, i, occ, gflag);
+        else res++;
       } else if (ci == 0 && cj == 0) {
         kind = 1;
       } else if (cj == 0 || (a.w >= b.w && ci != 0)) {
@@ -122,7 +131,12 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
     const int excl = wpre + incl - mine, exclk = wprek + inck - nk;
     if (kind == 0) {
       const unsigned long long sl = s_base[0] + (excl & 2047);
-      if (sl < mcap) m2l[sl] = make_int2(packed_i, j); else *overflow = 1;
+      if (sl < mcap) {
+        m2l[sl] = make_int2(packed_i, j);
+        m2l_key[sl] = key;
+      } else {
+        *overflow = 1;
+      }
     } else if (kind == 1) {
       const unsigned long long sl = s_base[1] + ((excl >> 11) & 2047);
       if (sl < pcap) p2p[sl] = make_int2(packed_i, j); else *overflow = 1;
@@ -137,6 +151,9 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
       }
     }
   }
+  if (res) atomicAdd_block(&s_res, res);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_res) atomicAdd(nres, s_res);
 }
 
 // Root pairs of the walk: (root, root) of every system of a batch (the roots
@@ -273,6 +290,9 @@ void build_lists(Handle &h) {
   h.m2l_cap = std::max<size_t>(h.m2l_cap, (size_t)C * 200 + 1024);
   h.p2p_cap = std::max<size_t>(h.p2p_cap, (size_t)h.nleaves * 90 + 1024);
   const int images = h.prm.images;
+  h.g_occ.need((size_t)KEY_SPACE * sizeof(int) * 2 + 64);  // key occupancy, then its scan
+  h.g_cnt.need((size_t)C * sizeof(int) * 2 + 64);           // targets with grouped entries, then tile slots
+  int *occ = h.g_occ.as<int>(), *gflag = h.g_cnt.as<int>();
   for (int attempt = 0;; attempt++) {
     h.frontier[0].need(h.frontier_cap * sizeof(int2));
     h.frontier[1].need(h.frontier_cap * sizeof(int2));
@@ -280,6 +300,11 @@ void build_lists(Handle &h) {
     h.p2p_raw.need(h.p2p_cap * sizeof(int2));
     FMM_CUDA(cudaMemsetAsync(&ctr->n_m2l, 0, sizeof(unsigned long long) * 5, s));  // list and frontier counts
     FMM_CUDA(cudaMemsetAsync(&ctr->list_overflow, 0, sizeof(int), s));
+    FMM_CUDA(cudaMemsetAsync(&ctr->walk_resid, 0, sizeof(int), s));
+    // group keys of the M2L entries, and the keys and targets that occur
+    h.m2l_key.need(h.m2l_cap * sizeof(int));
+    FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
+    FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
     k_seed<<<grid_for(std::max(h.nsys, 32), 256), 256, 0, s>>>(h.frontier[0].as<int2>(), &ctr->frontier[0], images,
                                                                 h.nsys);
     h.launches++;
@@ -290,10 +315,11 @@ void build_lists(Handle &h) {
     // (st + 2) % 3
     for (int st = 0; st < steps; st++) {
       const int a = st & 1, b = a ^ 1;
-      k_walk<<<148 * 8, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[st % 3], h.frontier[b].as<int2>(),
+      k_walk<<<148 * WALK_BLOCKS_PER_SM, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[st % 3], h.frontier[b].as<int2>(),
                                     &ctr->frontier[(st + 1) % 3], &ctr->frontier[(st + 2) % 3], h.frontier_cap,
                                     h.m2l_raw.as<int2>(), &ctr->n_m2l, h.m2l_cap, h.p2p_raw.as<int2>(), &ctr->n_p2p,
-                                    h.p2p_cap, h.prm.theta, images ? h.prm.cycle : 0.0, &ctr->list_overflow);
+                                    h.p2p_cap, h.prm.theta, images ? h.prm.cycle : 0.0, &ctr->list_overflow,
+                                    h.m2l_key.as<int>(), occ, gflag, &ctr->walk_resid);
       h.launches++;
       FMM_LAUNCH();
     }

@@ -31,6 +31,7 @@
 
 #include "fmm.cuh"
 #include "harmonics.cuh"
+#include "group_key.cuh"
 #include "m2l_group.h"
 #include "tc.cuh"
 
@@ -43,9 +44,6 @@ namespace {
 constexpr int TB = 256;
 constexpr int IMG_SHIFT = 26;
 constexpr u32 IDX_MASK = (1u << IMG_SHIFT) - 1;
-constexpr int KEY_DL = 4;   // level difference lt - ls in [-4, 3]
-constexpr int KEY_V = 32;   // offset components in [-32, 31]
-constexpr int KEY_SPACE = 8 << 18;
 constexpr int XS = 36;      // padded row stride of the staged multipoles (doubles)
 constexpr int TC_TILE = 128;    // targets per tile on the tensor core (MMA M)
 constexpr int TC_EPI_WARPS = 4; // warps 0-3: epilogue (warp w owns TMEM lanes 32w..32w+31)
@@ -57,38 +55,25 @@ constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
 // to the FP64 local expansion: keeps the FP32 accumulation short enough that
 // the mixed form's potential error stays within a few percent of FP64's.
 constexpr int TC_FLUSH_EVERY = 16;
+// group keys read back with the counts (more take a second read)
+constexpr int OP_KEYS_HOST = 8192;
 
-// Group key of every M2L entry (pairs: the walk's raw (target | img << 26,
-// source) entries, or the CSR lists expanded in order): (level difference,
-// integer offset in units of the smaller radius); -1 for residual entries
-// (images, or outside the key space).  Marks the keys that occur and the
-// targets that have grouped entries.
+// Group key of every M2L entry of the ordered CSR lists (expanded to pairs);
+// marks the keys that occur and the targets that have grouped entries.  (The
+// walk does the same for its raw entries.)
 __global__ void k_gkeys(long n, const int2 *pairs, const double4 *xr, const int *level, int *ekey, int *occ,
-                        int *gflag, int *counts /*[0] residual entries*/) {
+                        int *gflag, int *nres) {
   const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
   int key = -1;
   if (e < n) {
     const int2 pr = pairs[e];
     const int t = pr.x & (int)IDX_MASK, img = (int)((u32)pr.x >> IMG_SHIFT), s = pr.y;
-    if (img == 13) {
-      const double4 X = xr[t], Y = xr[s];
-      const int dl = level[t] - level[s];
-      const double inv = 1.0 / fmin(X.w, Y.w);  // the quotients are integers up to rounding
-      const double vx = rint((X.x - Y.x) * inv), vy = rint((X.y - Y.y) * inv), vz = rint((X.z - Y.z) * inv);
-      if (dl >= -KEY_DL && dl < KEY_DL && vx >= -KEY_V && vx < KEY_V && vy >= -KEY_V && vy < KEY_V &&
-          vz >= -KEY_V && vz < KEY_V) {
-        key = ((dl + KEY_DL) << 18) | (((int)vx + KEY_V) << 12) | (((int)vy + KEY_V) << 6) | ((int)vz + KEY_V);
-        // a few hundred keys (and every target) take many entries: store
-        // only what this SM has not seen set (the L1-cached reads keep the
-        // stores off the few hot L2 lines)
-        if (occ[key] == 0) occ[key] = 1;
-        if (gflag[t] == 0) gflag[t] = 1;
-      }
-    }
+    if (img == 13) key = m2l_group_key(xr[t], xr[s], level[t] - level[s]);
+    if (key >= 0) m2l_mark_key(key, t, occ, gflag);
     ekey[e] = key;
   }
-  const int nres = __syncthreads_count(e < n && key < 0);  // one atomic per block
-  if (threadIdx.x == 0 && nres) atomicAdd(&counts[0], nres);
+  const int nr = __syncthreads_count(e < n && key < 0);  // one atomic per block
+  if (threadIdx.x == 0 && nr) atomicAdd(nres, nr);
 }
 
 // CSR lists expanded to (target | img << 26, source) pairs in list order.
@@ -252,20 +237,33 @@ __global__ void k_mscale(int ncells, int P, int KP, const double4 *xr, const dou
 }
 
 // Mixed form: the scaled multipoles split into FP16 hi and lo parts
-// (M16[c][0..KP) hi, M16[c][KP..2KP) lo), written directly.
-__global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const double2 *M, __half *M16) {
+// (M16[c][0..KP) hi, M16[c][KP..2KP) lo), written directly; one thread per
+// coefficient (n, m) writes its real and imaginary parts.
+__global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const double2 *M, __half2 *M16) {
+  const int half_kp = KP / 2;
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long)ncells * KP) return;
-  const long c = i / KP;
-  const int k = (int)(i - c * KP);
-  const double v = mscaled((int)c, k, tri(P), xr, M);
-  const __half hi = __double2half(v);
-  M16[c * 2 * KP + k] = hi;
-  M16[c * 2 * KP + KP + k] = __double2half(v - (double)__half2float(hi));
+  if (i >= (long)ncells * half_kp) return;
+  const long c = i / half_kp;
+  const int ci = (int)(i - c * half_kp), NT = tri(P);
+  double2 v = make_double2(0, 0);
+  if (ci < NT) {
+    int n = (int)((sqrtf(8.0f * ci + 1.0f) - 1.0f) * 0.5f);  // degree: tri(n) <= ci < tri(n + 1)
+    while (tri(n) > ci) n--;
+    while (tri(n + 1) <= ci) n++;
+    const double inv = 1.0 / xr[c].w;
+    double s = 1, b = inv;  // inv^n
+    for (int e = n; e; e >>= 1, b *= b)
+      if (e & 1) s *= b;
+    const double2 m = M[c * NT + ci];
+    v = make_double2(m.x * s, m.y * s);
+  }
+  const __half hx = __double2half(v.x), hy = __double2half(v.y);
+  __half2 *row = M16 + c * KP;  // KP half2 = 2 KP halves: hi then lo
+  row[ci] = __halves2half2(hx, hy);
+  row[half_kp + ci] = __halves2half2(__double2half(v.x - (double)__half2float(hx)),
+                                     __double2half(v.y - (double)__half2float(hy)));
 }
 
-// Tile order of the flagged targets: by level, then child class; counts
-// them (counts[1]).
 __global__ void k_tkeys(int ncells, const int *gflag, const int *level, const int *parent, const int *child,
                         u64 *keys, u32 *vals, int *counts) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -320,6 +318,12 @@ __global__ void k_seg_gid(long nmark, int ngroups, const int *mark, const int *s
                           int *tg_gid) {
   const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r < nmark && mark[r]) tg_gid[segid[r]] = slot_of_gid[(int)(r % ngroups)];
+}
+
+// The rows of the segments that exist (count on the device) set to -1.
+__global__ void k_fill_rows(int *tg_src, const int *nseg, int tile_n) {
+  const long n = (long)*nseg * tile_n;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) tg_src[i] = -1;
 }
 
 // First segment of every tile (the exclusive scan at the tile's first
@@ -788,45 +792,54 @@ void m2l_grouped_pass(Handle &h) {
   // scaled multipoles: FP64 (DMMA) or FP16 hi/lo (tensor core)
   if (tcore) {
     h.g_m16.need((size_t)C * 2 * KP16 * sizeof(__half));
-    k_mscale16<<<grid_for((long)C * KP16, TB), TB, 0, s>>>(C, P, KP16, h.c_xr.as<double4>(), h.M.as<double2>(),
-                                                           h.g_m16.as<__half>());
+    k_mscale16<<<grid_for((long)C * (KP16 / 2), TB), TB, 0, s>>>(C, P, KP16, h.c_xr.as<double4>(),
+                                                                 h.M.as<double2>(), h.g_m16.as<__half2>());
   } else {
     h.g_mt.need((size_t)C * gp.KP * sizeof(double));
     k_mscale<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>(C, P, gp.KP, h.c_xr.as<double4>(), h.M.as<double2>(),
                                                           h.g_mt.as<double>());
   }
-  // the entries: the walk's raw pairs, or the ordered CSR lists expanded
-  // (then the entry index is the CSR position the residual kernel reads)
+  // the entries and their group keys: the walk's raw pairs with the keys
+  // (and key / target occupancy) it produced, or the ordered CSR lists
+  // expanded (then the entry index is the CSR position the residual kernel
+  // reads) with their keys computed here
   const int2 *pairs = h.m2l_raw.as<int2>();
+  const int *ekey = h.m2l_key.as<int>();
+  int *occ = h.g_occ.as<int>(), *gidx = occ + KEY_SPACE;  // sized by build_lists
+  int *gflag = h.g_cnt.as<int>(), *tslot = gflag + C;
+  DevCounters *ctr = h.counters.as<DevCounters>();
+  int *counts = ctr->gcounts;
+  FMM_CUDA(cudaMemsetAsync(counts, 0, 4 * sizeof(int), s));
   if (h.m2l_ordered) {
     h.g_pairs.need(nent * sizeof(int2));
     k_csr_pairs<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
                                                           h.g_pairs.as<int2>());
-    h.launches++;
     pairs = h.g_pairs.as<int2>();
+    h.g_ekey.need(nent * sizeof(int));
+    FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
+    FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
+    k_gkeys<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.c_xr.as<double4>(), h.c_level.as<int>(),
+                                              h.g_ekey.as<int>(), occ, gflag, &counts[0]);
+    ekey = h.g_ekey.as<int>();
+    h.launches += 2;
   }
-  // keys, occupancy, flagged targets and their tile order, counts
-  h.g_ekey.need(nent * sizeof(int));
-  h.g_occ.need((size_t)KEY_SPACE * sizeof(int) * 2 + 64);
-  int *occ = h.g_occ.as<int>(), *gidx = occ + KEY_SPACE;
-  h.g_cnt.need(C * sizeof(int) * 2 + 64);
-  int *gflag = h.g_cnt.as<int>(), *tslot = gflag + C;
-  DevCounters *ctr = h.counters.as<DevCounters>();
-  int *counts = ctr->gcounts;
-  FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
-  FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
-  FMM_CUDA(cudaMemsetAsync(counts, 0, 4 * sizeof(int), s));
-  k_gkeys<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.c_xr.as<double4>(), h.c_level.as<int>(),
-                                            h.g_ekey.as<int>(), occ, gflag, counts);
+  // dense group ids, the key of each, the flagged targets in tile order;
+  // then one read of the counts and of the keys (for the operator cache)
   scan_exclusive_int(h, occ, gidx, KEY_SPACE, &counts[2]);
+  const long keys_cap = std::max<long>(OP_KEYS_HOST, std::min<long>(KEY_SPACE, nent));
+  h.g_keyof.need((size_t)keys_cap * sizeof(int));
+  k_key_of_gid<<<grid_for(KEY_SPACE, TB), TB, 0, s>>>(occ, gidx, h.g_keyof.as<int>());
   h.g_tk.need((size_t)C * 2 * (sizeof(u64) + sizeof(u32)) + 64);
   u64 *tk = h.g_tk.as<u64>(), *tk2 = tk + C;
   u32 *tv = (u32 *)(tk2 + C), *tv2 = tv + C;
   k_tkeys<<<grid_for(C, TB), TB, 0, s>>>(C, gflag, h.c_level.as<int>(), h.c_parent.as<int>(), h.c_child.as<int>(),
                                          tk, tv, counts);
+  if (!h.keys_host) FMM_CUDA(cudaMallocHost((void **)&h.keys_host, OP_KEYS_HOST * sizeof(int)));
   FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+  FMM_CUDA(cudaMemcpyAsync(h.keys_host, h.g_keyof.p, OP_KEYS_HOST * sizeof(int), cudaMemcpyDeviceToHost, s));
   FMM_CUDA(cudaStreamSynchronize(s));
-  const int nres = h.hc.gcounts[0], nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
+  const int nres = h.m2l_ordered ? h.hc.gcounts[0] : h.hc.walk_resid;
+  const int nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
   h.launches += 4;
   if (nres > 0 && !h.m2l_ordered) {  // residual entries are summed in list order: order, then start over
     order_m2l_lists(h);
@@ -834,9 +847,6 @@ void m2l_grouped_pass(Handle &h) {
     return;
   }
   if (ngroups > 0) {
-    // operators
-    h.g_keyof.need(ngroups * sizeof(int));
-    k_key_of_gid<<<grid_for(KEY_SPACE, TB), TB, 0, s>>>(occ, gidx, h.g_keyof.as<int>());
     // operators: cached per handle by group key (they depend only on the key
     // and P); only keys not seen before are built
     const int layout = tcore ? 1 : 0;
@@ -847,9 +857,12 @@ void m2l_grouped_pass(Handle &h) {
     }
     const size_t op_bytes = tcore ? (size_t)2 * tp.bimg : (size_t)gp.wsize * sizeof(double);
     std::vector<int> &key_of = h.op_host_keys;
-    key_of.resize(ngroups);
-    FMM_CUDA(cudaMemcpyAsync(key_of.data(), h.g_keyof.p, (size_t)ngroups * sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
+    key_of.assign(h.keys_host, h.keys_host + std::min(ngroups, OP_KEYS_HOST));
+    if (ngroups > OP_KEYS_HOST) {  // more keys than the first read carried
+      key_of.resize(ngroups);
+      FMM_CUDA(cudaMemcpy(key_of.data() + OP_KEYS_HOST, h.g_keyof.as<int>() + OP_KEYS_HOST,
+                          (size_t)(ngroups - OP_KEYS_HOST) * sizeof(int), cudaMemcpyDeviceToHost));
+    }
     std::vector<int> &slot_of = h.op_host_slots, &new_keys = h.op_host_new_keys, &new_slots = h.op_host_new_slots;
     slot_of.resize(ngroups);
     new_keys.clear();
@@ -901,17 +914,21 @@ void m2l_grouped_pass(Handle &h) {
     h.g_seg.need((size_t)(nmark + 1) * sizeof(int) * 2);
     int *mark = h.g_seg.as<int>(), *segid = mark + nmark + 1;
     FMM_CUDA(cudaMemsetAsync(mark, 0, (size_t)nmark * sizeof(int), s));
-    k_gmark<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.g_ekey.as<int>(), gidx, tslot, tile_n, ngroups, mark);
+    k_gmark<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, ekey, gidx, tslot, tile_n, ngroups, mark);
     scan_exclusive_int(h, mark, segid, nmark, &counts[3]);
-    FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
-    const int nseg = h.hc.gcounts[3];
+    // segment tables sized for every (tile, group) pair when that is small
+    // (no read of the segment count), else read the count
+    long nseg = nmark;
+    if ((size_t)nmark * (tile_n + 1) * sizeof(int) > ((size_t)1 << 30)) {
+      FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+      FMM_CUDA(cudaStreamSynchronize(s));
+      nseg = h.hc.gcounts[3];
+    }
     h.g_tg.need(((size_t)nseg * (tile_n + 1) + ntiles + 2) * sizeof(int));
     // tg_src first: its rows of tile_n slots stay 16-byte aligned
     int *tg_src = h.g_tg.as<int>(), *tg_gid = tg_src + (size_t)nseg * tile_n, *tg_off = tg_gid + nseg;
-    FMM_CUDA(cudaMemsetAsync(tg_src, 0xff, (size_t)nseg * tile_n * sizeof(int), s));
-    k_gfill<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.g_ekey.as<int>(), gidx, tslot, tile_n, ngroups, segid,
-                                              tg_src);
+    k_fill_rows<<<148 * 4, TB, 0, s>>>(tg_src, &counts[3], tile_n);  // absent targets: -1
+    k_gfill<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, ekey, gidx, tslot, tile_n, ngroups, segid, tg_src);
     k_seg_gid<<<grid_for(nmark, TB), TB, 0, s>>>(nmark, ngroups, mark, segid, d_slot_of, tg_gid);
     k_tg_off<<<grid_for(ntiles + 1, TB), TB, 0, s>>>(ntiles, ngroups, segid, &counts[3], tg_off);
     // contraction
@@ -934,10 +951,10 @@ void m2l_grouped_pass(Handle &h) {
     h.launches += 11;
     h.g_ntiles = ntiles;
     h.g_ngroups = ngroups;
-    h.g_nseg = nseg;
+    h.g_nseg = nseg;  // an upper bound unless it was read
     FMM_LAUNCH();
   }
-  if (nres > 0) m2l_residual(h, h.g_ekey.as<int>());
+  if (nres > 0) m2l_residual(h, ekey);
 }
 
 }  // namespace fmm
