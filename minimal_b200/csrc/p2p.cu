@@ -265,7 +265,7 @@ template <bool F32>
 constexpr int ct_cap() { return F32 ? 1536 : 1024; }
 constexpr int CT_MAXTGT = 256;    // target-leaf bodies: two per thread
 constexpr int CT_TPT = 2;         // targets per thread (register blocking)
-constexpr int CT_BLOCK = 64;      // sources summed in FP32 before one compensated addition
+constexpr int CT_BLOCK = 128;     // sources summed in FP32 before one compensated addition
 // 32-body blocks a warp loads before storing them (register-bound)
 template <bool F32>
 constexpr int ct_unroll() { return F32 ? 2 : 1; }
@@ -422,8 +422,7 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
     }
     __syncthreads();
     if (act) {
-      // a slot range, CT_BLOCK sources at a time (FP32: one compensated
-      // addition per block), four per iteration
+      // FP64: a slot range, CT_BLOCK sources at a time, four per iteration
       auto sweep = [&](int from, int to, auto check) {
         constexpr bool CHECK = decltype(check)::value;
         const BT *sp = stage + from;
@@ -465,10 +464,51 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
         }
       };
       if constexpr (F32) {
-        // the target leaf with the zero-distance check, the others without
-        if (pre) sweep(g * pre / G, (g + 1) * pre / G, std::true_type{});
-        const int rest = T - pre;
-        sweep(pre + g * rest / G, pre + (g + 1) * rest / G, std::false_type{});
+        // the target leaf (its own few slots per thread) with the
+        // zero-distance check, summed into the first block of the others
+        // (without the check)
+        RT p[CT_TPT][4];
+#pragma unroll
+        for (int u = 0; u < CT_TPT; u++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) p[u][q] = 0;
+        auto acc = [&](const BT &sv, auto check) {
+          constexpr bool CHECK = decltype(check)::value;
+#pragma unroll
+          for (int u = 0; u < CT_TPT; u++)
+            pair_f32<CHECK>(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
+        };
+        auto flush = [&]() {  // one compensated addition per block
+#pragma unroll
+          for (int u = 0; u < CT_TPT; u++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              two_sum_acc(sacc[u][q], eacc[u][q], p[u][q]);
+              p[u][q] = 0;
+            }
+        };
+        for (int cs = g * pre / G, ce = (g + 1) * pre / G; cs < ce; cs++) acc(stage[cs], std::true_type{});
+        const int rest = T - pre, from = pre + g * rest / G, to = pre + (g + 1) * rest / G;
+        const BT *sp = stage + from;
+        for (int c0 = from; c0 < to; c0 += CT_BLOCK) {
+          const int cend = min(to, c0 + CT_BLOCK);
+          int cs = c0;
+          for (; cs + 4 <= cend; cs += 4) {
+            const BT s0 = sp[0], s1 = sp[1], s2 = sp[2], s3 = sp[3];
+            sp += 4;
+            acc(s0, std::false_type{});
+            acc(s1, std::false_type{});
+            acc(s2, std::false_type{});
+            acc(s3, std::false_type{});
+          }
+          for (; cs < cend; cs++) {
+            const BT s0 = sp[0];
+            sp += 1;
+            acc(s0, std::false_type{});
+          }
+          flush();
+        }
+        if (from == to && pre) flush();  // only the target leaf's slots
       } else {
         sweep(g * T / G, (g + 1) * T / G, std::true_type{});
       }

@@ -67,19 +67,32 @@ __global__ void k_bounds_partial(const double4 *in, long n, double *part) {
   }
 }
 
+// Min/max of the block's threads into thread 0 (exact operations: the
+// reduction order cannot change the result).
+__device__ void block_minmax(double lo[3], double hi[3]) {
+  __shared__ double s[TB / 32][6];
+  for (int o = 16; o > 0; o >>= 1)
+    for (int d = 0; d < 3; d++) {
+      lo[d] = dmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = dmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int d = 0; d < 3; d++) { s[w][d] = lo[d]; s[w][3 + d] = hi[d]; }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 1; k < TB / 32; k++)
+      for (int d = 0; d < 3; d++) { lo[d] = dmin(s[k][d], lo[d]); hi[d] = dmax(s[k][3 + d], hi[d]); }
+}
+
 // getBounds (3d/build_tree.h:7-21): centre = (max+min)/2, R0 = largest
 // half-extent about that centre, times 1.00001.
 __global__ void k_bounds_final(const double *part, int nb, RootGeom *g) {
-  // min/max are exact, so the reduction order cannot change the result
-  __shared__ double s[TB][6];
   double lo[3] = {part[0], part[1], part[2]}, hi[3] = {part[3], part[4], part[5]};
   for (int k = threadIdx.x; k < nb; k += blockDim.x)
     for (int d = 0; d < 3; d++) { lo[d] = dmin(part[6 * k + d], lo[d]); hi[d] = dmax(part[6 * k + 3 + d], hi[d]); }
-  for (int d = 0; d < 3; d++) { s[threadIdx.x][d] = lo[d]; s[threadIdx.x][3 + d] = hi[d]; }
-  __syncthreads();
+  block_minmax(lo, hi);
   if (threadIdx.x != 0) return;
-  for (int k = 1; k < blockDim.x; k++)
-    for (int d = 0; d < 3; d++) { lo[d] = dmin(s[k][d], lo[d]); hi[d] = dmax(s[k][3 + d], hi[d]); }
   double R0 = 0;
   for (int d = 0; d < 3; d++) {
     g->X0[d] = __ddiv_rn(__dadd_rn(hi[d], lo[d]), 2.0);
@@ -92,7 +105,6 @@ __global__ void k_bounds_final(const double *part, int nb, RootGeom *g) {
 // Bounds of every system of a batch: one block per system, then the same
 // getBounds arithmetic as k_bounds_final.
 __global__ void k_bounds_systems(const double4 *in, const long long *off, RootGeom *geom) {
-  __shared__ double s[TB][6];
   const long b0 = off[blockIdx.x], b1 = off[blockIdx.x + 1];
   double lo[3] = {in[b0].x, in[b0].y, in[b0].z}, hi[3] = {lo[0], lo[1], lo[2]};
   for (long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
@@ -100,11 +112,8 @@ __global__ void k_bounds_systems(const double4 *in, const long long *off, RootGe
     lo[0] = dmin(b.x, lo[0]); lo[1] = dmin(b.y, lo[1]); lo[2] = dmin(b.z, lo[2]);
     hi[0] = dmax(b.x, hi[0]); hi[1] = dmax(b.y, hi[1]); hi[2] = dmax(b.z, hi[2]);
   }
-  for (int d = 0; d < 3; d++) { s[threadIdx.x][d] = lo[d]; s[threadIdx.x][3 + d] = hi[d]; }
-  __syncthreads();
+  block_minmax(lo, hi);
   if (threadIdx.x != 0) return;
-  for (int k = 1; k < blockDim.x; k++)
-    for (int d = 0; d < 3; d++) { lo[d] = dmin(s[k][d], lo[d]); hi[d] = dmax(s[k][3 + d], hi[d]); }
   RootGeom *g = geom + blockIdx.x;
   double R0 = 0;
   for (int d = 0; d < 3; d++) {
@@ -137,10 +146,11 @@ __global__ void k_keys(const double4 *in, long n, const RootGeom *geom, const lo
   double cx = g->X0[0], cy = g->X0[1], cz = g->X0[2];
   const double R0 = g->R0;
   u64 key = (u64)sys;
+  double r = R0;
   for (int l = 0; l < D; l++) {
     const int ox = b.x > cx, oy = b.y > cy, oz = b.z > cz;
     key = (key << 3) | (u64)(ox | (oy << 1) | (oz << 2));
-    const double r = __ddiv_rn(R0, (double)(1 << (l + 1)));
+    r = __dmul_rn(r, 0.5);  // R0 / 2^(l+1): halving is the correctly rounded quotient
     cx = __dadd_rn(cx, ox ? r : -r);
     cy = __dadd_rn(cy, oy ? r : -r);
     cz = __dadd_rn(cz, oz ? r : -r);
@@ -230,9 +240,10 @@ __global__ void k_cells(const u64 *keys, long n, int D, int ncrit, const int *lf
   const RootGeom *gs = g + (long)(key >> (3 * D));  // the body's system
   const double R0 = gs->R0;
   double cx = gs->X0[0], cy = gs->X0[1], cz = gs->X0[2];
+  double r = R0;  // R0 / 2^l, halved exactly level by level
   for (int l = 0; l < lf; l++) {  // centre of the level-lf cell holding body i
     const int o = (int)((key >> (3 * (D - 1 - l))) & 7);
-    const double r = __ddiv_rn(R0, (double)(1 << (l + 1)));
+    r = __dmul_rn(r, 0.5);
     cx = __dadd_rn(cx, (o & 1) ? r : -r);
     cy = __dadd_rn(cy, (o & 2) ? r : -r);
     cz = __dadd_rn(cz, (o & 4) ? r : -r);
@@ -253,12 +264,12 @@ __global__ void k_cells(const u64 *keys, long n, int D, int ncrit, const int *lf
     t.count[p] = (int)(e - i);
     t.level[p] = l;
     t.parent[p] = parent;
-    t.xr[p] = make_double4(cx, cy, cz, __ddiv_rn(R0, (double)(1 << l)));
+    t.xr[p] = make_double4(cx, cy, cz, r);
     atomicAdd(&ctr->level_count[l], 1);
     if (parent >= 0) atomicAdd(&t.nchild[parent], 1);
     if (l < D) {  // next chain member is the first child: advance the centre
       const int o = (int)((key >> (3 * (D - 1 - l))) & 7);
-      const double r = __ddiv_rn(R0, (double)(1 << (l + 1)));
+      r = __dmul_rn(r, 0.5);
       cx = __dadd_rn(cx, (o & 1) ? r : -r);
       cy = __dadd_rn(cy, (o & 2) ? r : -r);
       cz = __dadd_rn(cz, (o & 4) ? r : -r);
