@@ -93,6 +93,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m(const int *leaves, int nleav
 // the FP32 copy the near field uses), same lock-step generator in float;
 // expansions stay FP64 in memory.
 __constant__ float c_recip_f[2 * EXAFMM_MAX_P + 4];
+#ifndef P2M_TRANSPOSE
+#define P2M_TRANSPOSE 1
+#endif
+#ifndef L2P_F32_MIN_BLOCKS
+#define L2P_F32_MIN_BLOCKS 4  // the unrolled L2P would otherwise hold all of L in registers
+#endif
+// orders with unrolled FP32 P2M / L2P kernels (others take the runtime-order ones)
+#define EXAFMM_UNROLLED_ORDERS(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
 struct SphF {
   float r, c, s, inv_s;
@@ -121,27 +129,33 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-template <bool WITH_DY, class F>
-__device__ __forceinline__ void regular_all_f(int P, const SphF &g, float2 e1, F f) {
+// PT > 0: the order as a compile-time constant -- the loops unroll and the
+// integer factors and reciprocals become immediates; PT = 0: runtime order Prt.
+template <int PT, bool WITH_DY, class F>
+__device__ __forceinline__ void regular_all_f(int Prt, const SphF &g, float2 e1, F f) {
+  const int P = PT > 0 ? PT : Prt;
+  auto rcp = [](int k) { return PT > 0 ? 1.0f / (float)k : c_recip_f[k]; };
   float2 em = make_float2(1.f, 0.f);
   float pmm = 1.f, odd = 1.f, cm = 1.f;
+#pragma unroll
   for (int m = 0; m < P; m++) {
     float p = pmm, p1 = 0.f, cn = cm;
+#pragma unroll
     for (int n = m; n < P; n++) {
       const float pn1 =
-          n == m ? g.c * (2 * m + 1) * p : (g.c * (2 * n + 1) * p - (n + m) * p1) * c_recip_f[n - m + 1];
+          n == m ? g.c * (float)(2 * m + 1) * p : (g.c * (float)(2 * n + 1) * p - (float)(n + m) * p1) * rcp(n - m + 1);
       const float2 Y = make_float2(em.x * cn * p, em.y * cn * p);
       float2 dY = make_float2(0.f, 0.f);
       if (WITH_DY) {
-        const float d = cn * ((n - m + 1) * pn1 - (n + 1) * g.c * p) * g.inv_s;
+        const float d = cn * ((float)(n - m + 1) * pn1 - (float)(n + 1) * g.c * p) * g.inv_s;
         dY = make_float2(em.x * d, em.y * d);
       }
       f(n, m, Y, dY);
       p1 = p;
       p = pn1;
-      cn *= -g.r * c_recip_f[n + 1 + m];
+      cn *= -g.r * rcp(n + 1 + m);
     }
-    cm *= -g.r * c_recip_f[2 * m + 2] * c_recip_f[2 * m + 1];
+    cm *= -g.r * rcp(2 * m + 2) * rcp(2 * m + 1);
     pmm = -pmm * odd * g.s;
     odd += 2.f;
     em = cmulf(em, e1);
@@ -150,9 +164,11 @@ __device__ __forceinline__ void regular_all_f(int P, const SphF &g, float2 e1, F
 
 // P2M in FP32: lane per body, each coefficient reduced over the warp by a
 // float butterfly, chunks of 32 bodies summed in FP64.
+template <int PT>
 __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int nleaves, const int *begin,
-                                                        const int *count, const float4 *srcf, double2 *M, int P) {
+                                                        const int *count, const float4 *srcf, double2 *M, int Prt) {
   extern __shared__ double2 sh[];
+  const int P = PT > 0 ? PT : Prt;
   const int nt = tri(P);
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * WARPS + wid;
@@ -166,7 +182,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int n
     const bool ok = t + lane < nb;
     const float4 B = ok ? srcf[b0 + t + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
     const SphF g = sph_of_f(B.x, B.y, B.z);
-    regular_all_f<false>(P, g, make_float2(g.e.x, -g.e.y), [&](int n, int m, float2 Y, float2) {
+    regular_all_f<PT, false>(P, g, make_float2(g.e.x, -g.e.y), [&](int n, int m, float2 Y, float2) {
       float x = B.w * Y.x, y = B.w * Y.y;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -183,12 +199,55 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int n
   for (int k = lane; k < nt; k += 32) M[(long)c * nt + k] = acc[k];
 }
 
+// P2M in FP32 for a compile-time order: each lane writes its body's q Y
+// terms to shared memory, then lane k sums term k over the 32 bodies (rows
+// padded to 33 entries: conflict-free), and the chunk sums are added in FP64.
+template <int PT>
+__global__ void __launch_bounds__(WARPS * 32) k_p2m_f32t(const int *leaves, int nleaves, const int *begin,
+                                                         const int *count, const float4 *srcf, double2 *M) {
+  constexpr int NT = PT * (PT + 1) / 2, ROW = 33;
+  extern __shared__ double2 sh[];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * WARPS + wid;
+  if (w >= nleaves) return;
+  double2 *acc = sh + wid * NT;
+  float2 *buf = (float2 *)(sh + WARPS * NT) + wid * NT * ROW;
+  for (int k = lane; k < NT; k += 32) acc[k] = make_double2(0, 0);
+  const int c = leaves[w];
+  const int b0 = begin[c], nb = count[c];
+  for (int t = 0; t < nb; t += 32) {
+    const bool ok = t + lane < nb;
+    const float4 B = ok ? srcf[b0 + t + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const SphF g = sph_of_f(B.x, B.y, B.z);
+    __syncwarp();
+    regular_all_f<PT, false>(PT, g, make_float2(g.e.x, -g.e.y), [&](int n, int m, float2 Y, float2) {
+      buf[(tri(n) + m) * ROW + lane] = make_float2(B.w * Y.x, B.w * Y.y);
+    });
+    __syncwarp();
+    for (int k = lane; k < NT; k += 32) {
+      float sx = 0.f, sy = 0.f;
+#pragma unroll 8
+      for (int b = 0; b < 32; b++) {
+        const float2 v = buf[k * ROW + b];
+        sx += v.x;
+        sy += v.y;
+      }
+      acc[k].x += (double)sx;
+      acc[k].y += (double)sy;
+    }
+  }
+  __syncwarp();
+  for (int k = lane; k < NT; k += 32) M[(long)c * NT + k] = acc[k];
+}
+
 // L2P in FP32: lane per body, the leaf's local expansion broadcast from
 // shared memory as float; p and F added to the FP64 results.
-__global__ void __launch_bounds__(WARPS * 32) k_l2p_f32(const int *leaves, int nleaves, const int *begin,
+template <int PT>
+__global__ void __launch_bounds__(WARPS * 32, L2P_F32_MIN_BLOCKS) k_l2p_f32(const int *leaves, int nleaves, const int *begin,
                                                         const int *count, const float4 *srcf, const double2 *L,
-                                                        double4 *out, int P) {
+                                                        double4 *out, int Prt) {
   extern __shared__ float2 shf[];
+  const int P = PT > 0 ? PT : Prt;
   const int nt = tri(P);
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * WARPS + wid;
@@ -207,16 +266,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_l2p_f32(const int *leaves, int n
     const float4 B = ok ? srcf[b] : make_float4(1.f, 0.f, 0.f, 0.f);
     const SphF g = sph_of_f(B.x, B.y, B.z);
     float pot = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
-    regular_all_f<true>(P, g, g.e, [&](int n, int m, float2 Y, float2 dY) {
+    regular_all_f<PT, true>(P, g, g.e, [&](int n, int m, float2 Y, float2 dY) {
       const float2 l = Lc[tri(n) + m];
       const float w2 = m == 0 ? 1.f : 2.f;
       const float re = l.x * Y.x - l.y * Y.y;
       const float red = l.x * dY.x - l.y * dY.y;
       const float rei = -(l.x * Y.y + l.y * Y.x);
       pot += w2 * re;
-      s0 += w2 * re * n;
+      s0 += w2 * re * (float)n;
       s1 += w2 * red;
-      s2 += w2 * rei * m;
+      s2 += w2 * rei * (float)m;
     });
     s0 = g.r != 0.f ? s0 / g.r : 0.f;
     if (ok) {
@@ -385,9 +444,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_l2p(const int *leaves, int nleav
       const double red = l.x * dY.x - l.y * dY.y;     // Re(L dY)
       const double rei = -(l.x * Y.y + l.y * Y.x);    // Re(L Y i)
       pot += w2 * re;
-      s0 += w2 * re * n;
+      s0 += w2 * re * (float)n;
       s1 += w2 * red;
-      s2 += w2 * rei * m;
+      s2 += w2 * rei * (float)m;
     });
     s0 = g.r != 0 ? s0 / g.r : 0.0;
     if (ok) {
@@ -425,8 +484,14 @@ void expansions_set_attributes() {
   FMM_CUDA(cudaMemcpyToSymbol(c_recip_f, rf, sizeof(rf)));
   cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2p, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_p2m_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_l2p_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+#define EXAFMM_F32_ATTR(p)                                                                     \
+  cudaFuncSetAttribute(k_p2m_f32<p>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
+  cudaFuncSetAttribute(k_p2m_f32t<p>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
+  cudaFuncSetAttribute(k_l2p_f32<p>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_p2m_f32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_l2p_f32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  EXAFMM_UNROLLED_ORDERS(EXAFMM_F32_ATTR)
+#undef EXAFMM_F32_ATTR
   cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
@@ -493,9 +558,27 @@ void upward_pass(Handle &h) {
   h.L.need((size_t)h.ncells * nt * sizeof(double2));
   if (h.prm.precision == EXAFMM_MIXED) {
     make_srcf(h);
-    k_p2m_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
-        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.srcf.as<float4>(),
-        h.M.as<double2>(), P);
+    const dim3 grid(grid_for(h.nleaves, WARPS)), block(WARPS * 32);
+    const size_t sm = WARPS * nt * sizeof(double2);
+    auto args = [&](auto kernel) {
+      kernel<<<grid, block, sm, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
+                                     h.srcf.as<float4>(), h.M.as<double2>(), P);
+    };
+    const size_t smt = WARPS * nt * (sizeof(double2) + 33 * sizeof(float2));
+    auto argst = [&](auto kernel) {
+      kernel<<<grid, block, smt, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
+                                      h.srcf.as<float4>(), h.M.as<double2>());
+    };
+    switch (P) {
+#define EXAFMM_P2M_CASE(p) \
+  case p:                  \
+    if (P2M_TRANSPOSE && p <= 12) argst(k_p2m_f32t<p>); else args(k_p2m_f32<p>); \
+    break;
+      EXAFMM_UNROLLED_ORDERS(EXAFMM_P2M_CASE)
+#undef EXAFMM_P2M_CASE
+      default:
+        args(k_p2m_f32<0>);
+    }
   } else {
     k_p2m<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
         h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
@@ -530,9 +613,22 @@ void downward_pass(Handle &h) {
   }
   if (h.prm.precision == EXAFMM_MIXED) {
     make_srcf(h);
-    k_l2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(float2), s>>>(
-        h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.srcf.as<float4>(),
-        h.L.as<double2>(), h.out.as<double4>(), P);
+    const dim3 grid(grid_for(h.nleaves, WARPS)), block(WARPS * 32);
+    const size_t sm = WARPS * nt * sizeof(float2);
+    auto args = [&](auto kernel) {
+      kernel<<<grid, block, sm, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
+                                     h.srcf.as<float4>(), h.L.as<double2>(), h.out.as<double4>(), P);
+    };
+    switch (P) {
+#define EXAFMM_L2P_CASE(p) \
+  case p:                  \
+    args(k_l2p_f32<p>);    \
+    break;
+      EXAFMM_UNROLLED_ORDERS(EXAFMM_L2P_CASE)
+#undef EXAFMM_L2P_CASE
+      default:
+        args(k_l2p_f32<0>);
+    }
   } else {
     k_l2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, WARPS * nt * sizeof(double2), s>>>(
         h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
