@@ -162,21 +162,37 @@ __global__ void k_keys(const double4 *in, long n, const RootGeom *geom, const lo
 // Level-l prefix of a key: the system index and the first l octant digits.
 __device__ __forceinline__ u64 prefix_of(u64 key, int D, int l) { return key >> (3 * (D - l)); }
 
-// First index in [lo, hi) whose level-l prefix exceeds p (keys sorted).
+// First index in [lo, hi) whose level-l prefix exceeds p (keys sorted, and
+// keys[lo] has a prefix <= p): a galloping search up from lo, then a binary
+// search in the last step -- runs near the leaves are short, so this takes
+// about twice the log of the run length instead of the log of the range.
 __device__ long upper_run(const u64 *keys, long lo, long hi, int D, int l, u64 p) {
-  while (lo < hi) {
-    long mid = (lo + hi) >> 1;
-    if (prefix_of(keys[mid], D, l) > p) hi = mid; else lo = mid + 1;
+  long a = lo, step = 1;
+  while (a + step < hi && prefix_of(keys[a + step], D, l) <= p) {
+    a += step;
+    step <<= 1;
   }
-  return lo;
+  long L = a + 1, H = a + step < hi ? a + step : hi;  // the answer is in [L, H]
+  while (L < H) {
+    const long mid = (L + H) >> 1;
+    if (prefix_of(keys[mid], D, l) > p) H = mid; else L = mid + 1;
+  }
+  return L;
 }
-// First index in [lo, hi) whose level-l prefix is >= p.
+// First index in [lo, hi) whose level-l prefix is >= p (keys[hi], when it
+// exists, has a prefix >= p): galloping down from hi.
 __device__ long lower_run(const u64 *keys, long lo, long hi, int D, int l, u64 p) {
-  while (lo < hi) {
-    long mid = (lo + hi) >> 1;
-    if (prefix_of(keys[mid], D, l) >= p) hi = mid; else lo = mid + 1;
+  long b = hi, step = 1;
+  while (b - step >= lo && prefix_of(keys[b - step], D, l) >= p) {
+    b -= step;
+    step <<= 1;
   }
-  return lo;
+  long L = b - step < lo ? lo : b - step + 1, H = b;  // the answer is in [L, H]
+  while (L < H) {
+    const long mid = (L + H) >> 1;
+    if (prefix_of(keys[mid], D, l) >= p) H = mid; else L = mid + 1;
+  }
+  return L;
 }
 
 // Shallowest level whose key prefix at i differs from i-1 (D+1: same key).
@@ -189,8 +205,32 @@ __device__ __forceinline__ int first_level(const u64 *keys, long i, int D) {
   return D - h / 3;
 }
 
+// Shallowest level whose key prefixes of x and y differ (D+1: none).
+__device__ __forceinline__ int diff_level(u64 x, u64 y, int D) {
+  const u64 d = x ^ y;
+  if (d == 0) return D + 1;
+  const int h = 63 - __clzll((long long)d);
+  if (h >= 3 * D) return 0;  // another system
+  return D - h / 3;
+}
+
+// Bodies from i on (i included) in i's level-l run, counted up to cap.
+__device__ long run_ahead(const u64 *keys, long i, long n, int D, int l, u64 p, long cap) {
+  const long last = i + cap < n ? i + cap : n;
+  if (last == i + cap && prefix_of(keys[last - 1], D, l) == p) return cap;
+  long L = i + 1, H = last;  // the run ends in [L, H]
+  while (L < H) {
+    const long mid = (L + H) >> 1;
+    if (prefix_of(keys[mid], D, l) > p) H = mid; else L = mid + 1;
+  }
+  return L - i;
+}
+
 // Number of cells whose first body is sorted position i (a chain of nested
-// first-children), plus the depth overflow check.
+// first-children), plus the depth overflow check.  A run that starts at i
+// holds more than ncrit bodies iff body i + ncrit shares its prefix, so the
+// chain length follows from one comparison of keys; the parent test counts
+// at most ncrit + 1 bodies on either side of i.
 __global__ void k_chain(const u64 *keys, long n, int D, int ncrit, int *lfirst, int *chain, DevCounters *ctr) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -199,25 +239,22 @@ __global__ void k_chain(const u64 *keys, long n, int D, int ncrit, int *lfirst, 
   int len = 0;
   if (lf <= D) {
     const u64 key = keys[i];
-    long end;
-    bool parent_splits = true;
-    if (lf == 0) {  // a system's root: always a cell
-      end = upper_run(keys, i, n, D, 0, prefix_of(key, D, 0));
-    } else {
+    bool parent_splits = true;  // a system's root is always a cell
+    if (lf > 0) {
       const u64 pp = prefix_of(key, D, lf - 1);
-      const long b0 = lower_run(keys, 0, i, D, lf - 1, pp);
-      const long e0 = upper_run(keys, i, n, D, lf - 1, pp);
-      parent_splits = e0 - b0 > ncrit;
-      end = e0;
+      const long R = run_ahead(keys, i, n, D, lf - 1, pp, (long)ncrit + 1);
+      const long need = (long)ncrit + 1 - R;  // parent bodies wanted before i
+      parent_splits = need <= 0 || (i - need >= 0 && prefix_of(keys[i - need], D, lf - 1) == pp);
     }
     if (parent_splits) {
-      for (int l = lf; l <= D; l++) {
-        const long e = upper_run(keys, i, end, D, l, prefix_of(key, D, l));
-        len++;
-        if (e - i <= ncrit) break;
-        if (l == D) { ctr->overflow = 1; break; }
-        end = e;
+      // levels lf, lf+1, ... while the run from i exceeds ncrit, then the leaf
+      int last = i + ncrit < n ? diff_level(key, keys[i + ncrit], D) : lf;
+      if (last < lf) last = lf;
+      if (last > D) {
+        ctr->overflow = 1;
+        last = D;
       }
+      len = last - lf + 1;
     }
   }
   chain[i] = len;
@@ -228,55 +265,55 @@ struct PreTables {
   double4 *xr;
 };
 
-// Writes the cells of each chain at their pre-order ranks.
-__global__ void k_cells(const u64 *keys, long n, int D, int ncrit, const int *lfirst, const int *chain,
-                        const int *prebase, const RootGeom *g, PreTables t, DevCounters *ctr) {
+// The body that starts each cell (pre-order rank -> sorted body position).
+__global__ void k_cell_owner(long n, const int *chain, const int *prebase, int *owner) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int len = chain[i];
-  if (len == 0) return;
-  const int lf = lfirst[i];
-  const u64 key = keys[i];
-  const RootGeom *gs = g + (long)(key >> (3 * D));  // the body's system
-  const double R0 = gs->R0;
-  double cx = gs->X0[0], cy = gs->X0[1], cz = gs->X0[2];
-  double r = R0;  // R0 / 2^l, halved exactly level by level
-  for (int l = 0; l < lf; l++) {  // centre of the level-lf cell holding body i
-    const int o = (int)((key >> (3 * (D - 1 - l))) & 7);
-    r = __dmul_rn(r, 0.5);
-    cx = __dadd_rn(cx, (o & 1) ? r : -r);
-    cy = __dadd_rn(cy, (o & 2) ? r : -r);
-    cz = __dadd_rn(cz, (o & 4) ? r : -r);
-  }
-  const int p0 = prebase[i];
-  int parent = -1;
-  long end = upper_run(keys, i, n, D, 0, prefix_of(key, D, 0));  // the system's bodies
-  if (lf > 0) {
-    const u64 pp = prefix_of(key, D, lf - 1);
-    const long b0 = lower_run(keys, 0, i, D, lf - 1, pp);
-    end = upper_run(keys, i, n, D, lf - 1, pp);
-    parent = prebase[b0] + (lf - 1 - lfirst[b0]);
-  }
-  for (int k = 0; k < len; k++) {
-    const int l = lf + k, p = p0 + k;
-    const long e = upper_run(keys, i, end, D, l, prefix_of(key, D, l));
-    t.begin[p] = (int)i;
-    t.count[p] = (int)(e - i);
-    t.level[p] = l;
-    t.parent[p] = parent;
-    t.xr[p] = make_double4(cx, cy, cz, r);
-    atomicAdd(&ctr->level_count[l], 1);
-    if (parent >= 0) atomicAdd(&t.nchild[parent], 1);
-    if (l < D) {  // next chain member is the first child: advance the centre
-      const int o = (int)((key >> (3 * (D - 1 - l))) & 7);
+  for (int k = 0; k < len; k++) owner[prebase[i] + k] = (int)i;
+}
+
+// One thread per cell (pre-order rank p): the k-th cell of the chain that
+// starts at body i = owner[p] is at level lfirst[i] + k.
+__global__ void k_cells(const u64 *keys, long n, long C, int D, const int *lfirst, const int *owner,
+                        const int *prebase, const RootGeom *g, PreTables t, DevCounters *ctr) {
+  __shared__ int lc[EXAFMM_MAX_LEVEL + 2];  // cells per level made by this block
+  if (threadIdx.x < EXAFMM_MAX_LEVEL + 2) lc[threadIdx.x] = 0;
+  __syncthreads();
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < C) {
+    const long i = owner[p];
+    const int k = (int)(p - prebase[i]), lf = lfirst[i], l = lf + k;
+    const u64 key = keys[i];
+    const RootGeom *gs = g + (long)(key >> (3 * D));  // the body's system
+    double cx = gs->X0[0], cy = gs->X0[1], cz = gs->X0[2];
+    double r = gs->R0;  // R0 / 2^l, halved exactly level by level
+    for (int q = 0; q < l; q++) {  // centre of the level-l cell holding body i
+      const int o = (int)((key >> (3 * (D - 1 - q))) & 7);
       r = __dmul_rn(r, 0.5);
       cx = __dadd_rn(cx, (o & 1) ? r : -r);
       cy = __dadd_rn(cy, (o & 2) ? r : -r);
       cz = __dadd_rn(cz, (o & 4) ? r : -r);
     }
-    parent = p;
-    end = e;
+    int parent = (int)p - 1;  // the chain's previous cell
+    if (k == 0) {
+      parent = -1;
+      if (lf > 0) {
+        const long b0 = lower_run(keys, 0, i, D, lf - 1, prefix_of(key, D, lf - 1));
+        parent = prebase[b0] + (lf - 1 - lfirst[b0]);
+      }
+    }
+    const long e = upper_run(keys, i, n, D, l, prefix_of(key, D, l));
+    t.begin[p] = (int)i;
+    t.count[p] = (int)(e - i);
+    t.level[p] = l;
+    t.parent[p] = parent;
+    t.xr[p] = make_double4(cx, cy, cz, r);
+    atomicAdd_block(&lc[l], 1);
+    if (parent >= 0) atomicAdd(&t.nchild[parent], 1);
   }
+  __syncthreads();
+  if (threadIdx.x < EXAFMM_MAX_LEVEL + 2 && lc[threadIdx.x]) atomicAdd(&ctr->level_count[threadIdx.x], lc[threadIdx.x]);
 }
 
 __global__ void k_level_keys(const int *level, long c, u64 *k, u32 *v) {
@@ -421,7 +458,7 @@ void build_tree(Handle &h) {
     h.ncells = (int)C;
     h.key_levels = D;
     // pre-order tables (reuse the idle sort buffers' siblings)
-    h.pre_tmp.need(C * (5 * sizeof(int) + sizeof(double4)) + 256);
+    h.pre_tmp.need(C * (6 * sizeof(int) + sizeof(double4)) + 256);
     PreTables t;
     t.xr = h.pre_tmp.as<double4>();
     t.begin = (int *)(t.xr + C);
@@ -429,10 +466,11 @@ void build_tree(Handle &h) {
     t.level = t.count + C;
     t.parent = t.level + C;
     t.nchild = t.parent + C;
+    int *owner = t.nchild + C;
     FMM_CUDA(cudaMemsetAsync(t.nchild, 0, C * sizeof(int), s));
-    k_cells<<<grid_for(n, TB), TB, 0, s>>>(k, n, D, h.prm.ncrit, h.lfirst.as<int>(), h.chain.as<int>(),
-                                           h.prebase.as<int>(), g, t, ctr);
-    h.launches++;
+    k_cell_owner<<<grid_for(n, TB), TB, 0, s>>>(n, h.chain.as<int>(), h.prebase.as<int>(), owner);
+    k_cells<<<grid_for(C, TB), TB, 0, s>>>(k, n, C, D, h.lfirst.as<int>(), owner, h.prebase.as<int>(), g, t, ctr);
+    h.launches += 2;
     FMM_LAUNCH();
 
     // 5. BFS order = stable sort of pre-order cells by level
