@@ -106,44 +106,96 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const u64 *keys, long n,
   hist[(long)threadIdx.x * ntiles + blockIdx.x] = hs[threadIdx.x];
 }
 
-// Stable scatter: items are ranked in (round, warp, lane) order, which is
-// their input order inside the tile.
+// Stable scatter of one tile.  Warp w ranks its contiguous 256 items
+// (8 rounds of 32 lanes, per-warp digit counters bumped by the leader of
+// each group of equal digits), the counts of the 8 warps are combined into
+// tile-local digit offsets, the items are sorted by digit inside the tile in
+// shared memory, and then written out in order: items of one digit are
+// contiguous in the output, so the stores coalesce.
 __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const u64 *kin, const u32 *vin, u64 *kout, u32 *vout,
                                                           long n, int shift, u64 mask, const int *offs,
                                                           int ntiles) {
-  __shared__ int run[RS_BINS];
-  __shared__ int wcnt[RS_THREADS / 32][RS_BINS];
+  constexpr int NW = RS_THREADS / 32, PER = RS_TILE / NW;  // 256 items per warp
+  __shared__ int wcnt[NW][RS_BINS + 1];                     // per-warp digit counts, then offsets
+  __shared__ int loff[RS_BINS + 1];                         // tile-local digit offsets
+  __shared__ u64 sk[RS_TILE];
+  __shared__ u32 sv[RS_TILE];
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  run[t] = offs[(long)t * ntiles + blockIdx.x];
+  for (int k = t; k < NW * (RS_BINS + 1); k += RS_THREADS) (&wcnt[0][0])[k] = 0;
+  __syncthreads();
   const long tile0 = (long)blockIdx.x * RS_TILE;
-  for (int k = 0; k < RS_ITEMS; k++) {
-    const long i = tile0 + (long)k * RS_THREADS + t;
-    const bool valid = i < n;
-    const u64 key = valid ? kin[i] : 0;
-    const u32 val = valid ? vin[i] : 0;
-    const int d = valid ? (int)((key >> shift) & mask) : RS_BINS;
+  const int valid = (int)(n - tile0 < RS_TILE ? n - tile0 : RS_TILE);
+  u64 key[RS_ITEMS];
+  u32 val[RS_ITEMS];
+  int dig[RS_ITEMS], pos[RS_ITEMS];
 #pragma unroll
-    for (int w = 0; w < RS_THREADS / 32; w++) wcnt[w][t] = 0;
-    __syncthreads();
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
-    const int rank = __popc(peers & ((1u << lane) - 1u));
-    if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
-    __syncthreads();
-    int r = run[t];
+  for (int r = 0; r < RS_ITEMS; r++) {
+    const int j = warp * PER + r * 32 + lane;
+    const bool ok = j < valid;
+    key[r] = ok ? kin[tile0 + j] : 0;
+    val[r] = ok ? vin[tile0 + j] : 0;
+    dig[r] = ok ? (int)((key[r] >> shift) & mask) : RS_BINS;  // padding sorts last
+  }
 #pragma unroll
-    for (int w = 0; w < RS_THREADS / 32; w++) {
-      int c = wcnt[w][t];
-      wcnt[w][t] = r;
-      r += c;
+  for (int r = 0; r < RS_ITEMS; r++) {
+    const unsigned peers = __match_any_sync(0xffffffffu, dig[r]);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) {
+      base = wcnt[warp][dig[r]];
+      wcnt[warp][dig[r]] = base + __popc(peers);
     }
-    run[t] = r;
-    __syncthreads();
-    if (valid) {
-      const int pos = wcnt[warp][d] + rank;
-      kout[pos] = key;
-      vout[pos] = val;
+    pos[r] = __shfl_sync(0xffffffffu, base, leader) + __popc(peers & ((1u << lane) - 1u));
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: offsets of the warps' runs, and the digit's total
+  for (int d = t; d <= RS_BINS; d += RS_THREADS) {
+    int run = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+      const int c = wcnt[w][d];
+      wcnt[w][d] = run;
+      run += c;
     }
-    __syncthreads();
+    loff[d] = run;
+  }
+  __syncthreads();
+  // exclusive scan of the digit totals (thread 0 of each warp scans a slice)
+  if (t < 32) {
+    constexpr int SL = (RS_BINS + 1 + 31) / 32;
+    int tot = 0;
+    for (int k = 0; k < SL; k++) tot += lane * SL + k <= RS_BINS ? loff[lane * SL + k] : 0;
+    int incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    int run = incl - tot;
+    for (int k = 0; k < SL; k++) {
+      const int d = lane * SL + k;
+      if (d <= RS_BINS) {
+        const int c = loff[d];
+        loff[d] = run;
+        run += c;
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RS_ITEMS; r++) {
+    const int lp = loff[dig[r]] + wcnt[warp][dig[r]] + pos[r];
+    sk[lp] = key[r];
+    sv[lp] = val[r];
+  }
+  __syncthreads();
+  for (int j = t; j < valid; j += RS_THREADS) {
+    const u64 k = sk[j];
+    const int d = (int)((k >> shift) & mask);
+    const long o = (long)offs[(long)d * ntiles + blockIdx.x] + (j - loff[d]);
+    kout[o] = k;
+    vout[o] = sv[j];
   }
 }
 
