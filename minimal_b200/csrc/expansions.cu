@@ -416,6 +416,111 @@ __global__ void __launch_bounds__(SH_T) k_l2l(int c0, const int *child, const in
   }
 }
 
+// ---- octant-batched L2L (orders P <= OB_MAXP).  One thread per output
+// coefficient walks that output's term list once for all eight children:
+// the parent's input and the term's index arithmetic are shared, and the
+// signs live in the tables -- the parent's local expansion is staged as
+// (conjugate / negated) copies and the unit harmonics as conjugate
+// variants, so a term is two plain index offsets.  A scaled expansion keeps
+// both parents of a CTA on the same unit tables: the kernel stages
+// L(n) * rho^n and multiplies output degree j by rho^-j (rho = the child
+// radius), each by repeated multiplication so no intermediate leaves the
+// range of the scaled values.  (For M2M the per-octant kernel above is as
+// fast: its eight children bring eight different inputs.)
+constexpr int OB_PAR = 2;    // parents per CTA
+constexpr int OB_T = 64;     // threads per parent (outputs)
+constexpr int OB_MAXP = 16;
+
+// degree of coefficient index ci
+__device__ __forceinline__ int deg_of(int ci) {
+  int n = (int)((sqrtf(8.0f * ci + 1.0f) - 1.0f) * 0.5f);
+  while (tri(n) > ci) n--;
+  while (tri(n + 1) <= ci) n++;
+  return n;
+}
+
+__device__ __forceinline__ void cfma(double2 &acc, const double2 a, const double2 y) {
+  acc.x = fma(a.x, y.x, fma(-a.y, y.y, acc.x));
+  acc.y = fma(a.x, y.y, fma(a.y, y.x, acc.y));
+}
+
+// Unit harmonic variants into shared memory: Yv[v][oct][idx], v bit 0
+// conjugate, bit 1 negate (nv = 2 or 4 variants).
+__device__ void stage_unit_variants(double2 *Yv, const double2 *ytab, int dir, int nt, int nv) {
+  for (int e = threadIdx.x; e < nv * 8 * nt; e += blockDim.x) {
+    const int v = e / (8 * nt), r = e - v * 8 * nt;
+    double2 y = ytab[(size_t)dir * 8 * nt + r];
+    if (v & 1) y.y = -y.y;
+    if (v & 2) y = make_double2(-y.x, -y.y);
+    Yv[e] = y;
+  }
+}
+
+__global__ void __launch_bounds__(OB_PAR * OB_T) k_l2l_ob(int c0, int np, const int *child, const int *nchild,
+                                                       const double4 *xr, const double2 *ytab, TermTable tab,
+                                                       double2 *L, int P) {
+  extern __shared__ double2 sm2[];
+  const int nt = tri(P);
+  double2 *Yv = sm2;          // [2][8][nt] unit harmonics (child - parent)
+  double2 *A = Yv + 16 * nt;  // [OB_PAR][4][nt] scaled parent local: plain, conjugate, negated, both
+  __shared__ int cho[OB_PAR][8];
+  const int slot = threadIdx.x / OB_T, tl = threadIdx.x % OB_T;
+  const int pi = blockIdx.x * OB_PAR + slot, c = c0 + pi;
+  const bool has = pi < np && nchild[c] > 0;  // a leaf has no children to shift to
+  if (tl < 8) cho[slot][tl] = -1;
+  __syncthreads();
+  if (has && tl < nchild[c]) {
+    const int q = child[c] + tl;
+    cho[slot][octant_of(xr[q], xr[c])] = q;
+  }
+  stage_unit_variants(Yv, ytab, 1, nt, 2);
+  const double rho = has ? xr[c].w * 0.5 : 0.0;  // R_child
+  for (int ci = tl; ci < nt; ci += OB_T) {
+    double2 v = make_double2(0, 0);
+    if (has) {
+      v = L[(long)c * nt + ci];
+      for (int d = deg_of(ci); d > 0; d--) v = make_double2(v.x * rho, v.y * rho);
+    }
+    double2 *a = A + (size_t)slot * 4 * nt;
+    a[ci] = v;
+    a[nt + ci] = make_double2(v.x, -v.y);
+    a[2 * nt + ci] = make_double2(-v.x, -v.y);
+    a[3 * nt + ci] = make_double2(-v.x, v.y);
+  }
+  __syncthreads();
+  if (!has) return;
+  const double2 *As = A + (size_t)slot * 4 * nt;
+  const double inv = 1.0 / rho;
+  int kids[8];
+#pragma unroll
+  for (int oct = 0; oct < 8; oct++) kids[oct] = cho[slot][oct];
+  for (int r = tl; r < nt; r += OB_T) {
+    const int o = tab.perm[r];
+    const unsigned *t = tab.terms + tab.off[r];
+    const int nterm = tab.off[r + 1] - tab.off[r];
+    double2 acc[8];
+#pragma unroll
+    for (int oct = 0; oct < 8; oct++) acc[oct] = make_double2(0, 0);
+    for (int qq = 0; qq < nterm; qq++) {
+      const unsigned e = t[qq];
+      const double2 a = As[e & 2047u];
+      const int iy = (int)(e >> 11);
+#pragma unroll
+      for (int oct = 0; oct < 8; oct++) cfma(acc[oct], a, Yv[iy + oct * nt]);
+    }
+    const int dj = deg_of(o);
+#pragma unroll
+    for (int oct = 0; oct < 8; oct++) {
+      if (kids[oct] < 0) continue;
+      double2 v = acc[oct];
+      for (int d = dj; d > 0; d--) v = make_double2(v.x * inv, v.y * inv);
+      double2 &dst = L[(long)kids[oct] * nt + o];
+      dst.x += v.x;
+      dst.y += v.y;
+    }
+  }
+}
+
 // L2P (3d/kernel.h:293-323): potential and force at each body of a leaf.
 __global__ void __launch_bounds__(WARPS * 32) k_l2p(const int *leaves, int nleaves, const int *begin,
                                                     const int *count, const double4 *xr, const double4 *src,
@@ -493,22 +598,40 @@ void expansions_set_attributes() {
   EXAFMM_UNROLLED_ORDERS(EXAFMM_F32_ATTR)
 #undef EXAFMM_F32_ATTR
   cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_l2l_ob, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 // Term tables of M2M and L2L for order P, built on the host from the same
 // enumerators the formulas use.  Layout (ints): per direction perm[nt],
 // off[nt + 1], terms[...].
-std::vector<int> term_tables(int P, size_t *l2l_at) {
+// Term tables of M2M (dir 0) and L2L (dir 1) for the per-octant kernels, and
+// of L2L (dir 3, orders up to OB_MAXP) for the octant-batched kernel, whose
+// terms are ia' | iy' << 11: the input index in its variant plane
+// (conjugate + 2 * negate) and the harmonic index in its variant plane of 8
+// octant tables (conjugate).  (Dir 2, an M2M variant table, is not built.)
+std::vector<int> term_tables(int P, size_t at[4]) {
   const int nt = tri(P);
   std::vector<int> out;
-  for (int dir = 0; dir < 2; dir++) {
-    if (dir == 1) *l2l_at = out.size();
+  for (int dir = 0; dir < 4; dir++) {
+    at[dir] = out.size();
+    if (dir == 2 || (dir == 3 && P > OB_MAXP)) continue;
     std::vector<std::vector<unsigned>> per(nt);
     for (int j = 0; j < P; j++)
       for (int k = 0; k <= j; k++) {
-        auto emit = [&](int ia, bool ca, int n, int o, int f) { per[tri(j) + k].push_back(pack_term(ia, ca, n, o, f)); };
-        if (dir == 0) m2m_terms(j, k, emit);
+        auto emit = [&](int ia, bool ca, int n, int o, int f) {
+          unsigned t;
+          if (dir < 2) {
+            t = pack_term(ia, ca, n, o, f);
+          } else {
+            const int iy = tri(n) + (o < 0 ? -o : o);
+            const int cy = o < 0, neg = f < 0;
+            const int va = dir == 2 ? (int)ca : (int)ca + 2 * neg, vy = dir == 2 ? cy + 2 * neg : cy;
+            t = (unsigned)(ia + va * nt) | ((unsigned)(iy + vy * 8 * nt) << 11);
+          }
+          per[tri(j) + k].push_back(t);
+        };
+        if (dir % 2 == 0) m2m_terms(j, k, emit);
         else l2l_terms(j, k, P, emit);
       }
     std::vector<int> perm(nt);
@@ -531,7 +654,7 @@ std::vector<int> term_tables(int P, size_t *l2l_at) {
 
 TermTable table_view(const Handle &h, int P, int dir) {
   const int nt = tri(P);
-  const int *b = h.shift_terms.as<int>() + (dir ? h.shift_l2l_at : 0);
+  const int *b = h.shift_terms.as<int>() + h.shift_at[dir];
   return TermTable{b, b + nt, (const unsigned *)(b + 2 * nt + 1)};
 }
 
@@ -543,11 +666,9 @@ void unit_tables(Handle &h) {
   k_unit_tables<<<16, 32, 0, h.stream>>>(P, h.shift_ops.as<double2>());
   h.launches++;
   FMM_LAUNCH();
-  size_t at = 0;
-  const std::vector<int> t = term_tables(P, &at);
+  const std::vector<int> t = term_tables(P, h.shift_at);
   h.shift_terms.need(t.size() * sizeof(int));
   FMM_CUDA(cudaMemcpy(h.shift_terms.p, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
-  h.shift_l2l_at = at;
   h.shift_P = P;
 }
 
@@ -605,9 +726,14 @@ void downward_pass(Handle &h) {
   for (int l = 0; l < h.depth; l++) {  // parents at level l push to their children
     const int c0 = h.level_base[l], c1 = h.level_base[l + 1];
     if (c1 <= c0) continue;
-    k_l2l<<<c1 - c0, SH_T, 9 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
-                                                         h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
-                                                         table_view(h, P, 1), h.L.as<double2>(), P);
+    if (P <= OB_MAXP)
+      k_l2l_ob<<<(c1 - c0 + OB_PAR - 1) / OB_PAR, OB_PAR * OB_T, (16 + OB_PAR * 4) * nt * sizeof(double2), s>>>(
+          c0, c1 - c0, h.c_child.as<int>(), h.c_nchild.as<int>(), h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
+          table_view(h, P, 3), h.L.as<double2>(), P);
+    else
+      k_l2l<<<c1 - c0, SH_T, 9 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
+                                                           h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
+                                                           table_view(h, P, 1), h.L.as<double2>(), P);
     h.launches++;
     FMM_LAUNCH();
   }

@@ -137,7 +137,7 @@ struct Handle {
   Buf M, L;   // double2 [ncells][nterm]
   Buf shift_ops;   // M2M / L2L harmonics of the unit child offsets (expansions.cu)
   Buf shift_terms; // M2M / L2L term tables (expansions.cu)
-  size_t shift_l2l_at = 0;
+  size_t shift_at[4] = {0, 0, 0, 0};  // offsets of the four term tables
   int shift_P = -1;
   Buf m2l_units;  // balanced contraction table for the M2L kernel (per P)
   int m2l_units_P = -1;
