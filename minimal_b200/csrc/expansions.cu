@@ -425,8 +425,9 @@ __global__ void __launch_bounds__(SH_T) k_l2l(int c0, const int *child, const in
 // both parents of a CTA on the same unit tables: the kernel stages
 // L(n) * rho^n and multiplies output degree j by rho^-j (rho = the child
 // radius), each by repeated multiplication so no intermediate leaves the
-// range of the scaled values.  (For M2M the per-octant kernel above is as
-// fast: its eight children bring eight different inputs.)
+// range of the scaled values.  (In FP64 the per-octant M2M kernel above is
+// as fast as an octant-batched one: its eight children bring eight
+// different inputs; the mixed form uses the octant-batched k_m2m_ob32.)
 constexpr int OB_PAR = 2;    // parents per CTA
 constexpr int OB_T = 64;     // threads per parent (outputs)
 constexpr int OB_MAXP = 16;
@@ -439,30 +440,115 @@ __device__ __forceinline__ int deg_of(int ci) {
   return n;
 }
 
-__device__ __forceinline__ void cfma(double2 &acc, const double2 a, const double2 y) {
+template <class V>
+__device__ __forceinline__ void cfma(V &acc, const V a, const V y) {
   acc.x = fma(a.x, y.x, fma(-a.y, y.y, acc.x));
   acc.y = fma(a.x, y.y, fma(a.y, y.x, acc.y));
 }
 
+// complex value type of a compute precision
+template <bool F32>
+struct Cplx {
+  typedef double2 V;
+  typedef double R;
+};
+template <>
+struct Cplx<true> {
+  typedef float2 V;
+  typedef float R;
+};
+
 // Unit harmonic variants into shared memory: Yv[v][oct][idx], v bit 0
 // conjugate, bit 1 negate (nv = 2 or 4 variants).
-__device__ void stage_unit_variants(double2 *Yv, const double2 *ytab, int dir, int nt, int nv) {
+template <class V>
+__device__ void stage_unit_variants(V *Yv, const double2 *ytab, int dir, int nt, int nv) {
   for (int e = threadIdx.x; e < nv * 8 * nt; e += blockDim.x) {
     const int v = e / (8 * nt), r = e - v * 8 * nt;
     double2 y = ytab[(size_t)dir * 8 * nt + r];
     if (v & 1) y.y = -y.y;
     if (v & 2) y = make_double2(-y.x, -y.y);
-    Yv[e] = y;
+    Yv[e].x = y.x;
+    Yv[e].y = y.y;
   }
 }
 
+// Octant-batched M2M for the mixed form: one thread per output coefficient
+// sums all eight children in one walk of the output's term list; children
+// staged as scaled multipoles M(d) / rho^d (plain and conjugate copies, zero
+// for an absent child), the unit harmonics in four sign variants, products
+// in FP32 on these order-one values, the output rescaled by rho^j in FP64.
+__global__ void __launch_bounds__(OB_PAR * OB_T) k_m2m_ob32(int c0, int np, const int *child, const int *nchild,
+                                                         const double4 *xr, const double2 *ytab, TermTable tab,
+                                                         double2 *M, int P) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *sm2 = (float2 *)smraw;
+  const int nt = tri(P);
+  float2 *Yv = sm2;           // [4][8][nt] unit harmonics (parent - child)
+  float2 *A = Yv + 32 * nt;   // [OB_PAR][8][2][nt] scaled child multipoles, plain and conjugate
+  __shared__ int cho[OB_PAR][8];
+  const int slot = threadIdx.x / OB_T, tl = threadIdx.x % OB_T;
+  const int pi = blockIdx.x * OB_PAR + slot, c = c0 + pi;
+  const bool has = pi < np && nchild[c] > 0;  // a leaf keeps its P2M multipole
+  if (tl < 8) cho[slot][tl] = -1;
+  __syncthreads();
+  if (has && tl < nchild[c]) {
+    const int q = child[c] + tl;
+    cho[slot][octant_of(xr[q], xr[c])] = q;
+  }
+  stage_unit_variants(Yv, ytab, 0, nt, 4);
+  __syncthreads();
+  const double inv = has ? 1.0 / (xr[c].w * 0.5) : 0.0;  // 1 / R_child
+  for (int e = tl; e < 8 * nt; e += OB_T) {
+    const int oct = e / nt, ci = e - oct * nt, q = cho[slot][oct];
+    double2 v = make_double2(0, 0);
+    if (has && q >= 0) {
+      v = M[(long)q * nt + ci];
+      for (int d = deg_of(ci); d > 0; d--) v = make_double2(v.x * inv, v.y * inv);
+    }
+    float2 *a = A + ((size_t)slot * 8 + oct) * 2 * nt;
+    a[ci] = make_float2((float)v.x, (float)v.y);
+    a[nt + ci] = make_float2((float)v.x, (float)-v.y);
+  }
+  __syncthreads();
+  if (!has) return;
+  const float2 *As = A + (size_t)slot * 8 * 2 * nt;
+  const double rho = xr[c].w * 0.5;
+  for (int r = tl; r < nt; r += OB_T) {
+    const int o = tab.perm[r];
+    const unsigned *t = tab.terms + tab.off[r];
+    const int nterm = tab.off[r + 1] - tab.off[r];
+    float2 acc[8];  // one chain per octant
+#pragma unroll
+    for (int oct = 0; oct < 8; oct++) acc[oct] = make_float2(0.f, 0.f);
+    for (int qq = 0; qq < nterm; qq++) {
+      const unsigned e = t[qq];
+      const int ia = (int)(e & 2047u), iy = (int)(e >> 11);
+#pragma unroll
+      for (int oct = 0; oct < 8; oct++) cfma(acc[oct], As[oct * 2 * nt + ia], Yv[iy + oct * nt]);
+    }
+    double2 v = make_double2(0, 0);
+#pragma unroll
+    for (int oct = 0; oct < 8; oct++) {
+      v.x += acc[oct].x;
+      v.y += acc[oct].y;
+    }
+    for (int d = deg_of(o); d > 0; d--) v = make_double2(v.x * rho, v.y * rho);
+    M[(long)c * nt + o] = v;
+  }
+}
+
+// F32 (mixed form): the products in FP32 on the scaled (order-one) values;
+// staging, the rescaling and the sums into L stay FP64.
+template <bool F32>
 __global__ void __launch_bounds__(OB_PAR * OB_T) k_l2l_ob(int c0, int np, const int *child, const int *nchild,
                                                        const double4 *xr, const double2 *ytab, TermTable tab,
                                                        double2 *L, int P) {
-  extern __shared__ double2 sm2[];
+  typedef typename Cplx<F32>::V V;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V *sm2 = (V *)smraw;
   const int nt = tri(P);
-  double2 *Yv = sm2;          // [2][8][nt] unit harmonics (child - parent)
-  double2 *A = Yv + 16 * nt;  // [OB_PAR][4][nt] scaled parent local: plain, conjugate, negated, both
+  V *Yv = sm2;          // [2][8][nt] unit harmonics (child - parent)
+  V *A = Yv + 16 * nt;  // [OB_PAR][4][nt] scaled parent local: plain, conjugate, negated, both
   __shared__ int cho[OB_PAR][8];
   const int slot = threadIdx.x / OB_T, tl = threadIdx.x % OB_T;
   const int pi = blockIdx.x * OB_PAR + slot, c = c0 + pi;
@@ -481,15 +567,19 @@ __global__ void __launch_bounds__(OB_PAR * OB_T) k_l2l_ob(int c0, int np, const 
       v = L[(long)c * nt + ci];
       for (int d = deg_of(ci); d > 0; d--) v = make_double2(v.x * rho, v.y * rho);
     }
-    double2 *a = A + (size_t)slot * 4 * nt;
-    a[ci] = v;
-    a[nt + ci] = make_double2(v.x, -v.y);
-    a[2 * nt + ci] = make_double2(-v.x, -v.y);
-    a[3 * nt + ci] = make_double2(-v.x, v.y);
+    V *a = A + (size_t)slot * 4 * nt;
+    a[ci].x = v.x;
+    a[ci].y = v.y;
+    a[nt + ci].x = v.x;
+    a[nt + ci].y = -v.y;
+    a[2 * nt + ci].x = -v.x;
+    a[2 * nt + ci].y = -v.y;
+    a[3 * nt + ci].x = -v.x;
+    a[3 * nt + ci].y = v.y;
   }
   __syncthreads();
   if (!has) return;
-  const double2 *As = A + (size_t)slot * 4 * nt;
+  const V *As = A + (size_t)slot * 4 * nt;
   const double inv = 1.0 / rho;
   int kids[8];
 #pragma unroll
@@ -498,12 +588,12 @@ __global__ void __launch_bounds__(OB_PAR * OB_T) k_l2l_ob(int c0, int np, const 
     const int o = tab.perm[r];
     const unsigned *t = tab.terms + tab.off[r];
     const int nterm = tab.off[r + 1] - tab.off[r];
-    double2 acc[8];
+    V acc[8];
 #pragma unroll
-    for (int oct = 0; oct < 8; oct++) acc[oct] = make_double2(0, 0);
+    for (int oct = 0; oct < 8; oct++) acc[oct].x = acc[oct].y = 0;
     for (int qq = 0; qq < nterm; qq++) {
       const unsigned e = t[qq];
-      const double2 a = As[e & 2047u];
+      const V a = As[e & 2047u];
       const int iy = (int)(e >> 11);
 #pragma unroll
       for (int oct = 0; oct < 8; oct++) cfma(acc[oct], a, Yv[iy + oct * nt]);
@@ -512,7 +602,7 @@ __global__ void __launch_bounds__(OB_PAR * OB_T) k_l2l_ob(int c0, int np, const 
 #pragma unroll
     for (int oct = 0; oct < 8; oct++) {
       if (kids[oct] < 0) continue;
-      double2 v = acc[oct];
+      double2 v = make_double2(acc[oct].x, acc[oct].y);
       for (int d = dj; d > 0; d--) v = make_double2(v.x * inv, v.y * inv);
       double2 &dst = L[(long)kids[oct] * nt + o];
       dst.x += v.x;
@@ -598,7 +688,9 @@ void expansions_set_attributes() {
   EXAFMM_UNROLLED_ORDERS(EXAFMM_F32_ATTR)
 #undef EXAFMM_F32_ATTR
   cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_l2l_ob, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_l2l_ob<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_m2m_ob32, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_l2l_ob<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
@@ -606,16 +698,16 @@ void expansions_set_attributes() {
 // enumerators the formulas use.  Layout (ints): per direction perm[nt],
 // off[nt + 1], terms[...].
 // Term tables of M2M (dir 0) and L2L (dir 1) for the per-octant kernels, and
-// of L2L (dir 3, orders up to OB_MAXP) for the octant-batched kernel, whose
-// terms are ia' | iy' << 11: the input index in its variant plane
-// (conjugate + 2 * negate) and the harmonic index in its variant plane of 8
-// octant tables (conjugate).  (Dir 2, an M2M variant table, is not built.)
+// (dirs 2, 3, orders up to OB_MAXP) for the octant-batched ones, whose terms
+// are ia' | iy' << 11: the input index in its variant plane (M2M: conjugate;
+// L2L: conjugate + 2 * negate) and the harmonic index in its variant plane
+// of 8 octant tables (M2M: conjugate + 2 * negate; L2L: conjugate).
 std::vector<int> term_tables(int P, size_t at[4]) {
   const int nt = tri(P);
   std::vector<int> out;
   for (int dir = 0; dir < 4; dir++) {
     at[dir] = out.size();
-    if (dir == 2 || (dir == 3 && P > OB_MAXP)) continue;
+    if (dir >= 2 && P > OB_MAXP) continue;
     std::vector<std::vector<unsigned>> per(nt);
     for (int j = 0; j < P; j++)
       for (int k = 0; k <= j; k++) {
@@ -711,9 +803,14 @@ void upward_pass(Handle &h) {
   for (int l = h.depth - 1; l >= 0; l--) {
     const int c0 = h.level_base[l], c1 = h.level_base[l + 1];
     if (c1 <= c0) continue;
-    k_m2m<<<c1 - c0, SH_T, 24 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
-                                                          h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
-                                                          table_view(h, P, 0), h.M.as<double2>(), P);
+    if (P <= OB_MAXP && h.prm.precision == EXAFMM_MIXED)
+      k_m2m_ob32<<<(c1 - c0 + OB_PAR - 1) / OB_PAR, OB_PAR * OB_T, (32 + OB_PAR * 16) * nt * sizeof(float2), s>>>(
+          c0, c1 - c0, h.c_child.as<int>(), h.c_nchild.as<int>(), h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
+          table_view(h, P, 2), h.M.as<double2>(), P);
+    else
+      k_m2m<<<c1 - c0, SH_T, 24 * nt * sizeof(double2), s>>>(c0, h.c_child.as<int>(), h.c_nchild.as<int>(),
+                                                            h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
+                                                            table_view(h, P, 0), h.M.as<double2>(), P);
     h.launches++;
     FMM_LAUNCH();
   }
@@ -726,8 +823,13 @@ void downward_pass(Handle &h) {
   for (int l = 0; l < h.depth; l++) {  // parents at level l push to their children
     const int c0 = h.level_base[l], c1 = h.level_base[l + 1];
     if (c1 <= c0) continue;
-    if (P <= OB_MAXP)
-      k_l2l_ob<<<(c1 - c0 + OB_PAR - 1) / OB_PAR, OB_PAR * OB_T, (16 + OB_PAR * 4) * nt * sizeof(double2), s>>>(
+    const dim3 grid((c1 - c0 + OB_PAR - 1) / OB_PAR), block(OB_PAR * OB_T);
+    if (P <= OB_MAXP && h.prm.precision == EXAFMM_MIXED)
+      k_l2l_ob<true><<<grid, block, (16 + OB_PAR * 4) * nt * sizeof(float2), s>>>(
+          c0, c1 - c0, h.c_child.as<int>(), h.c_nchild.as<int>(), h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
+          table_view(h, P, 3), h.L.as<double2>(), P);
+    else if (P <= OB_MAXP)
+      k_l2l_ob<false><<<grid, block, (16 + OB_PAR * 4) * nt * sizeof(double2), s>>>(
           c0, c1 - c0, h.c_child.as<int>(), h.c_nchild.as<int>(), h.c_xr.as<double4>(), h.shift_ops.as<double2>(),
           table_view(h, P, 3), h.L.as<double2>(), P);
     else
