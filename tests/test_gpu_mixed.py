@@ -75,17 +75,21 @@ def test_mixed_full_size_error_target():
     assert rel(out[:, 4], d[:, 4]) <= 1.5 * rel(g["fmm"][:, 4], d[:, 4])
 
 
-def test_mixed_p20_falls_back_and_stays_correct():
+@pytest.mark.parametrize("P", [14, 16, 18])
+def test_mixed_high_orders_stay_correct(P):
     """Orders whose operators do not fit the tensor-core tile run the FP64
-    contraction; the FP32 near field still applies."""
+    contraction; the FP32 near field still applies.  P=14 and 16 take the
+    unrolled FP32 P2M/L2P (butterfly sums) and the octant-batched FP32
+    shifts, P=18 the runtime-order FP32 P2M/L2P and the per-octant FP64
+    shifts."""
     from minimal_b200 import FMM, drand48_bodies
 
     xq = drand48_bodies(8000, 1)
-    f = FMM(P=16, ncrit=64, theta=0.4, precision="mixed")
+    f = FMM(P=P, ncrit=64, theta=0.4, precision="mixed")
     f.set_bodies(xq)
     f.evaluate()
     pm, fm, _ = errors(f, 8000, 200)
-    g = FMM(P=16, ncrit=64, theta=0.4)
+    g = FMM(P=P, ncrit=64, theta=0.4)
     g.set_bodies(xq)
     g.evaluate()
     p6, f6, _ = errors(g, 8000, 200)
