@@ -300,6 +300,15 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
   const int tb = begin[c], tn = count[c];
   const int H = (tn + CT_TPT - 1) / CT_TPT, G = CT / H;
   const int i = tid % H, g = tid / H;
+  // x / G for the FP32 form's part bounds of every chunk, without an integer
+  // division: a float estimate (x < 2^24) corrected by one step
+  const float rG = 1.0f / (float)G;
+  auto divG = [&](int x) {
+    int q = (int)((float)x * rG);
+    q -= q * G > x;
+    q += (q + 1) * G <= x;
+    return q;
+  };
   const bool act = g < G;
   const double4 CA = xr[c];
   const int sexp = CA.w > 0 ? max(-100, min(100, ilogb(CA.w))) : 0;
@@ -487,8 +496,8 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
               p[u][q] = 0;
             }
         };
-        for (int cs = g * pre / G, ce = (g + 1) * pre / G; cs < ce; cs++) acc(stage[cs], std::true_type{});
-        const int rest = T - pre, from = pre + g * rest / G, to = pre + (g + 1) * rest / G;
+        for (int cs = divG(g * pre), ce = divG((g + 1) * pre); cs < ce; cs++) acc(stage[cs], std::true_type{});
+        const int rest = T - pre, from = pre + divG(g * rest), to = pre + divG((g + 1) * rest);
         const BT *sp = stage + from;
         for (int c0 = from; c0 < to; c0 += CT_BLOCK) {
           const int cend = min(to, c0 + CT_BLOCK);
