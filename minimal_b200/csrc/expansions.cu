@@ -200,18 +200,24 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int n
 }
 
 // P2M in FP32 for a compile-time order: each lane writes its body's q Y
-// terms to shared memory, then lane k sums term k over the 32 bodies (rows
-// padded to 33 entries: conflict-free), and the chunk sums are added in FP64.
+// terms to shared memory 32 terms at a time, then lane k sums term k of the
+// batch over the 32 bodies (rows padded to 33 entries: conflict-free), and
+// the sums are added in FP64.  The batch buffer (8 KB per warp) keeps
+// enough warps resident to hide the recurrence's latency.
+constexpr int P2M_ROW = 33;
+constexpr size_t p2m_t_smem(int nt) { return WARPS * (nt * sizeof(double2) + 32 * P2M_ROW * sizeof(float2) + 32 * sizeof(int)); }
+
 template <int PT>
 __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32t(const int *leaves, int nleaves, const int *begin,
                                                          const int *count, const float4 *srcf, double2 *M) {
-  constexpr int NT = PT * (PT + 1) / 2, ROW = 33;
+  constexpr int NT = PT * (PT + 1) / 2, ROW = P2M_ROW;
   extern __shared__ double2 sh[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * WARPS + wid;
   if (w >= nleaves) return;
   double2 *acc = sh + wid * NT;
-  float2 *buf = (float2 *)(sh + WARPS * NT) + wid * NT * ROW;
+  float2 *buf = (float2 *)(sh + WARPS * NT) + wid * 32 * ROW;
+  int *rowidx = (int *)((float2 *)(sh + WARPS * NT) + WARPS * 32 * ROW) + wid * 32;
   for (int k = lane; k < NT; k += 32) acc[k] = make_double2(0, 0);
   const int c = leaves[w];
   const int b0 = begin[c], nb = count[c];
@@ -219,22 +225,30 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32t(const int *leaves, int 
     const bool ok = t + lane < nb;
     const float4 B = ok ? srcf[b0 + t + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
     const SphF g = sph_of_f(B.x, B.y, B.z);
+    int gen = 0;  // terms generated so far (a constant at every unrolled step)
     __syncwarp();
     regular_all_f<PT, false>(PT, g, make_float2(g.e.x, -g.e.y), [&](int n, int m, float2 Y, float2) {
-      buf[(tri(n) + m) * ROW + lane] = make_float2(B.w * Y.x, B.w * Y.y);
-    });
-    __syncwarp();
-    for (int k = lane; k < NT; k += 32) {
-      float sx = 0.f, sy = 0.f;
+      const int slot = gen & 31;
+      buf[slot * ROW + lane] = make_float2(B.w * Y.x, B.w * Y.y);
+      if (lane == 0) rowidx[slot] = tri(n) + m;
+      gen++;
+      if ((gen & 31) == 0 || gen == NT) {  // sum the batch over the bodies
+        __syncwarp();
+        if (lane <= ((gen - 1) & 31)) {
+          float sx = 0.f, sy = 0.f;
 #pragma unroll 8
-      for (int b = 0; b < 32; b++) {
-        const float2 v = buf[k * ROW + b];
-        sx += v.x;
-        sy += v.y;
+          for (int b = 0; b < 32; b++) {
+            const float2 v = buf[lane * ROW + b];
+            sx += v.x;
+            sy += v.y;
+          }
+          double2 &a = acc[rowidx[lane]];
+          a.x += (double)sx;
+          a.y += (double)sy;
+        }
+        __syncwarp();
       }
-      acc[k].x += (double)sx;
-      acc[k].y += (double)sy;
-    }
+    });
   }
   __syncwarp();
   for (int k = lane; k < NT; k += 32) M[(long)c * NT + k] = acc[k];
@@ -777,7 +791,7 @@ void upward_pass(Handle &h) {
       kernel<<<grid, block, sm, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
                                      h.srcf.as<float4>(), h.M.as<double2>(), P);
     };
-    const size_t smt = WARPS * nt * (sizeof(double2) + 33 * sizeof(float2));
+    const size_t smt = p2m_t_smem(nt);
     auto argst = [&](auto kernel) {
       kernel<<<grid, block, smt, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
                                       h.srcf.as<float4>(), h.M.as<double2>());
@@ -785,7 +799,7 @@ void upward_pass(Handle &h) {
     switch (P) {
 #define EXAFMM_P2M_CASE(p) \
   case p:                  \
-    if (P2M_TRANSPOSE && p <= 12) argst(k_p2m_f32t<p>); else args(k_p2m_f32<p>); \
+    if (P2M_TRANSPOSE) argst(k_p2m_f32t<p>); else args(k_p2m_f32<p>); \
     break;
       EXAFMM_UNROLLED_ORDERS(EXAFMM_P2M_CASE)
 #undef EXAFMM_P2M_CASE
