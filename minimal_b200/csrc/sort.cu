@@ -12,6 +12,7 @@ namespace {
 constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr long SCAN_SMALL_TILES = 64;  // single-launch scan up to 64 tiles (256K ints)
 
 __device__ __forceinline__ int warp_incl_scan(int v) {
   const int lane = threadIdx.x & 31;
@@ -64,6 +65,58 @@ __global__ void k_scan_add(int *out, long n, const int *block_off) {
 }
 
 __global__ void k_copy_int(int *dst, const int *src) { *dst = *src; }
+
+// Exclusive scan of a short array (a few tiles) in one launch: block b
+// first sums all input before its tile (every block reads at most a few
+// hundred KB), then scans its tile as k_scan_tile does; the last block also
+// writes the total.  Input and output must not overlap.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_small(const int *in, int *out, long n, int *total_dev) {
+  __shared__ int warp_sum[SCAN_THREADS / 32];
+  __shared__ int s_prefix;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long lim = (long)blockIdx.x * SCAN_TILE;  // a multiple of 4: int4 loads
+  int pre = 0;
+  for (long i = threadIdx.x; 4 * i < lim; i += SCAN_THREADS) {
+    const int4 v = ((const int4 *)in)[i];
+    pre += (v.x + v.y) + (v.z + v.w);
+  }
+  pre = warp_incl_scan(pre);
+  if (lane == 31) warp_sum[warp] = pre;
+  __syncthreads();
+  if (warp == 0) {
+    const int t = warp_incl_scan(warp_sum[lane]);
+    if (lane == 31) s_prefix = t;
+  }
+  __syncthreads();
+  const int prefix = s_prefix;
+  __syncthreads();  // warp_sum is reused below
+  const long base = lim + (long)threadIdx.x * SCAN_ITEMS;
+  int v[SCAN_ITEMS];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = base + k < n ? in[base + k] : 0;
+    sum += v[k];
+  }
+  const int incl = warp_incl_scan(sum);
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int w = warp_sum[lane];
+    const int wi = warp_incl_scan(w);
+    warp_sum[lane] = wi - w;
+    if (lane == 31 && total_dev && blockIdx.x == gridDim.x - 1) *total_dev = prefix + wi;
+  }
+  __syncthreads();
+  int run = prefix + warp_sum[warp] + incl - sum;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+}
+
+
 
 void scan_rec(Handle &h, const int *in, int *out, long n, int *total_dev, int *work) {
   const long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
@@ -203,6 +256,13 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const u64 *kin, const
 
 void scan_exclusive_int(Handle &h, const int *in, int *out, long n, int *total_dev) {
   if (n <= 0) return;
+  const long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  if (nb <= SCAN_SMALL_TILES && ((uintptr_t)in & 15) == 0) {  // short: one launch
+    k_scan_small<<<(unsigned)nb, SCAN_THREADS, 0, h.stream>>>(in, out, n, total_dev);
+    h.launches++;
+    FMM_LAUNCH();
+    return;
+  }
   long need = 0, m = n;
   while (true) {
     long nb = (m + SCAN_TILE - 1) / SCAN_TILE;
