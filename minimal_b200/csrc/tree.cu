@@ -474,11 +474,12 @@ void build_tree(Handle &h) {
     FMM_LAUNCH();
 
     // 5. BFS order = stable sort of pre-order cells by level
-    h.ctmp.need(C * (2 * sizeof(u64) + 2 * sizeof(u32) + 4 * sizeof(int)) + 256);
-    u64 *lk = h.ctmp.as<u64>(), *lk2 = lk + C;
-    u32 *lv = (u32 *)(lk2 + C), *lv2 = lv + C;
-    int *bfs_of_pre = (int *)(lv2 + C), *is_leaf = bfs_of_pre + C, *blockstart = is_leaf + C,
-        *leafpos = blockstart + C;
+    const long Cp = (C + 3) & ~3L;  // every table starts 16-byte aligned (vector loads in the scans)
+    h.ctmp.need(Cp * (2 * sizeof(u64) + 2 * sizeof(u32) + 4 * sizeof(int)) + 256);
+    u64 *lk = h.ctmp.as<u64>(), *lk2 = lk + Cp;
+    u32 *lv = (u32 *)(lk2 + Cp), *lv2 = lv + Cp;
+    int *bfs_of_pre = (int *)(lv2 + Cp), *is_leaf = bfs_of_pre + Cp, *blockstart = is_leaf + Cp,
+        *leafpos = blockstart + Cp;
     k_level_keys<<<grid_for(C, TB), TB, 0, s>>>(t.level, C, lk, lv);
     h.launches++;
     FMM_LAUNCH();
