@@ -13,6 +13,7 @@ constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr long SCAN_SMALL_TILES = 64;  // single-launch scan up to 64 tiles (256K ints)
+constexpr long SCAN_TWO_TILES = 4096;  // two-launch scan up to 4096 tiles (16M ints)
 
 __device__ __forceinline__ int warp_incl_scan(int v) {
   const int lane = threadIdx.x & 31;
@@ -65,6 +66,67 @@ __global__ void k_scan_add(int *out, long n, const int *block_off) {
 }
 
 __global__ void k_copy_int(int *dst, const int *src) { *dst = *src; }
+
+// Per-tile sums (first launch of the two-launch scan).
+__global__ void __launch_bounds__(SCAN_THREADS) k_tile_sums(const int *in, long n, int *sums) {
+  __shared__ int warp_sum[SCAN_THREADS / 32];
+  const long base = (long)blockIdx.x * SCAN_TILE + (long)threadIdx.x * SCAN_ITEMS;
+  int v = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) v += base + k < n ? in[base + k] : 0;
+  v = warp_incl_scan(v);
+  if ((threadIdx.x & 31) == 31) warp_sum[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int t = warp_incl_scan(warp_sum[threadIdx.x]);
+    if (threadIdx.x == 31) sums[blockIdx.x] = t;
+  }
+}
+
+// Second launch: block b adds up the sums of the tiles before it (at most a
+// few thousand ints), then scans its tile; the last block writes the total.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles2(const int *in, int *out, long n, const int *sums,
+                                                             int *total_dev) {
+  __shared__ int warp_sum[SCAN_THREADS / 32];
+  __shared__ int s_prefix;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int pre = 0;
+  for (int i = threadIdx.x; i < (int)blockIdx.x; i += SCAN_THREADS) pre += sums[i];
+  pre = warp_incl_scan(pre);
+  if (lane == 31) warp_sum[warp] = pre;
+  __syncthreads();
+  if (warp == 0) {
+    const int t = warp_incl_scan(warp_sum[lane]);
+    if (lane == 31) s_prefix = t;
+  }
+  __syncthreads();
+  const int prefix = s_prefix;
+  __syncthreads();
+  const long base = (long)blockIdx.x * SCAN_TILE + (long)threadIdx.x * SCAN_ITEMS;
+  int v[SCAN_ITEMS];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = base + k < n ? in[base + k] : 0;
+    sum += v[k];
+  }
+  const int incl = warp_incl_scan(sum);
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int w = warp_sum[lane];
+    const int wi = warp_incl_scan(w);
+    warp_sum[lane] = wi - w;
+    if (lane == 31 && total_dev && blockIdx.x == gridDim.x - 1) *total_dev = prefix + wi;
+  }
+  __syncthreads();
+  int run = prefix + warp_sum[warp] + incl - sum;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+}
 
 // Exclusive scan of a short array (a few tiles) in one launch: block b
 // first sums all input before its tile (every block reads at most a few
@@ -260,6 +322,14 @@ void scan_exclusive_int(Handle &h, const int *in, int *out, long n, int *total_d
   if (nb <= SCAN_SMALL_TILES && ((uintptr_t)in & 15) == 0) {  // short: one launch
     k_scan_small<<<(unsigned)nb, SCAN_THREADS, 0, h.stream>>>(in, out, n, total_dev);
     h.launches++;
+    FMM_LAUNCH();
+    return;
+  }
+  if (nb <= SCAN_TWO_TILES) {  // tile sums, then every tile adds the sums before it
+    h.scan_tmp.need(nb * sizeof(int));
+    k_tile_sums<<<(unsigned)nb, SCAN_THREADS, 0, h.stream>>>(in, n, h.scan_tmp.as<int>());
+    k_scan_tiles2<<<(unsigned)nb, SCAN_THREADS, 0, h.stream>>>(in, out, n, h.scan_tmp.as<int>(), total_dev);
+    h.launches += 2;
     FMM_LAUNCH();
     return;
   }
