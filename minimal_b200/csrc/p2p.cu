@@ -174,6 +174,71 @@ __device__ __forceinline__ void pair_f32(float xi, float yi, float zi, const flo
   az = fmaf(dz, qir3, az);
 }
 
+// ---- packed FP32x2 arithmetic (sm_100a): two FP32 lanes per 64-bit value,
+// one instruction for both.  The packed near field evaluates one target
+// against two sources at a time, with the sources staged in pairs:
+// slot 2p = {x_2p, x_2p+1, y_2p, y_2p+1}, slot 2p+1 = {z.., z.., q.., q..}.
+typedef unsigned long long f2x;
+__device__ __forceinline__ f2x pk2(float a, float b) {
+  f2x r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(f2x v, float &a, float &b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ f2x sub2(f2x a, f2x b) {
+  f2x r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2x add2(f2x a, f2x b) {
+  f2x r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2x mul2(f2x a, f2x b) {
+  f2x r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
+  f2x r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// A staged source that adds nothing: zero charge, far from every target.
+constexpr float NEAR_DUMMY = 1e15f;
+
+// One target (X, Y, Z = the coordinate in both lanes) against a staged
+// source pair (sx, sy from the first slot, sz, sq from the second); the same
+// arithmetic as pair_f32 in each lane.
+template <bool CHECK>
+__device__ __forceinline__ void pair_x2(f2x X, f2x Y, f2x Z, f2x sx, f2x sy, f2x sz, f2x sq, f2x &pot, f2x &ax,
+                                        f2x &ay, f2x &az) {
+  const f2x dx = sub2(X, sx), dy = sub2(Y, sy), dz = sub2(Z, sz);
+  float r0, r1;
+  f2x ir;
+  if constexpr (CHECK) {
+    upk2(fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))), r0, r1);
+    ir = pk2(rsqrt_or_zero(r0), rsqrt_or_zero(r1));
+  } else {
+    const f2x tiny = pk2(NEAR_TINY, NEAR_TINY);
+    upk2(fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, tiny))), r0, r1);
+    ir = pk2(rsqrt_approx(r0), rsqrt_approx(r1));
+  }
+  const f2x qir = mul2(sq, ir);
+  const f2x qir3 = mul2(qir, mul2(ir, ir));
+  pot = add2(pot, qir);
+  ax = fma2(dx, qir3, ax);
+  ay = fma2(dy, qir3, ay);
+  az = fma2(dz, qir3, az);
+}
+
 // FP32 P2P: same mapping as k_p2p; FP32 partial sums per source leaf, then a
 // compensated (TwoSum) accumulation per target across the source leaves.
 __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int nleaves, const int *begin,
@@ -330,7 +395,9 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
 #pragma unroll
     for (int q = 0; q < 4; q++) sacc[u][q] = eacc[u][q] = 0;
   const int eb = off[c], ee = off[c + 1];
-  int pre = F32 ? tn : 0;  // slots [0, pre) of this chunk: the target leaf itself (FP32, first chunk)
+  // slots [0, pre) of the first chunk: the target leaf itself (FP32), padded
+  // to an even count (the FP32 stage holds sources in pairs)
+  int pre = F32 ? tn + (tn & 1) : 0;
   for (int e0i = eb; e0i < ee;) {
     // lane k: source leaf k of the chunk candidates
     const int cand = min(32, ee - e0i);
@@ -375,12 +442,19 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
     const int zs = zm ? __shfl_sync(FULL, start, __ffs(zm) - 1) : -1;
     __syncthreads();  // the previous chunk's sweep is done with the buffer
     if constexpr (F32) {
-      for (int j = tid; j < pre; j += CT) {  // the target leaf, in slots [0, tn)
-        BT t = bodies[tb + j];
-        t.x *= scale;
-        t.y *= scale;
-        t.z *= scale;
-        stage[j] = t;
+      for (int pp = tid; 2 * pp < pre; pp += CT) {  // the target leaf, in slots [0, tn), in pairs
+        float4 a = bodies[tb + 2 * pp], b = make_float4(NEAR_DUMMY, NEAR_DUMMY, NEAR_DUMMY, 0.f);
+        a.x *= scale;
+        a.y *= scale;
+        a.z *= scale;
+        if (2 * pp + 1 < tn) {
+          b = bodies[tb + 2 * pp + 1];
+          b.x *= scale;
+          b.y *= scale;
+          b.z *= scale;
+        }
+        stage[2 * pp] = make_float4(a.x, b.x, a.y, b.y);
+        stage[2 * pp + 1] = make_float4(a.z, b.z, a.w, b.w);
       }
     }
     for (int j0 = pre + wid * 32; j0 < T; j0 += CT * CT_UNROLL) {
@@ -413,17 +487,24 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
           sy = -((im / 3) % 3 - 1) * cycle;
           sz = -(im / 9 - 1) * cycle;
         }
-        if (j < T) {
-          BT t;
-          if constexpr (F32) {  // into the target frame, scaled (exact)
-            t.x = fmaf(v[u].x, scale, -sx);
-            t.y = fmaf(v[u].y, scale, -sy);
-            t.z = fmaf(v[u].z, scale, -sz);
-          } else {
-            t.x = v[u].x - sx;
-            t.y = v[u].y - sy;
-            t.z = v[u].z - sz;
+        if constexpr (F32) {  // into the target frame, scaled (exact); stored in source pairs
+          float4 t = make_float4(NEAR_DUMMY, NEAR_DUMMY, NEAR_DUMMY, 0.f);
+          if (j < T) t = make_float4(fmaf(v[u].x, scale, -sx), fmaf(v[u].y, scale, -sy), fmaf(v[u].z, scale, -sz), v[u].w);
+          const float4 o = make_float4(__shfl_xor_sync(FULL, t.x, 1), __shfl_xor_sync(FULL, t.y, 1),
+                                       __shfl_xor_sync(FULL, t.z, 1), __shfl_xor_sync(FULL, t.w, 1));
+          if (j < T) {
+            if ((j & 1) == 0) {  // the pair's first slot (its partner, or a dummy past the end)
+              stage[j] = make_float4(t.x, o.x, t.y, o.y);
+              if (j + 1 == T) stage[j + 1] = make_float4(t.z, NEAR_DUMMY, t.w, 0.f);
+            } else {
+              stage[j] = make_float4(o.z, t.z, o.w, t.w);
+            }
           }
+        } else if (j < T) {
+          BT t;
+          t.x = v[u].x - sx;
+          t.y = v[u].y - sy;
+          t.z = v[u].z - sz;
           t.w = v[u].w;
           stage[j] = t;
         }
@@ -473,51 +554,53 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
         }
       };
       if constexpr (F32) {
-        // the target leaf (its own few slots per thread) with the
+        // packed FP32x2: one target against a staged source pair per step;
+        // the target leaf's own pairs (a few per thread) with the
         // zero-distance check, summed into the first block of the others
-        // (without the check)
-        RT p[CT_TPT][4];
+        // (without the check).  Lane partial sums are combined at each
+        // block's compensated addition.
+        f2x X[CT_TPT], Y[CT_TPT], Z[CT_TPT], acc[CT_TPT][4];
 #pragma unroll
-        for (int u = 0; u < CT_TPT; u++)
+        for (int u = 0; u < CT_TPT; u++) {
+          X[u] = pk2(A[u].x, A[u].x);
+          Y[u] = pk2(A[u].y, A[u].y);
+          Z[u] = pk2(A[u].z, A[u].z);
 #pragma unroll
-          for (int q = 0; q < 4; q++) p[u][q] = 0;
-        auto acc = [&](const BT &sv, auto check) {
+          for (int q = 0; q < 4; q++) acc[u][q] = 0ull;
+        }
+        const f2x *sp2 = (const f2x *)stage;  // pair p: sp2[4p .. 4p + 3] = x, y, z, q pairs
+        auto step = [&](int pp, auto check) {
           constexpr bool CHECK = decltype(check)::value;
+          const ulonglong2 s0 = ((const ulonglong2 *)sp2)[2 * pp], s1 = ((const ulonglong2 *)sp2)[2 * pp + 1];
 #pragma unroll
           for (int u = 0; u < CT_TPT; u++)
-            pair_f32<CHECK>(A[u].x, A[u].y, A[u].z, sv, p[u][0], p[u][1], p[u][2], p[u][3]);
+            pair_x2<CHECK>(X[u], Y[u], Z[u], s0.x, s0.y, s1.x, s1.y, acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
         };
         auto flush = [&]() {  // one compensated addition per block
 #pragma unroll
           for (int u = 0; u < CT_TPT; u++)
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-              two_sum_acc(sacc[u][q], eacc[u][q], p[u][q]);
-              p[u][q] = 0;
+              float lo, hi;
+              upk2(acc[u][q], lo, hi);
+              two_sum_acc(sacc[u][q], eacc[u][q], lo + hi);
+              acc[u][q] = 0ull;
             }
         };
-        for (int cs = divG(g * pre), ce = divG((g + 1) * pre); cs < ce; cs++) acc(stage[cs], std::true_type{});
-        const int rest = T - pre, from = pre + divG(g * rest), to = pre + divG((g + 1) * rest);
-        const BT *sp = stage + from;
-        for (int c0 = from; c0 < to; c0 += CT_BLOCK) {
-          const int cend = min(to, c0 + CT_BLOCK);
-          int cs = c0;
-          for (; cs + 4 <= cend; cs += 4) {
-            const BT s0 = sp[0], s1 = sp[1], s2 = sp[2], s3 = sp[3];
-            sp += 4;
-            acc(s0, std::false_type{});
-            acc(s1, std::false_type{});
-            acc(s2, std::false_type{});
-            acc(s3, std::false_type{});
+        const int nps = pre / 2, npt = (T + 1) / 2;  // pairs of the target leaf, of the chunk
+        for (int pp = divG(g * nps), pe = divG((g + 1) * nps); pp < pe; pp++) step(pp, std::true_type{});
+        const int rest = npt - nps, from = nps + divG(g * rest), to = nps + divG((g + 1) * rest);
+        for (int c0 = from; c0 < to; c0 += CT_BLOCK / 2) {
+          const int cend = min(to, c0 + CT_BLOCK / 2);
+          int pp = c0;
+          for (; pp + 2 <= cend; pp += 2) {
+            step(pp, std::false_type{});
+            step(pp + 1, std::false_type{});
           }
-          for (; cs < cend; cs++) {
-            const BT s0 = sp[0];
-            sp += 1;
-            acc(s0, std::false_type{});
-          }
+          if (pp < cend) step(pp, std::false_type{});
           flush();
         }
-        if (from == to && pre) flush();  // only the target leaf's slots
+        if (from == to && nps) flush();  // only the target leaf's pairs
       } else {
         sweep(g * T / G, (g + 1) * T / G, std::true_type{});
       }
