@@ -205,6 +205,25 @@ def timed_steps(fmm, steps, flush, torch):
     return phase, launches
 
 
+def isolated_phases(fmm, reps, flush, torch):
+    """Per-phase device times of `reps` evaluations through the step API, in
+    which each phase runs alone on the GPU (a whole evaluation runs the near
+    field beside the far field): the kernel durations for the roofline."""
+    phase = {"p2p": [], "m2l": []}
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        fmm.build_tree()
+        fmm.build_lists()
+        fmm.upward()
+        fmm.horizontal()
+        fmm.downward()
+        t = fmm.timings()
+        phase["p2p"].append(t["p2p"])
+        phase["m2l"].append(t["m2l"])
+    return phase
+
+
 def errors_vs_direct(fmm, n, out=None):
     """Relative L2 error of p and F on 1000 stride-sampled tree positions
     against FP64 direct summation on the GPU."""
@@ -421,8 +440,9 @@ def run_ours(a, rank, world, local_rank):
     pairs, n_m2l = pair_count(fmm)
     mixed = a.precision == "mixed"
     peak_fma = fmm.fma_peak("mixed" if mixed else "fp64")
-    m2l_ms = statistics.mean(phase["m2l"])
-    p2p_ms = statistics.mean(phase["p2p"])
+    iso = isolated_phases(fmm, 3, flush, torch)
+    m2l_ms = statistics.mean(iso["m2l"])
+    p2p_ms = statistics.mean(iso["p2p"])
     p2p_flops = pairs * 20
     m2l_flops = n_m2l * m2l_flops_per_pair(a.P)
     p2p_tf = p2p_flops / (p2p_ms * 1e-3) / 1e12
@@ -443,7 +463,11 @@ def run_ours(a, rank, world, local_rank):
                            " FMA-pipe peak on this GPU (dependent-chain microbenchmark, exafmm_b200_fma_peak); "
                            "the pool's MEASURED_PEAKS.json has no FP32/FP64 figure",
             "flops_per_launch": p2p_flops, "flops_per_unit": "20 per body pair (3d/kernel.h:133-142)",
-            "time": "P2P phase events (source conversion + near-field kernel)"}
+            "time": "P2P phase events of 3 step-API evaluations after the timed region, the near field "
+                    "alone on the GPU (source conversion + near-field kernel)",
+            "in_step_ms": statistics.mean(phase["p2p"]),
+            "in_step_note": "P2P phase events inside the timed evaluations, where the near field shares the "
+                            "SMs with the far field on a second stream"}
     roof_m2l = None
     if mixed and peaks.get("bf16_tflops"):
         roof_m2l = {"bound": "tensor", "kernel": "k_m2l_tc (grouped M2L, tcgen05 split-FP16) + grouping",
@@ -451,7 +475,8 @@ def run_ours(a, rank, world, local_rank):
                     "frac": m2l_tf / peaks["bf16_tflops"], "peak_source": "MEASURED_PEAKS.json bf16 burst",
                     "flops_per_launch": m2l_flops,
                     "flops_per_unit": f"{m2l_flops_per_pair(a.P)} per M2L pair (dense realified, truncated)",
-                    "time": "M2L phase events (grouping kernels + contraction + residual)",
+                    "time": "M2L phase events of 3 step-API evaluations after the timed region (grouping "
+                            "kernels + contraction + residual, alone on the GPU)",
                     "traffic": traffic.get("k_m2l_tc", {}).get("bytes_per_launch_1M")}
 
     extra = {}

@@ -90,11 +90,12 @@ __global__ void k_direct_back(const double4 *pf, long n, double *rec) {
 struct Timer {
   Handle &h;
   int ph;
-  Timer(Handle &h_, int p) : h(h_), ph(p) {
-    if (h.ev_ok) cudaEventRecord(h.ev[ph][0], h.stream);
+  cudaStream_t s;
+  Timer(Handle &h_, int p, cudaStream_t s_ = nullptr) : h(h_), ph(p), s(s_ ? s_ : h_.stream) {
+    if (h.ev_ok) cudaEventRecord(h.ev[ph][0], s);
   }
   ~Timer() {
-    if (h.ev_ok) cudaEventRecord(h.ev[ph][1], h.stream);
+    if (h.ev_ok) cudaEventRecord(h.ev[ph][1], s);
   }
 };
 
@@ -141,7 +142,7 @@ void do_horiz(Handle &h) {
   }
   {
     Timer t(h, PH_P2P);
-    p2p_pass(h);
+    p2p_pass(h, h.stream);
   }
   h.have_horiz = true;
 }
@@ -151,6 +152,40 @@ void do_down(Handle &h) {
   Timer t(h, PH_DOWN);
   downward_pass(h);
   h.have_down = true;
+}
+
+void sync(Handle &h);
+
+// A whole evaluation.  The near field needs only the tree, the lists and the
+// bodies, and only L2P reads what it writes (L2P adds into the near-field
+// sums), so it runs on the side stream from the lists until the downward
+// pass, filling the SMs that the far field's per-level launches and its
+// host read of the group counts leave idle.  The far field's stream has the
+// higher priority.
+void run_all(Handle &h) {
+  do_tree(h);
+  do_lists(h);
+  if (h.prm.precision == EXAFMM_MIXED) make_srcf(h);  // read by P2M and the near field
+  FMM_CUDA(cudaEventRecord(h.fork_ev, h.stream));
+  FMM_CUDA(cudaStreamWaitEvent(h.side, h.fork_ev, 0));
+  {
+    Timer t(h, PH_P2P, h.side);
+    p2p_pass(h, h.side);
+  }
+  FMM_CUDA(cudaEventRecord(h.join_ev, h.side));
+  try {
+    do_up(h);
+    Timer t(h, PH_M2L);
+    m2l_pass(h);
+    periodic_pass(h);
+  } catch (...) {
+    cudaStreamSynchronize(h.side);  // nothing of this evaluation stays in flight
+    throw;
+  }
+  FMM_CUDA(cudaStreamWaitEvent(h.stream, h.join_ev, 0));
+  h.have_horiz = true;
+  do_down(h);
+  sync(h);
 }
 
 void sync(Handle &h) {
@@ -198,7 +233,12 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     Handle &h = H->h;
     h.prm = *params;
     h.nterm = nterm_of(params->P);
-    FMM_CUDA(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    int least = 0, greatest = 0;
+    FMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    FMM_CUDA(cudaStreamCreateWithPriority(&h.stream, cudaStreamNonBlocking, greatest));
+    FMM_CUDA(cudaStreamCreateWithPriority(&h.side, cudaStreamNonBlocking, least));
+    FMM_CUDA(cudaEventCreateWithFlags(&h.fork_ev, cudaEventDisableTiming));
+    FMM_CUDA(cudaEventCreateWithFlags(&h.join_ev, cudaEventDisableTiming));
     FMM_CUDA(cudaMallocHost(&h.flags_host, 4 * sizeof(int)));
     h.flags_host[0] = 0;
     h.ev_ok = true;
@@ -225,6 +265,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
   Handle &h = H->h;
   cudaSetDevice(h.prm.device);
   if (h.stream) cudaStreamSynchronize(h.stream);
+  if (h.side) cudaStreamSynchronize(h.side);
   Buf *bufs[] = {&h.in, &h.src, &h.out, &h.perm, &h.srcf, &h.keys[0], &h.keys[1], &h.vals[0], &h.vals[1],
                  &h.lfirst, &h.chain, &h.prebase, &h.scan_tmp, &h.hist, &h.c_begin, &h.c_count, &h.c_child,
                  &h.c_nchild, &h.c_parent, &h.c_level, &h.c_xr, &h.c_pre, &h.c_ref, &h.c_leaf_of_body,
@@ -237,6 +278,9 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
     for (int p = 0; p < PH_COUNT + 1; p++)
       for (int k = 0; k < 2; k++) cudaEventDestroy(h.ev[p][k]);
   if (h.stream) cudaStreamDestroy(h.stream);
+  if (h.side) cudaStreamDestroy(h.side);
+  if (h.fork_ev) cudaEventDestroy(h.fork_ev);
+  if (h.join_ev) cudaEventDestroy(h.join_ev);
   if (h.flags_host) cudaFreeHost(h.flags_host);
   if (h.keys_host) cudaFreeHost(h.keys_host);
   delete H;
@@ -341,12 +385,7 @@ int exafmm_b200_downward(exafmm_b200 *H) {
 int exafmm_b200_evaluate(exafmm_b200 *H) {
   return guarded(H, [&](Handle &h) {
     h.launches = 0;
-    do_tree(h);
-    do_lists(h);
-    do_up(h);
-    do_horiz(h);
-    do_down(h);
-    sync(h);
+    run_all(h);
   });
 }
 
@@ -365,12 +404,7 @@ int exafmm_b200_autotune(exafmm_b200 *H, const int *candidates, int ncand, int r
     if (repeats < 1 || repeats > 100) throw Error{EXAFMM_ERR_ARG, "autotune(): repeats in [1, 100]"};
     auto run = [&]() {
       h.launches = 0;
-      do_tree(h);
-      do_lists(h);
-      do_up(h);
-      do_horiz(h);
-      do_down(h);
-      sync(h);
+      run_all(h);
       return (double)h.ms[PH_COUNT];
     };
     int best = -1;

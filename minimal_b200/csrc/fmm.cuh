@@ -91,6 +91,10 @@ struct Handle {
   int nterm = 0;
   std::string err;
   cudaStream_t stream = nullptr;
+  // a whole evaluation runs the near field on `side` (lower priority), from
+  // the lists until the downward pass, beside the far field on `stream`
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int64_t launches = 0;
 
   // bodies; a batch holds nsys independent systems, system q owning input
@@ -182,7 +186,7 @@ void downward_pass(Handle &h);
 // m2l.cu
 void m2l_pass(Handle &h);
 // p2p.cu
-void p2p_pass(Handle &h);
+void p2p_pass(Handle &h, cudaStream_t s);  // s: h.stream, or h.side once the FP32 sources are made
 void make_srcf(Handle &h);
 void direct_sum(Handle &h, double4 *targets_pq /*x,y,z,q*/, double4 *out, long nt);
 // periodic.cu

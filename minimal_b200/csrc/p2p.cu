@@ -647,18 +647,19 @@ void p2p_set_attributes() {
                        ct_cap<true>() * (int)sizeof(float4));
 }
 
-void p2p_pass(Handle &h) {
+void p2p_pass(Handle &h, cudaStream_t s) {
   h.out.need((size_t)h.n * sizeof(double4));
   const double cyc = h.prm.images ? h.prm.cycle : 0.0;
   const bool cta = h.prm.ncrit <= CT_MAXTGT;  // every leaf fits two targets per thread and the buffer
   if (h.prm.precision == EXAFMM_MIXED) {
+    if (s != h.stream && !h.srcf_ready) throw Error{EXAFMM_ERR_STATE, "near field on a side stream before its sources"};
     make_srcf(h);
     if (cta)
-      k_p2p_cta<true><<<h.nleaves, CT, ct_cap<true>() * sizeof(float4), h.stream>>>(
+      k_p2p_cta<true><<<h.nleaves, CT, ct_cap<true>() * sizeof(float4), s>>>(
           h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
           h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
     else
-      k_p2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
+      k_p2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, s>>>(
           h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
           h.p2p_ent.as<u32>(), h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
     h.launches++;
@@ -666,11 +667,11 @@ void p2p_pass(Handle &h) {
     return;
   }
   if (cta)
-    k_p2p_cta<false><<<h.nleaves, CT, ct_cap<false>() * sizeof(double4), h.stream>>>(
+    k_p2p_cta<false><<<h.nleaves, CT, ct_cap<false>() * sizeof(double4), s>>>(
         h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
         h.c_xr.as<double4>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
   else
-    k_p2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, h.stream>>>(
+    k_p2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, s>>>(
         h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
         h.p2p_ent.as<u32>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
   h.launches++;
