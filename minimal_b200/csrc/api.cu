@@ -128,7 +128,7 @@ void do_lists(Handle &h) {
 void do_up(Handle &h) {
   need_tree(h);
   Timer t(h, PH_UP);
-  upward_pass(h);
+  upward_pass(h, h.stream);
   h.have_up = true;
 }
 
@@ -150,41 +150,55 @@ void do_horiz(Handle &h) {
 void do_down(Handle &h) {
   if (!h.have_horiz) throw Error{EXAFMM_ERR_STATE, "horizontal() must run before downward()"};
   Timer t(h, PH_DOWN);
-  downward_pass(h);
+  downward_pass(h, h.stream, nullptr);
   h.have_down = true;
 }
 
 void sync(Handle &h);
 
-// A whole evaluation.  The near field needs only the tree, the lists and the
-// bodies, and only L2P reads what it writes (L2P adds into the near-field
-// sums), so it runs on the side stream from the lists until the downward
-// pass, filling the SMs that the far field's per-level launches and its
-// host read of the group counts leave idle.  The far field's stream has the
-// higher priority.
+// A whole evaluation on three streams.  The upward pass needs only the tree
+// and the FP32 sources, so it runs on `aux` beside the dual-tree walk.  The
+// near field needs the tree, the lists and the bodies, and only L2P reads
+// what it writes (L2P adds into the near-field sums), so it runs on `side`
+// from the lists until L2P, filling the SMs that the far field's per-level
+// launches and its host read of the group counts leave idle.  The far field
+// and the upward pass have the higher stream priority.
 void run_all(Handle &h) {
   do_tree(h);
-  do_lists(h);
   if (h.prm.precision == EXAFMM_MIXED) make_srcf(h);  // read by P2M and the near field
   FMM_CUDA(cudaEventRecord(h.fork_ev, h.stream));
-  FMM_CUDA(cudaStreamWaitEvent(h.side, h.fork_ev, 0));
-  {
-    Timer t(h, PH_P2P, h.side);
-    p2p_pass(h, h.side);
-  }
-  FMM_CUDA(cudaEventRecord(h.join_ev, h.side));
   try {
-    do_up(h);
+    FMM_CUDA(cudaStreamWaitEvent(h.aux, h.fork_ev, 0));
+    {
+      Timer t(h, PH_UP, h.aux);
+      upward_pass(h, h.aux);
+    }
+    FMM_CUDA(cudaEventRecord(h.up_ev, h.aux));
+    h.have_up = true;
+    do_lists(h);
+    FMM_CUDA(cudaEventRecord(h.lists_ev, h.stream));
+    FMM_CUDA(cudaStreamWaitEvent(h.side, h.lists_ev, 0));
+    {
+      Timer t(h, PH_P2P, h.side);
+      p2p_pass(h, h.side);
+    }
+    FMM_CUDA(cudaEventRecord(h.join_ev, h.side));
+    FMM_CUDA(cudaStreamWaitEvent(h.stream, h.up_ev, 0));
     Timer t(h, PH_M2L);
     m2l_pass(h);
     periodic_pass(h);
   } catch (...) {
-    cudaStreamSynchronize(h.side);  // nothing of this evaluation stays in flight
+    // nothing of this evaluation stays in flight
+    cudaStreamSynchronize(h.aux);
+    cudaStreamSynchronize(h.side);
     throw;
   }
-  FMM_CUDA(cudaStreamWaitEvent(h.stream, h.join_ev, 0));
   h.have_horiz = true;
-  do_down(h);
+  {
+    Timer t(h, PH_DOWN);
+    downward_pass(h, h.stream, h.join_ev);
+  }
+  h.have_down = true;
   sync(h);
 }
 
@@ -237,8 +251,9 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     FMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     FMM_CUDA(cudaStreamCreateWithPriority(&h.stream, cudaStreamNonBlocking, greatest));
     FMM_CUDA(cudaStreamCreateWithPriority(&h.side, cudaStreamNonBlocking, least));
-    FMM_CUDA(cudaEventCreateWithFlags(&h.fork_ev, cudaEventDisableTiming));
-    FMM_CUDA(cudaEventCreateWithFlags(&h.join_ev, cudaEventDisableTiming));
+    FMM_CUDA(cudaStreamCreateWithPriority(&h.aux, cudaStreamNonBlocking, greatest));
+    for (cudaEvent_t *e : {&h.fork_ev, &h.up_ev, &h.lists_ev, &h.join_ev})
+      FMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     FMM_CUDA(cudaMallocHost(&h.flags_host, 4 * sizeof(int)));
     h.flags_host[0] = 0;
     h.ev_ok = true;
@@ -266,6 +281,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
   cudaSetDevice(h.prm.device);
   if (h.stream) cudaStreamSynchronize(h.stream);
   if (h.side) cudaStreamSynchronize(h.side);
+  if (h.aux) cudaStreamSynchronize(h.aux);
   Buf *bufs[] = {&h.in, &h.src, &h.out, &h.perm, &h.srcf, &h.keys[0], &h.keys[1], &h.vals[0], &h.vals[1],
                  &h.lfirst, &h.chain, &h.prebase, &h.scan_tmp, &h.hist, &h.c_begin, &h.c_count, &h.c_child,
                  &h.c_nchild, &h.c_parent, &h.c_level, &h.c_xr, &h.c_pre, &h.c_ref, &h.c_leaf_of_body,
@@ -279,8 +295,9 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
       for (int k = 0; k < 2; k++) cudaEventDestroy(h.ev[p][k]);
   if (h.stream) cudaStreamDestroy(h.stream);
   if (h.side) cudaStreamDestroy(h.side);
-  if (h.fork_ev) cudaEventDestroy(h.fork_ev);
-  if (h.join_ev) cudaEventDestroy(h.join_ev);
+  if (h.aux) cudaStreamDestroy(h.aux);
+  for (cudaEvent_t e : {h.fork_ev, h.up_ev, h.lists_ev, h.join_ev})
+    if (e) cudaEventDestroy(e);
   if (h.flags_host) cudaFreeHost(h.flags_host);
   if (h.keys_host) cudaFreeHost(h.keys_host);
   delete H;

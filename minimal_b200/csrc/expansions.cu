@@ -765,11 +765,11 @@ TermTable table_view(const Handle &h, int P, int dir) {
 }
 
 // Unit offset harmonics and term tables for order P (cached per handle).
-void unit_tables(Handle &h) {
+void unit_tables(Handle &h, cudaStream_t s) {
   const int P = h.prm.P;
   if (h.shift_P == P) return;
   h.shift_ops.need((size_t)16 * tri(P) * sizeof(double2));
-  k_unit_tables<<<16, 32, 0, h.stream>>>(P, h.shift_ops.as<double2>());
+  k_unit_tables<<<16, 32, 0, s>>>(P, h.shift_ops.as<double2>());
   h.launches++;
   FMM_LAUNCH();
   const std::vector<int> t = term_tables(P, h.shift_at);
@@ -778,12 +778,12 @@ void unit_tables(Handle &h) {
   h.shift_P = P;
 }
 
-void upward_pass(Handle &h) {
-  cudaStream_t s = h.stream;
+void upward_pass(Handle &h, cudaStream_t s) {
   const int P = h.prm.P, nt = tri(P);
   h.M.need((size_t)h.ncells * nt * sizeof(double2));
   h.L.need((size_t)h.ncells * nt * sizeof(double2));
   if (h.prm.precision == EXAFMM_MIXED) {
+    if (s != h.stream && !h.srcf_ready) throw Error{EXAFMM_ERR_STATE, "upward pass on a side stream before its sources"};
     make_srcf(h);
     const dim3 grid(grid_for(h.nleaves, WARPS)), block(WARPS * 32);
     const size_t sm = WARPS * nt * sizeof(double2);
@@ -813,7 +813,7 @@ void upward_pass(Handle &h) {
   }
   h.launches++;
   FMM_LAUNCH();
-  unit_tables(h);
+  unit_tables(h, s);
   for (int l = h.depth - 1; l >= 0; l--) {
     const int c0 = h.level_base[l], c1 = h.level_base[l + 1];
     if (c1 <= c0) continue;
@@ -830,10 +830,9 @@ void upward_pass(Handle &h) {
   }
 }
 
-void downward_pass(Handle &h) {
-  cudaStream_t s = h.stream;
+void downward_pass(Handle &h, cudaStream_t s, cudaEvent_t before_l2p) {
   const int P = h.prm.P, nt = tri(P);
-  unit_tables(h);
+  unit_tables(h, s);
   for (int l = 0; l < h.depth; l++) {  // parents at level l push to their children
     const int c0 = h.level_base[l], c1 = h.level_base[l + 1];
     if (c1 <= c0) continue;
@@ -853,6 +852,8 @@ void downward_pass(Handle &h) {
     h.launches++;
     FMM_LAUNCH();
   }
+  // L2P adds into the near-field sums
+  if (before_l2p) FMM_CUDA(cudaStreamWaitEvent(s, before_l2p, 0));
   if (h.prm.precision == EXAFMM_MIXED) {
     make_srcf(h);
     const dim3 grid(grid_for(h.nleaves, WARPS)), block(WARPS * 32);

@@ -94,7 +94,9 @@ struct Handle {
   // a whole evaluation runs the near field on `side` (lower priority), from
   // the lists until the downward pass, beside the far field on `stream`
   cudaStream_t side = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  // ... and the upward pass on `aux`, beside the dual-tree walk
+  cudaStream_t aux = nullptr;
+  cudaEvent_t fork_ev = nullptr, up_ev = nullptr, lists_ev = nullptr, join_ev = nullptr;
   int64_t launches = 0;
 
   // bodies; a batch holds nsys independent systems, system q owning input
@@ -181,8 +183,9 @@ void build_lists(Handle &h);
 void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img);
 void order_m2l_lists(Handle &h);
 // expansions.cu
-void upward_pass(Handle &h);
-void downward_pass(Handle &h);
+void upward_pass(Handle &h, cudaStream_t s);
+// before_l2p: an event the stream waits for before L2P (or nullptr)
+void downward_pass(Handle &h, cudaStream_t s, cudaEvent_t before_l2p);
 // m2l.cu
 void m2l_pass(Handle &h);
 // p2p.cu
