@@ -92,7 +92,10 @@ EXAFMM_API int exafmm_b200_upward(exafmm_b200 *h);
 EXAFMM_API int exafmm_b200_horizontal(exafmm_b200 *h);
 EXAFMM_API int exafmm_b200_downward(exafmm_b200 *h);
 
-/* All phases: tree, lists, upward, horizontal, downward (3d/fmm.cxx:40-53). */
+/* All phases: tree, lists, upward, horizontal, downward (3d/fmm.cxx:40-53).
+ * The handle runs them on three streams: the upward pass beside the list
+ * build, the near field beside the M2L and L2L; the results are those of
+ * the calls above made one after another. */
 EXAFMM_API int exafmm_b200_evaluate(exafmm_b200 *h);
 
 /* Results.  get_bodies writes N Body records in tree order (X,q as sorted,
@@ -166,8 +169,9 @@ EXAFMM_API int exafmm_b200_autotune(exafmm_b200 *h, const int *ncrit_candidates,
                                     int *best_ncrit, double *best_ms);
 
 /* Per-phase device times of the last evaluation in milliseconds, measured
- * with CUDA events on the handle's stream: tree, lists, upward, m2l, p2p,
- * downward, total (7 values). */
+ * with CUDA events on the stream each phase ran on: tree, lists, upward, m2l,
+ * p2p, downward, total (7 values).  In evaluate() phases overlap, so the
+ * phase times add up to more than the total. */
 EXAFMM_API int exafmm_b200_get_timings(exafmm_b200 *h, double *ms7);
 
 /* Library information: number of kernel launches issued by the last
