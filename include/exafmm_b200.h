@@ -98,6 +98,18 @@ EXAFMM_API int exafmm_b200_downward(exafmm_b200 *h);
  * the calls above made one after another. */
 EXAFMM_API int exafmm_b200_evaluate(exafmm_b200 *h);
 
+/* Repeated evaluations on fixed positions (an FMM matrix-vector product with
+ * new charges each time).  set_charges replaces the charges (N doubles in
+ * the input order of set_bodies / set_batch; a non-finite value is rejected
+ * and nothing changes) and keeps the tree and the interaction lists, which
+ * depend on the positions only.  reevaluate then runs upward, horizontal and
+ * downward over the kept tree and lists: the lazy traversal's evaluate()
+ * over its stored lists (3d/traverse_lazy.h:46-62).  Results are those of
+ * evaluate() on the same bodies; reevaluate needs a tree and lists from an
+ * earlier evaluate() or build_lists(). */
+EXAFMM_API int exafmm_b200_set_charges(exafmm_b200 *h, const double *q, int where);
+EXAFMM_API int exafmm_b200_reevaluate(exafmm_b200 *h);
+
 /* Results.  get_bodies writes N Body records in tree order (X,q as sorted,
  * p,F = FMM result) to host or device memory.  get_perm writes, per tree
  * position, the input index of that body. */

@@ -38,6 +38,7 @@ API = [
     "exafmm_b200_get_lists", "exafmm_b200_get_expansions", "exafmm_b200_direct", "exafmm_b200_get_timings",
     "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak", "exafmm_b200_direct_static",
     "exafmm_b200_dipole_correction", "exafmm_b200_ewald", "exafmm_b200_set_batch", "exafmm_b200_autotune",
+    "exafmm_b200_set_charges", "exafmm_b200_reevaluate",
 ]
 
 PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
@@ -96,6 +97,8 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_ewald": (i, [vp, i, d, d, d, vp, i64, i]),
         "exafmm_b200_set_batch": (i, [vp, vp, vp, i, i]),
         "exafmm_b200_autotune": (i, [vp, vp, i, i, vp, vp]),
+        "exafmm_b200_set_charges": (i, [vp, vp, i]),
+        "exafmm_b200_reevaluate": (i, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -206,6 +209,19 @@ class FMM:
 
     def evaluate(self):
         self._check(self.lib.exafmm_b200_evaluate(self.h))
+
+    def set_charges(self, q):
+        """New charges (N values, input order of set_bodies / set_batch) on
+        the same positions: the tree and the interaction lists are kept."""
+        q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).ravel())
+        if len(q) != self.n:
+            raise ValueError(f"need {self.n} charges, got {len(q)}")
+        self._check(self.lib.exafmm_b200_set_charges(self.h, _p(q), HOST))
+
+    def reevaluate(self):
+        """Upward, horizontal and downward passes over the kept tree and
+        lists (after set_charges, or again on the same bodies)."""
+        self._check(self.lib.exafmm_b200_reevaluate(self.h))
 
     # ---- results
     def bodies(self):

@@ -63,6 +63,20 @@ __global__ void k_pack_in(const double *rec, long n, double4 *in, int *bad) {
   in[i] = v;
 }
 
+__global__ void k_check_finite(const double *q, long n, int *bad) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !isfinite(q[i])) *bad = 1;
+}
+
+// New charges in input order: the caller-order bodies, and (once a tree
+// exists) the tree-order bodies through the permutation.
+__global__ void k_set_charges(const double *q, long n, double4 *in, const int *perm, double4 *src) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  in[i].w = q[i];
+  if (src) src[i].w = q[perm[i]];
+}
+
 __global__ void k_unpack_out(const double4 *src, const double4 *out, long n, double *rec) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -163,8 +177,15 @@ void sync(Handle &h);
 // from the lists until L2P, filling the SMs that the far field's per-level
 // launches and its host read of the group counts leave idle.  The far field
 // and the upward pass have the higher stream priority.
-void run_all(Handle &h) {
-  do_tree(h);
+void run_all(Handle &h, bool rebuild) {
+  if (rebuild) {
+    do_tree(h);
+  } else {
+    if (!h.have_lists) throw Error{EXAFMM_ERR_STATE, "reevaluate() needs the tree and lists of an earlier evaluation"};
+    if (h.ev_ok)  // tree and lists kept: zero time, and the total starts here
+      for (int p : {PH_TREE, PH_LISTS})
+        for (int k = 0; k < 2; k++) cudaEventRecord(h.ev[p][k], h.stream);
+  }
   if (h.prm.precision == EXAFMM_MIXED) make_srcf(h);  // read by P2M and the near field
   FMM_CUDA(cudaEventRecord(h.fork_ev, h.stream));
   try {
@@ -175,7 +196,7 @@ void run_all(Handle &h) {
     }
     FMM_CUDA(cudaEventRecord(h.up_ev, h.aux));
     h.have_up = true;
-    do_lists(h);
+    if (rebuild) do_lists(h);
     FMM_CUDA(cudaEventRecord(h.lists_ev, h.stream));
     FMM_CUDA(cudaStreamWaitEvent(h.side, h.lists_ev, 0));
     {
@@ -402,7 +423,46 @@ int exafmm_b200_downward(exafmm_b200 *H) {
 int exafmm_b200_evaluate(exafmm_b200 *H) {
   return guarded(H, [&](Handle &h) {
     h.launches = 0;
-    run_all(h);
+    run_all(h, true);
+  });
+}
+
+int exafmm_b200_reevaluate(exafmm_b200 *H) {
+  return guarded(H, [&](Handle &h) {
+    h.launches = 0;
+    run_all(h, false);
+  });
+}
+
+int exafmm_b200_set_charges(exafmm_b200 *H, const double *q, int where) {
+  return guarded(H, [&](Handle &h) {
+    if (!q) throw Error{EXAFMM_ERR_ARG, "null charges"};
+    if (where != EXAFMM_HOST && where != EXAFMM_DEVICE) throw Error{EXAFMM_ERR_ARG, "where must be HOST or DEVICE"};
+    if (h.n <= 0) throw Error{EXAFMM_ERR_STATE, "no bodies loaded"};
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    const double *dq = q;
+    if (where == EXAFMM_HOST) {
+      h.stage.need(h.n * sizeof(double));
+      FMM_CUDA(cudaMemcpyAsync(h.stage.p, q, h.n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+      dq = h.stage.as<double>();
+    }
+    int *bad = &h.counters.as<DevCounters>()->overflow;
+    FMM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), h.stream));
+    k_check_finite<<<grid_for(h.n, 256), 256, 0, h.stream>>>(dq, h.n, bad);
+    h.launches++;
+    FMM_LAUNCH();
+    int hb = 0;
+    FMM_CUDA(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    FMM_CUDA(cudaStreamSynchronize(h.stream));
+    if (hb) throw Error{EXAFMM_ERR_ARG, "non-finite charge"};  // nothing changed
+    k_set_charges<<<grid_for(h.n, 256), 256, 0, h.stream>>>(dq, h.n, h.in.as<double4>(), h.perm.as<int>(),
+                                                           h.have_tree ? h.src.as<double4>() : nullptr);
+    h.launches++;
+    FMM_LAUNCH();
+    FMM_CUDA(cudaStreamSynchronize(h.stream));
+    // the tree and the lists depend on the positions only; everything after them is redone
+    h.srcf_ready = false;
+    h.have_up = h.have_horiz = h.have_down = false;
   });
 }
 
@@ -421,7 +481,7 @@ int exafmm_b200_autotune(exafmm_b200 *H, const int *candidates, int ncand, int r
     if (repeats < 1 || repeats > 100) throw Error{EXAFMM_ERR_ARG, "autotune(): repeats in [1, 100]"};
     auto run = [&]() {
       h.launches = 0;
-      run_all(h);
+      run_all(h, true);
       return (double)h.ms[PH_COUNT];
     };
     int best = -1;
