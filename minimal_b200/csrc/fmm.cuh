@@ -158,6 +158,12 @@ struct Handle {
   int *keys_host = nullptr;  // pinned: the group keys read with the counts
   int g_ntiles = 0, g_ngroups = 0, g_nseg = 0;
   bool g_used_tc = false;
+  // the grouping of the last grouped M2L (tiles, segments, operator slots),
+  // valid for the same lists, P and form: a reevaluation contracts directly
+  struct {
+    bool valid = false, tcore = false, ordered = false;
+    int P = 0, nres = 0;
+  } g_plan;
   bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only
 
   // phase state

@@ -283,6 +283,7 @@ void order_m2l_lists(Handle &h) {
 
 void build_lists(Handle &h) {
   cudaStream_t s = h.stream;
+  h.g_plan.valid = false;  // new lists: the M2L grouping is redone
   DevCounters *ctr = h.counters.as<DevCounters>();
   const int C = h.ncells;
   // capacities: kept between calls, never below a size estimate for this tree

@@ -773,6 +773,32 @@ void m2l_grouped_set_attributes() {
 // M2L entry), residual entries added by the direct-form kernel.  FP64 form:
 // DMMA over tiles of 32 targets; mixed form: tcgen05 split-FP16 over tiles of
 // 128 targets (orders whose operator does not fit fall back to DMMA).
+// The contraction over the grouping held in the handle (tiles, segment
+// tables, operator slots) with this evaluation's scaled multipoles.
+void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan &gp, const PlanDev &pd) {
+  cudaStream_t s = h.stream;
+  const int P = h.prm.P, ntiles = h.g_ntiles, tile_n = tcore ? TC_TILE : GP_TILE;
+  const long nseg = h.g_nseg;
+  int *tg_src = h.g_tg.as<int>(), *tg_gid = tg_src + (size_t)nseg * tile_n, *tg_off = tg_gid + nseg;
+  DevCounters *ctr = h.counters.as<DevCounters>();
+  if (tcore) {
+    FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
+    const uint32_t hc = tc_half_cols(KP16);
+    k_m2l_tc<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                    h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
+                                                    h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
+                                                    tc_stages(tp), hc, 4 * hc <= 512 ? 1 : 0, TC_FLUSH_EVERY,
+                                                    &ctr->tc_error, 20000000L);
+    FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    h.g_used_tc = true;
+  } else {
+    k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                            h.g_ops.as<double>(), h.g_mt.as<double>(),
+                                                            h.c_xr.as<double4>(), h.L.as<double2>(), pd);
+  }
+  h.launches++;
+}
+
 void m2l_grouped_pass(Handle &h) {
   cudaStream_t s = h.stream;
   const int P = h.prm.P, NT = tri(P), C = h.ncells;
@@ -798,6 +824,14 @@ void m2l_grouped_pass(Handle &h) {
     h.g_mt.need((size_t)C * gp.KP * sizeof(double));
     k_mscale<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>(C, P, gp.KP, h.c_xr.as<double4>(), h.M.as<double2>(),
                                                           h.g_mt.as<double>());
+  }
+  // same lists, P and form as the last grouping: contract directly
+  if (h.g_plan.valid && h.g_plan.P == P && h.g_plan.tcore == tcore && h.g_plan.ordered == h.m2l_ordered) {
+    if (h.g_ngroups > 0) contract(h, tcore, tp, KP16, gp, pd);
+    h.launches++;
+    FMM_LAUNCH();
+    if (h.g_plan.nres > 0) m2l_residual(h, h.m2l_ordered ? h.g_ekey.as<int>() : h.m2l_key.as<int>());
+    return;
   }
   // the entries and their group keys: the walk's raw pairs with the keys
   // (and key / target occupancy) it produced, or the ordered CSR lists
@@ -846,6 +880,7 @@ void m2l_grouped_pass(Handle &h) {
     m2l_grouped_pass(h);
     return;
   }
+  h.g_ngroups = ngroups;
   if (ngroups > 0) {
     // operators: cached per handle by group key (they depend only on the key
     // and P); only keys not seen before are built
@@ -931,29 +966,17 @@ void m2l_grouped_pass(Handle &h) {
     k_gfill<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, ekey, gidx, tslot, tile_n, ngroups, segid, tg_src);
     k_seg_gid<<<grid_for(nmark, TB), TB, 0, s>>>(nmark, ngroups, mark, segid, d_slot_of, tg_gid);
     k_tg_off<<<grid_for(ntiles + 1, TB), TB, 0, s>>>(ntiles, ngroups, segid, &counts[3], tg_off);
-    // contraction
-    if (tcore) {
-      FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
-      const uint32_t hc = tc_half_cols(KP16);
-      k_m2l_tc<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                      h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
-                                                      h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
-                                                      tc_stages(tp), hc,
-                                                      4 * hc <= 512 ? 1 : 0, TC_FLUSH_EVERY, &ctr->tc_error,
-                                                      20000000L);
-      FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
-      h.g_used_tc = true;
-    } else {
-      k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                              h.g_ops.as<double>(), h.g_mt.as<double>(),
-                                                              h.c_xr.as<double4>(), h.L.as<double2>(), pd);
-    }
-    h.launches += 11;
     h.g_ntiles = ntiles;
-    h.g_ngroups = ngroups;
     h.g_nseg = nseg;  // an upper bound unless it was read
+    contract(h, tcore, tp, KP16, gp, pd);
+    h.launches += 10;
     FMM_LAUNCH();
   }
+  h.g_plan.valid = true;
+  h.g_plan.tcore = tcore;
+  h.g_plan.ordered = h.m2l_ordered;
+  h.g_plan.P = P;
+  h.g_plan.nres = nres;
   if (nres > 0) m2l_residual(h, ekey);
 }
 
