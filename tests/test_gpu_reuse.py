@@ -127,3 +127,25 @@ def test_reevaluate_and_set_charges_errors():
     f.reevaluate()
     assert np.array_equal(f.bodies(), stepped)
     f.close()
+
+
+def test_new_parameters_regroup():
+    """The kept grouping belongs to the lists, P and form it was made for:
+    after set_params the next evaluation regroups (and reevaluate needs new
+    lists first)."""
+    from minimal_b200 import FMM, FMMError, drand48_bodies
+
+    xq = drand48_bodies(50000, 9)
+    f = FMM(P=10, ncrit=64, theta=0.4, precision="mixed")
+    f.set_bodies(xq)
+    f.evaluate()
+    f.set_params(P=8, theta=0.5)
+    with pytest.raises(FMMError):
+        f.reevaluate()
+    f.evaluate()
+    got = f.bodies()
+    f.reevaluate()
+    again = f.bodies()
+    f.close()
+    assert np.array_equal(got, again)
+    assert np.array_equal(got, fresh(xq, xq[:, 3], P=8, ncrit=64, theta=0.5, precision="mixed"))
