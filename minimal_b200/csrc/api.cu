@@ -187,14 +187,17 @@ void run_all(Handle &h, bool rebuild) {
         for (int k = 0; k < 2; k++) cudaEventRecord(h.ev[p][k], h.stream);
   }
   if (h.prm.precision == EXAFMM_MIXED) make_srcf(h);  // read by P2M and the near field
+  // the mixed form's upward pass is shorter than the list build and yields
+  // to it; the FP64 one is longer and keeps the top priority
+  cudaStream_t up = h.prm.precision == EXAFMM_MIXED ? h.aux_lo : h.aux;
   FMM_CUDA(cudaEventRecord(h.fork_ev, h.stream));
   try {
-    FMM_CUDA(cudaStreamWaitEvent(h.aux, h.fork_ev, 0));
+    FMM_CUDA(cudaStreamWaitEvent(up, h.fork_ev, 0));
     {
-      Timer t(h, PH_UP, h.aux);
-      upward_pass(h, h.aux);
+      Timer t(h, PH_UP, up);
+      upward_pass(h, up);
     }
-    FMM_CUDA(cudaEventRecord(h.up_ev, h.aux));
+    FMM_CUDA(cudaEventRecord(h.up_ev, up));
     h.have_up = true;
     if (rebuild) do_lists(h);
     FMM_CUDA(cudaEventRecord(h.lists_ev, h.stream));
@@ -210,7 +213,7 @@ void run_all(Handle &h, bool rebuild) {
     periodic_pass(h);
   } catch (...) {
     // nothing of this evaluation stays in flight
-    cudaStreamSynchronize(h.aux);
+    cudaStreamSynchronize(up);
     cudaStreamSynchronize(h.side);
     throw;
   }
@@ -273,6 +276,7 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     FMM_CUDA(cudaStreamCreateWithPriority(&h.stream, cudaStreamNonBlocking, greatest));
     FMM_CUDA(cudaStreamCreateWithPriority(&h.side, cudaStreamNonBlocking, least));
     FMM_CUDA(cudaStreamCreateWithPriority(&h.aux, cudaStreamNonBlocking, greatest));
+    FMM_CUDA(cudaStreamCreateWithPriority(&h.aux_lo, cudaStreamNonBlocking, greatest < least ? greatest + 1 : greatest));
     for (cudaEvent_t *e : {&h.fork_ev, &h.up_ev, &h.lists_ev, &h.join_ev})
       FMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     FMM_CUDA(cudaMallocHost(&h.flags_host, 4 * sizeof(int)));
@@ -303,6 +307,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
   if (h.stream) cudaStreamSynchronize(h.stream);
   if (h.side) cudaStreamSynchronize(h.side);
   if (h.aux) cudaStreamSynchronize(h.aux);
+  if (h.aux_lo) cudaStreamSynchronize(h.aux_lo);
   Buf *bufs[] = {&h.in, &h.src, &h.out, &h.perm, &h.srcf, &h.keys[0], &h.keys[1], &h.vals[0], &h.vals[1],
                  &h.lfirst, &h.chain, &h.prebase, &h.scan_tmp, &h.hist, &h.c_begin, &h.c_count, &h.c_child,
                  &h.c_nchild, &h.c_parent, &h.c_level, &h.c_xr, &h.c_pre, &h.c_ref, &h.c_leaf_of_body,
@@ -317,6 +322,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
   if (h.stream) cudaStreamDestroy(h.stream);
   if (h.side) cudaStreamDestroy(h.side);
   if (h.aux) cudaStreamDestroy(h.aux);
+  if (h.aux_lo) cudaStreamDestroy(h.aux_lo);
   for (cudaEvent_t e : {h.fork_ev, h.up_ev, h.lists_ev, h.join_ev})
     if (e) cudaEventDestroy(e);
   if (h.flags_host) cudaFreeHost(h.flags_host);

@@ -94,8 +94,9 @@ struct Handle {
   // a whole evaluation runs the near field on `side` (lower priority), from
   // the lists until the downward pass, beside the far field on `stream`
   cudaStream_t side = nullptr;
-  // ... and the upward pass on `aux`, beside the dual-tree walk
-  cudaStream_t aux = nullptr;
+  // ... and the upward pass on `aux` (top priority) or `aux_lo` (one level
+  // below the list build), beside the dual-tree walk
+  cudaStream_t aux = nullptr, aux_lo = nullptr;
   cudaEvent_t fork_ev = nullptr, up_ev = nullptr, lists_ev = nullptr, join_ev = nullptr;
   int64_t launches = 0;
 
