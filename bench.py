@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--n", "--bodies", dest="n", type=int, default=1 << 20)  # --bodies under torchrun
     ap.add_argument("--P", type=int, default=10)
     ap.add_argument("--theta", type=float, default=0.4)
     ap.add_argument("--ncrit", type=int, default=64)
@@ -188,6 +188,21 @@ def run_reference(a, rank, world):
 
 
 # ---------------------------------------------------------------- our arm
+def max_over_ranks(x, device):
+    """Max of x over the ranks of the default process group (a replica
+    time: the job takes as long as its slowest replica); x itself without a
+    group.  `device` holds the reduction tensor: the rank's GPU under NCCL,
+    "cpu" under gloo."""
+    import torch
+    import torch.distributed as td
+
+    if not (td.is_available() and td.is_initialized()) or td.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
 def timed_steps(fmm, steps, flush, torch):
     """Per-phase device times (library CUDA events) of `steps` evaluations,
     each after an L2 flush; returns (phase lists, kernel launches)."""
@@ -393,13 +408,7 @@ def run_ours(a, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
 
     def barrier_max(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        import torch.distributed as td
-
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, dev)
 
     # each rank: its own system (seed = rank), the reference's generator
     xq = drand48_bodies(a.n, rank)
