@@ -1,0 +1,59 @@
+"""The C++ driver shim (include/exafmm_b200.hpp): the reference's own drivers,
+3d/fmm.cxx and test/test_fmm.h, compiled unchanged against it
+(tests/shim/Makefile, into oracle/_ref/shim).  Linked against an
+oracle-backed stand-in of the C entry points they run on the CPU and must
+print the reference's own results, which checks the shim's host logic (body
+permutation, cell wiring, accumulation of p and F, direct sums on a second
+handle); linked against the library they reach the GPU path."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from tests.conftest import ROOT
+
+OUT = os.path.join(ROOT, "oracle", "_ref", "shim")
+
+
+def binary(name):
+    path = os.path.join(OUT, name)
+    if not os.path.exists(path):
+        pytest.skip("shim checks not built (the reference sources were not found at build time)")
+    return path
+
+
+def errors(text):
+    """(p, F) from the 'Rel. L2 Error' lines 3d/fmm.cxx prints."""
+    p = re.search(r"Rel\. L2 Error \(p\)\s*:\s*([0-9.eE+-]+)", text)
+    f = re.search(r"Rel\. L2 Error \(F\)\s*:\s*([0-9.eE+-]+)", text)
+    assert p and f, text[-2000:]
+    return float(p.group(1)), float(f.group(1))
+
+
+def run(path):
+    return subprocess.run([path], capture_output=True, text=True, timeout=600, cwd=OUT)
+
+
+def test_fmm_cxx_through_the_shim_prints_the_reference_results():
+    ref, shim = run(binary("fmm_ref")), run(binary("fmm_cpu"))
+    assert ref.returncode == 0 and shim.returncode == 0, shim.stderr[-2000:]
+    assert errors(shim.stdout) == errors(ref.stdout)
+
+
+def test_test_fmm_through_the_shim_gives_the_known_answers():
+    import numpy as np
+
+    kat = {k: float(v) for k, v in np.load(os.path.join(ROOT, "tests", "golden", "kat.npz")).items()}
+    r = run(binary("test_fmm_cpu"))
+    assert r.returncode == 0, r.stderr[-2000:]
+    e10, e20 = map(float, re.search(r"test_fmm (\S+) (\S+)", r.stdout).groups())
+    assert e10 == pytest.approx(kat["fmm_p10"], rel=1e-8) and e20 == pytest.approx(kat["fmm_p20"], rel=1e-8)
+
+
+def test_drivers_linked_against_the_library_reach_it():
+    r = run(binary("fmm_gpu"))
+    if r.returncode != 0:  # no GPU here: the library's own error, thrown by the shim
+        assert "exafmm_b200: no CUDA device" in r.stderr, r.stderr[-2000:]
+    else:
+        errors(r.stdout)
