@@ -53,6 +53,11 @@ def test_arch_and_argument_checks_without_gpu():
     bad = minimal_b200.Params(10, 64, 0.4, 2, 0.0, 0, 0)  # images without a period
     assert lib.exafmm_b200_create(ctypes.byref(bad), ctypes.byref(h)) == -1
     assert lib.exafmm_b200_destroy(None) == -1
+    # every handle call refuses a null handle without touching the GPU
+    one = ctypes.c_double(0.0)
+    assert lib.exafmm_b200_set_charges(None, ctypes.byref(one), 0) == -1
+    assert lib.exafmm_b200_reevaluate(None) == -1
+    assert lib.exafmm_b200_evaluate(None) == -1
 
 
 def test_no_gpu_is_reported_not_faked():
