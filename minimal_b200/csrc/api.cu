@@ -6,6 +6,8 @@
 
 #include <algorithm>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "fmm.cuh"
 
 namespace fmm {
@@ -101,15 +103,22 @@ __global__ void k_direct_back(const double4 *pf, long n, double *rec) {
   r[4] = pf[i].x; r[5] = pf[i].y; r[6] = pf[i].z; r[7] = pf[i].w;
 }
 
+// A phase: CUDA events on its stream (the timings), and an NVTX range on
+// the host around its launches (named in a profiler's timeline; no cost
+// without one).
+const char *const kPhaseNames[PH_COUNT] = {"tree", "lists", "upward", "m2l", "p2p", "downward"};
+
 struct Timer {
   Handle &h;
   int ph;
   cudaStream_t s;
   Timer(Handle &h_, int p, cudaStream_t s_ = nullptr) : h(h_), ph(p), s(s_ ? s_ : h_.stream) {
+    nvtxRangePushA(kPhaseNames[ph]);
     if (h.ev_ok) cudaEventRecord(h.ev[ph][0], s);
   }
   ~Timer() {
     if (h.ev_ok) cudaEventRecord(h.ev[ph][1], s);
+    nvtxRangePop();
   }
 };
 
