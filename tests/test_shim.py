@@ -57,3 +57,14 @@ def test_drivers_linked_against_the_library_reach_it():
         assert "exafmm_b200: no CUDA device" in r.stderr, r.stderr[-2000:]
     else:
         errors(r.stdout)
+
+
+def test_shim_header_compiles_without_warnings(tmp_path):
+    src = tmp_path / "use.cpp"
+    src.write_text('#include "exafmm_b200.hpp"\n'
+                   "int main() { exafmm::P = 10; exafmm::initKernel(); return exafmm::NTERM == 55 ? 0 : 1; }\n")
+    exe = tmp_path / "use"
+    c = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I" + os.path.join(ROOT, "include"),
+                        str(src), "-o", str(exe)], capture_output=True, text=True)
+    assert c.returncode == 0, c.stderr
+    assert subprocess.run([str(exe)]).returncode == 0
