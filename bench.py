@@ -266,6 +266,43 @@ def form_leg(FMM, d_rec, n, P, a, precision, flush, torch, local_rank, steps=3, 
             "phases_ms": {k: statistics.mean(v) for k, v in phase.items()}}
 
 
+def plummer_leg(FMM, flush, torch, local_rank, n=1 << 22, orders=(6, 8, 10, 12), steps=3, warmup=2):
+    """Non-uniform bodies: 4,194,304 bodies of a Plummer sphere (scale radius
+    1, radii above 10 rejected, equal charges 1/N; positions and charges
+    rounded to FP32 values).  Per order P: the mixed form with its leaf size
+    autotuned, timed, and its error against FP64 direct summation on 1,000
+    sampled targets, beside the FP64 form's error with the same leaf size
+    (the same tree, so the same sampled bodies)."""
+    from minimal_b200 import plummer_bodies
+
+    xq = plummer_bodies(n, 7).astype(np.float32).astype(np.float64)
+    res = {"workload": f"{n} bodies, Plummer sphere (a=1, r<=10), charges 1/N, positions and charges FP32 "
+                       "values; theta=0.4; mixed form with ncrit autotuned; errors vs FP64 direct on 1000 "
+                       "targets"}
+    for P in orders:
+        f = FMM(P=P, ncrit=64, theta=0.4, precision="mixed", device=local_rank)
+        f.set_bodies(xq)
+        ncrit, _ = f.autotune(repeats=2)
+        ts = []
+        for s in range(warmup + steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            f.evaluate()
+            if s >= warmup:
+                ts.append(f.timings()["total"])
+        err = errors_vs_direct(f, n)
+        f.close()
+        g = FMM(P=P, ncrit=ncrit, theta=0.4, precision="fp64", device=local_rank)
+        g.set_bodies(xq)
+        g.evaluate()
+        err64 = errors_vs_direct(g, n)
+        g.close()
+        ms = statistics.mean(ts)
+        res[f"P{P}"] = {"ncrit": ncrit, "ms_per_eval": ms, "evals_per_s": 1e3 / ms, "error_vs_direct": err,
+                        "fp64_error_vs_direct": err64}
+    return res
+
+
 def reevaluate_leg(fmm, n, flush, torch, full_ms, steps=5, warmup=3):
     """Fixed positions, new charges every evaluation (an FMM matrix-vector
     product): set_charges keeps the tree and the lists, reevaluate runs the
@@ -524,6 +561,10 @@ def run_ours(a, rank, world, local_rank):
         extra["same_positions_new_charges"] = reevaluate_leg(fmm, a.n, flush, torch, ms_dev)
         extra["batched"] = batched_leg(FMM, torch, dev, local_rank)
         extra["periodic"] = periodic_leg(FMM, torch, dev, local_rank, a.n)
+        try:  # a side leg: its failure is reported, the headline line still prints
+            extra["plummer_4M"] = plummer_leg(FMM, flush, torch, local_rank)
+        except Exception as e:
+            extra["plummer_4M"] = {"error": f"{type(e).__name__}: {e}"}
 
     cpu = None
     if not a.no_cpu_baseline and world == 1:
