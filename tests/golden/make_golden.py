@@ -24,7 +24,7 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 # name: (variant, n, seed, P, ncrit, theta, images, body kind, cluster)
 CASES = {
     "3d_n2000_p10": ("3d", 2000, 0, 10, 64, 0.4, 0, "3d", False),
-    "3d_n10000_p10": ("3d", 10000, 0, 10, 64, 0.4, 0, "3d", False),  # configs[0] / test_fmm size
+    "3d_n10000_p10": ("3d", 10000, 0, 10, 64, 0.4, 0, "3d", False),  # the CPU reference case / test_fmm size
     "3d_n3000_p6_nc16_th05": ("3d", 3000, 7, 6, 16, 0.5, 0, "3d", False),
     "3d_clustered_n4000_p8": ("3d", 4000, 3, 8, 32, 0.4, 0, "3d", True),
     "3d_n1": ("3d", 1, 0, 10, 64, 0.4, 0, "3d", False),

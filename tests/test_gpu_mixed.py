@@ -1,7 +1,7 @@
 """Mixed-precision form on the GPU: FP32 P2P with compensated accumulation and
 tensor-core (tcgen05, split-FP16, FP32 accumulation) M2L.
 
-The form is judged as the spec states: its error against FP64 direct
+The form is held to its accuracy contract: its error against FP64 direct
 summation must stay within 1.1x of the FP64 form's error at the same P (force)
 -- and within 1.5x for the potential, which is dominated by the far field --
 while the tree and the lists stay bit-exact (they are shared with FP64).
