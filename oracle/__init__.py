@@ -9,6 +9,10 @@ ctypes:
 * ``Ref``  -- ``oracle/_ref/libref*.so``, the reference's own headers compiled
   unmodified by ``oracle/Makefile`` around ``oracle/ref/ref_driver.cpp``.
 
+and, for the reference's 2D code (`2d/`), ``Fmm2D("port")`` (the restatement in
+``oracle/fmm2d_oracle.c``) and ``Fmm2D("ref")`` (the reference's 2d headers
+around ``oracle/ref/ref2d_driver.cpp``).
+
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py``
 use this package, and only as the checker or the timed CPU baseline.  The
 product library (``minimal_b200``) never imports it.
@@ -241,3 +245,90 @@ class Ref(_Common):
 
     def test_fmm(self, P):
         return self.lib.ref_test_fmm(P)
+
+
+# ---------------------------------------------------------------- 2D
+REF2D_LIB = os.path.join(HERE, "_ref", "libref2d_lazy.so")
+
+
+class Fmm2D:
+    """One of the two 2D checkers (minimal ExaFMM `2d/`, lazy traversal):
+    ``Fmm2D("port")`` is the C restatement in oracle/fmm2d_oracle.c (in
+    liboracle.so), ``Fmm2D("ref")`` the reference's own 2d headers compiled by
+    oracle/Makefile.  Bodies are 6 doubles: X[2], q, p, F[2]."""
+
+    def __init__(self, which="port"):
+        path, self._pre = (PORT_LIB, "orc2_") if which == "port" else (REF2D_LIB, "ref2_")
+        if not os.path.exists(path):
+            build()
+        self.lib = L = ctypes.CDLL(path)
+        f = lambda name: getattr(L, self._pre + name)  # noqa: E731
+        f("tree").restype = _l
+        f("tree").argtypes = [_l, _p, _i]
+        f("fmm").restype = _l
+        f("fmm").argtypes = [_l, _p, _i, _i, _d]
+        f("get_bodies").argtypes = [_p]
+        f("get_cells").argtypes = [_p] * 5
+        f("count_lists").argtypes = [_p, _p]
+        f("get_lists").argtypes = [_p] * 4
+        f("get_expansions").argtypes = [_p, _p]
+        f("direct").argtypes = [_l, _p, _l, _p]
+        f("direct").restype = None
+        self.n = self.ncells = self.P = 0
+
+    def _f(self, name):
+        return getattr(self.lib, self._pre + name)
+
+    def tree(self, xyq, ncrit):
+        xyq = np.ascontiguousarray(xyq, dtype=np.float64)
+        self.n = len(xyq)
+        self.ncells = int(self._f("tree")(self.n, _ptr(xyq), ncrit))
+        return self.ncells
+
+    def fmm(self, xyq, P, ncrit, theta):
+        xyq = np.ascontiguousarray(xyq, dtype=np.float64)
+        self.n, self.P = len(xyq), P
+        self.ncells = int(self._f("fmm")(self.n, _ptr(xyq), P, ncrit, theta))
+        return self.ncells
+
+    def bodies(self):
+        out = np.zeros((self.n, 6))
+        self._f("get_bodies")(_ptr(out))
+        return out
+
+    def cells(self):
+        C = self.ncells
+        nchild, child, body, nbody = (np.zeros(C, np.int32) for _ in range(4))
+        xr = np.zeros((C, 3))
+        self._f("get_cells")(_ptr(nchild), _ptr(child), _ptr(body), _ptr(nbody), _ptr(xr))
+        return dict(nchild=nchild, child=child, body=body, nbody=nbody, xr=xr)
+
+    def lists(self):
+        a, b = np.zeros(1, np.int64), np.zeros(1, np.int64)
+        self._f("count_lists")(_ptr(a), _ptr(b))
+        na, nb = int(a[0]), int(b[0])
+        mo, po = np.zeros(self.ncells + 1, np.int32), np.zeros(self.ncells + 1, np.int32)
+        ms, ps = np.zeros(max(na, 1), np.int32), np.zeros(max(nb, 1), np.int32)
+        self._f("get_lists")(_ptr(mo), _ptr(ms), _ptr(po), _ptr(ps))
+        return dict(m2l_off=mo, m2l_src=ms[:na], p2p_off=po, p2p_src=ps[:nb])
+
+    def expansions(self):
+        M = np.zeros((self.ncells, self.P, 2))
+        L = np.zeros((self.ncells, self.P, 2))
+        self._f("get_expansions")(_ptr(M), _ptr(L))
+        return M[..., 0] + 1j * M[..., 1], L[..., 0] + 1j * L[..., 1]
+
+    def direct(self, targets6, sources6):
+        t = np.ascontiguousarray(targets6, dtype=np.float64).copy()
+        s = np.ascontiguousarray(sources6, dtype=np.float64)
+        self._f("direct")(len(t), _ptr(t), len(s), _ptr(s))
+        return t
+
+
+def reference_bodies_2d(n, seed=0):
+    """n x 3 (x, y, q) as the reference's 2d driver makes them (2d/fmm.cxx:21-35)."""
+    L = ctypes.CDLL(PORT_LIB)
+    L.orc2_reference_bodies.argtypes = [_l, _l, _p]
+    xyq = np.zeros((n, 3))
+    L.orc2_reference_bodies(n, seed, _ptr(xyq))
+    return xyq

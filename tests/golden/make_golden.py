@@ -6,7 +6,8 @@ expansions and potentials/forces as compressed .npz files.  The tests compare
 the oracle restatement and the GPU library against these files; the GPU box
 has no reference sources, only these fixtures.
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py       # 3D
+    make -C oracle && python tests/golden/make_golden.py 2d    # 2D
 """
 import os
 import sys
@@ -111,5 +112,45 @@ def main():
     print(kat)
 
 
+# 2D (minimal ExaFMM `2d/`): name -> (n, seed, P, ncrit, theta, clustered)
+CASES_2D = {
+    "2d_n2000_p10": (2000, 0, 10, 8, 0.4, False),       # the 2d driver's parameters, small N
+    "2d_n5000_p14_nc4_th03": (5000, 2, 14, 4, 0.3, False),
+    "2d_clustered_n3000_p8": (3000, 5, 8, 8, 0.4, True),
+    "2d_n1": (1, 0, 10, 8, 0.4, False),
+    "2d_n8_single_leaf": (8, 0, 10, 8, 0.4, False),     # N = ncrit
+    "2d_n9": (9, 0, 10, 8, 0.4, False),                 # N = ncrit + 1
+}
+
+
+def bodies_2d(n, seed, clustered):
+    """x, y, q: the 2d driver's generator, or three seeded Gaussian clusters."""
+    if not clustered:
+        return oracle.reference_bodies_2d(n, seed)
+    g = np.random.default_rng(seed)
+    xy = g.normal(0.0, 0.05, (n, 2)) + g.choice([-1.5, 0.3, 2.0], (n, 1))
+    q = g.uniform(-0.5, 0.5, n)
+    return np.c_[xy, q - q.mean()]
+
+
+def main_2d():
+    ref = oracle.Fmm2D("ref")
+    for name, (n, seed, P, ncrit, theta, clustered) in CASES_2D.items():
+        xyq = bodies_2d(n, seed, clustered)
+        ref.fmm(xyq, P, ncrit, theta)
+        out = ref.bodies()
+        cells = ref.cells()
+        lists = ref.lists()
+        M, L = ref.expansions()
+        # direct sum onto up to 20 stride-sampled bodies (tree order, p = F = 0)
+        tgt = out[:: max(1, n // 20)][:20].copy()
+        tgt[:, 3:] = 0
+        direct = ref.direct(tgt, out)
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), xyq=xyq, P=P, ncrit=ncrit, theta=theta, bodies=out,
+                            M=M, L=L, direct_targets=tgt, direct=direct, **cells, **lists)
+        print(name, "cells", ref.ncells, "m2l", len(lists["m2l_src"]), "p2p", len(lists["p2p_src"]))
+
+
 if __name__ == "__main__":
-    main()
+    # `make_golden.py 2d` writes the 2D fixtures only
+    main_2d() if sys.argv[1:] == ["2d"] else main()
