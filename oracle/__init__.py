@@ -249,16 +249,19 @@ class Ref(_Common):
 
 # ---------------------------------------------------------------- 2D
 REF2D_LIB = os.path.join(HERE, "_ref", "libref2d_lazy.so")
+REF2DP_LIB = os.path.join(HERE, "_ref", "libref2dp_lazy.so")
 
 
 class Fmm2D:
-    """One of the two 2D checkers (minimal ExaFMM `2d/`, lazy traversal):
+    """A 2D checker (minimal ExaFMM `2d/` and `2dp/`, lazy traversal):
     ``Fmm2D("port")`` is the C restatement in oracle/fmm2d_oracle.c (in
-    liboracle.so), ``Fmm2D("ref")`` the reference's own 2d headers compiled by
-    oracle/Makefile.  Bodies are 6 doubles: X[2], q, p, F[2]."""
+    liboracle.so, both variants), ``Fmm2D("ref")`` / ``Fmm2D("refp")`` the
+    reference's own 2d / 2dp headers compiled by oracle/Makefile.  Bodies are
+    6 doubles: X[2], q, p, F[2]."""
 
     def __init__(self, which="port"):
-        path, self._pre = (PORT_LIB, "orc2_") if which == "port" else (REF2D_LIB, "ref2_")
+        path, self._pre = {"port": (PORT_LIB, "orc2_"), "ref": (REF2D_LIB, "ref2_"),
+                           "refp": (REF2DP_LIB, "ref2_")}[which]
         if not os.path.exists(path):
             build()
         self.lib = L = ctypes.CDLL(path)
@@ -266,13 +269,13 @@ class Fmm2D:
         f("tree").restype = _l
         f("tree").argtypes = [_l, _p, _i]
         f("fmm").restype = _l
-        f("fmm").argtypes = [_l, _p, _i, _i, _d]
+        f("fmm").argtypes = [_l, _p, _i, _i, _d, _i, _d]
         f("get_bodies").argtypes = [_p]
         f("get_cells").argtypes = [_p] * 5
         f("count_lists").argtypes = [_p, _p]
-        f("get_lists").argtypes = [_p] * 4
+        f("get_lists").argtypes = [_p] * 6
         f("get_expansions").argtypes = [_p, _p]
-        f("direct").argtypes = [_l, _p, _l, _p]
+        f("direct").argtypes = [_l, _p, _l, _p, _i, _d]
         f("direct").restype = None
         self.n = self.ncells = self.P = 0
 
@@ -285,10 +288,11 @@ class Fmm2D:
         self.ncells = int(self._f("tree")(self.n, _ptr(xyq), ncrit))
         return self.ncells
 
-    def fmm(self, xyq, P, ncrit, theta):
+    def fmm(self, xyq, P, ncrit, theta, images=0, cycle=0.0):
         xyq = np.ascontiguousarray(xyq, dtype=np.float64)
         self.n, self.P = len(xyq), P
-        self.ncells = int(self._f("fmm")(self.n, _ptr(xyq), P, ncrit, theta))
+        self.ncells = int(self._f("fmm")(self.n, _ptr(xyq), P, ncrit, theta, images, cycle))
+        assert self.ncells > 0, "images > 0 needs the periodic build"
         return self.ncells
 
     def bodies(self):
@@ -308,9 +312,10 @@ class Fmm2D:
         self._f("count_lists")(_ptr(a), _ptr(b))
         na, nb = int(a[0]), int(b[0])
         mo, po = np.zeros(self.ncells + 1, np.int32), np.zeros(self.ncells + 1, np.int32)
-        ms, ps = np.zeros(max(na, 1), np.int32), np.zeros(max(nb, 1), np.int32)
-        self._f("get_lists")(_ptr(mo), _ptr(ms), _ptr(po), _ptr(ps))
-        return dict(m2l_off=mo, m2l_src=ms[:na], p2p_off=po, p2p_src=ps[:nb])
+        ms, mi = np.zeros(max(na, 1), np.int32), np.zeros(max(na, 1), np.int32)
+        ps, pi = np.zeros(max(nb, 1), np.int32), np.zeros(max(nb, 1), np.int32)
+        self._f("get_lists")(_ptr(mo), _ptr(ms), _ptr(mi), _ptr(po), _ptr(ps), _ptr(pi))
+        return dict(m2l_off=mo, m2l_src=ms[:na], m2l_img=mi[:na], p2p_off=po, p2p_src=ps[:nb], p2p_img=pi[:nb])
 
     def expansions(self):
         M = np.zeros((self.ncells, self.P, 2))
@@ -318,10 +323,10 @@ class Fmm2D:
         self._f("get_expansions")(_ptr(M), _ptr(L))
         return M[..., 0] + 1j * M[..., 1], L[..., 0] + 1j * L[..., 1]
 
-    def direct(self, targets6, sources6):
+    def direct(self, targets6, sources6, images=0, cycle=0.0):
         t = np.ascontiguousarray(targets6, dtype=np.float64).copy()
         s = np.ascontiguousarray(sources6, dtype=np.float64)
-        self._f("direct")(len(t), _ptr(t), len(s), _ptr(s))
+        self._f("direct")(len(t), _ptr(t), len(s), _ptr(s), images, cycle)
         return t
 
 

@@ -1,5 +1,6 @@
-/* Oracle, 2D: plain-C restatement of minimal ExaFMM's 2D Laplace FMM.  TEST
- * INFRASTRUCTURE ONLY (see fmm2d_oracle.h).  Each function cites the
+/* Oracle, 2D: plain-C restatement of minimal ExaFMM's 2D Laplace FMM, free
+ * space (`2d/`) and periodic (`2dp/`).  TEST INFRASTRUCTURE ONLY (see
+ * fmm2d_oracle.h).  Each function cites the
  * reference lines it restates.  Bit-identity with the reference needs the
  * same operations in the same order: complex products are written out as
  * (ac - bd, ad + bc), a complex times or over a real acts on each part, and
@@ -42,16 +43,17 @@ typedef struct {
 typedef struct {
   int nchild, nbody, child, body;  /* child: first child's index (-1: leaf); body: first body */
   double X[2], R;
-  int *m2l, nm2l, cm2l;            /* interaction lists, in recording order */
-  int *p2p, np2p, cp2p;
+  int *m2l, nm2l, cm2l;            /* interaction lists, in recording order: */
+  int *p2p, np2p, cp2p;            /* source cell, then its image index */
 } Cell2;
 
 static Body2 *g_b;
 static long g_n;
 static Cell2 *g_c;
 static long g_nc, g_cap;
-static int g_P, g_ncrit;
-static double g_theta;
+static int g_P, g_ncrit, g_images;
+static double g_theta, g_cycle;
+static int g_iX[2]; /* the image of the current source: a shift of iX * cycle */
 static cpx *g_M, *g_L; /* P per cell */
 
 static void free_cells(void) {
@@ -167,13 +169,14 @@ long orc2_tree(long n, const double *xyq, int ncrit) {
   return g_nc;
 }
 
-/* 2d/kernel.h:12-31 P2P */
+/* 2d/kernel.h:12-31 P2P; 2dp/kernel.h:12-35 with the source image shifted
+ * by iX * cycle (zero in free space: x - 0.0 is x) */
 static void p2p(Body2 *Bi, long ni, const Body2 *Bj, long nj) {
   for (long i = 0; i < ni; i++) {
     double p = 0, F[2] = {0, 0};
     for (long j = 0; j < nj; j++) {
       double dX[2];
-      for (int d = 0; d < 2; d++) dX[d] = Bi[i].X[d] - Bj[j].X[d];
+      for (int d = 0; d < 2; d++) dX[d] = Bi[i].X[d] - Bj[j].X[d] - g_iX[d] * g_cycle;
       const double R2 = dX[0] * dX[0] + dX[1] * dX[1];
       if (R2 != 0) {
         const double invR = 1 / sqrt(R2);
@@ -201,29 +204,29 @@ static void p2m(long c) {
   }
 }
 
-/* 2d/kernel.h:46-59 M2M */
-static void m2m(long ci) {
-  const Cell2 *Ci = &g_c[ci];
-  cpx *Mi = g_M + ci * g_P;
-  for (long cj = Ci->child; cj < Ci->child + Ci->nchild; cj++) {
-    const cpx Z = {g_c[cj].X[0] - Ci->X[0], g_c[cj].X[1] - Ci->X[1]};
-    const cpx *Mj = g_M + cj * g_P;
-    for (int k = 0; k < g_P; k++) {
-      cpx pw = {1.0, 0.0};
-      cacc(&Mi[k], Mj[k]);
-      for (int n = 1; n <= k; n++) {
-        pw = cmul(pw, cdivr(Z, (double)n));
-        cacc(&Mi[k], cmul(Mj[k - n], pw));
-      }
+/* 2d/kernel.h:46-59 M2M: one child's multipole Mj (centre Xj) into the
+ * parent's Mi (centre Xi) */
+static void m2m_one(const double *Xi, cpx *Mi, const double *Xj, const cpx *Mj) {
+  const cpx Z = {Xj[0] - Xi[0], Xj[1] - Xi[1]};
+  for (int k = 0; k < g_P; k++) {
+    cpx pw = {1.0, 0.0};
+    cacc(&Mi[k], Mj[k]);
+    for (int n = 1; n <= k; n++) {
+      pw = cmul(pw, cdivr(Z, (double)n));
+      cacc(&Mi[k], cmul(Mj[k - n], pw));
     }
   }
 }
 
-/* 2d/kernel.h:61-89 M2L */
-static void m2l(long ci, long cj) {
-  const cpx Z = {g_c[ci].X[0] - g_c[cj].X[0], g_c[ci].X[1] - g_c[cj].X[1]};
-  const cpx *M = g_M + cj * g_P;
-  cpx *L = g_L + ci * g_P;
+static void m2m(long ci) {
+  for (long cj = g_c[ci].child; cj < g_c[ci].child + g_c[ci].nchild; cj++)
+    m2m_one(g_c[ci].X, g_M + ci * g_P, g_c[cj].X, g_M + cj * g_P);
+}
+
+/* 2d/kernel.h:61-89 M2L (2dp/kernel.h:65-93: source shifted by iX * cycle),
+ * from the multipole M to the local expansion L */
+static void m2l_at(const double *Xi, const double *Xj, const cpx *M, cpx *L) {
+  const cpx Z = {Xi[0] - Xj[0] - g_iX[0] * g_cycle, Xi[1] - Xj[1] - g_iX[1] * g_cycle};
   const cpx one = {1.0, 0.0}, invZ = cdiv(one, Z);
   cpx pzn, pznk = one;
   cacc(&L[0], cmul(cneg(M[0]), clogc(Z)));
@@ -251,6 +254,8 @@ static void m2l(long ci, long cj) {
     pznk = cscale(pznk, (double)(n - 1));
   }
 }
+
+static void m2l(long ci, long cj) { m2l_at(g_c[ci].X, g_c[cj].X, g_M + cj * g_P, g_L + ci * g_P); }
 
 /* 2d/kernel.h:91-105 L2L */
 static void l2l(long cj) {
@@ -308,16 +313,21 @@ static void push(int **a, int *n, int *cap, int v) {
   (*a)[(*n)++] = v;
 }
 
-/* 2d/traverse_lazy.h:26-43 getList: the MAC, then the branch rules */
+/* 2d/traverse_lazy.h:26-43 getList: the MAC, then the branch rules
+ * (2dp/traverse_lazy.h:33-52: source image iX, recorded per entry as
+ * periodic1D = iX0 + 1 + 3 (iX1 + 1)) */
 static void get_list(long ci, long cj) {
   Cell2 *Ci = &g_c[ci];
   const Cell2 *Cj = &g_c[cj];
-  const double dX[2] = {Ci->X[0] - Cj->X[0], Ci->X[1] - Cj->X[1]};
+  const double dX[2] = {Ci->X[0] - Cj->X[0] - g_iX[0] * g_cycle, Ci->X[1] - Cj->X[1] - g_iX[1] * g_cycle};
   const double R2 = (dX[0] * dX[0] + dX[1] * dX[1]) * g_theta * g_theta;
+  const int img = g_iX[0] + 1 + 3 * (g_iX[1] + 1);
   if (R2 > (Ci->R + Cj->R) * (Ci->R + Cj->R)) {
     push(&Ci->m2l, &Ci->nm2l, &Ci->cm2l, (int)cj);
+    push(&Ci->m2l, &Ci->nm2l, &Ci->cm2l, img);
   } else if (Ci->nchild == 0 && Cj->nchild == 0) {
     push(&Ci->p2p, &Ci->np2p, &Ci->cp2p, (int)cj);
+    push(&Ci->p2p, &Ci->np2p, &Ci->cp2p, img);
   } else if (Cj->nchild == 0 || (Ci->R >= Cj->R && Ci->nchild != 0)) {
     for (long k = Ci->child; k < Ci->child + Ci->nchild; k++) get_list(k, cj);
   } else {
@@ -333,22 +343,77 @@ static void downward(long c) {
   for (long k = g_c[c].child; k < g_c[c].child + g_c[c].nchild; k++) downward(k);
 }
 
-long orc2_fmm(long n, const double *xyq, int P, int ncrit, double theta) {
+/* 2dp/traverse_lazy.h:79-122 periodic: the far images as a hierarchy of 3 x 3
+ * super-cells around the root.  Per image level: M2L into the root from the
+ * 72 cells of the level's ring (8 neighbours x 9 sub-cells), then the
+ * super-cell's multipole from its 8 neighbour copies (M2M), cycle x 3. */
+static void periodic(void) {
+  cpx *Mp = (cpx *)malloc(sizeof(cpx) * g_P), *Mc = (cpx *)malloc(sizeof(cpx) * 8 * g_P);
+  memcpy(Mp, g_M, sizeof(cpx) * g_P);
+  const double Xp[2] = {g_c[0].X[0], g_c[0].X[1]};
+  for (int level = 0; level < g_images - 1; level++) {
+    for (int ix = -1; ix <= 1; ix++)
+      for (int iy = -1; iy <= 1; iy++) {
+        if (ix == 0 && iy == 0) continue;
+        for (int cx = -1; cx <= 1; cx++)
+          for (int cy = -1; cy <= 1; cy++) {
+            g_iX[0] = ix * 3 + cx;
+            g_iX[1] = iy * 3 + cy;
+            m2l_at(g_c[0].X, Xp, Mp, g_L);
+          }
+      }
+    double Xc[8][2];
+    int c = 0;
+    for (int ix = -1; ix <= 1; ix++)
+      for (int iy = -1; iy <= 1; iy++) {
+        if (ix == 0 && iy == 0) continue;
+        Xc[c][0] = Xp[0] + ix * g_cycle;
+        Xc[c][1] = Xp[1] + iy * g_cycle;
+        memcpy(Mc + c * g_P, Mp, sizeof(cpx) * g_P);
+        c++;
+      }
+    for (c = 0; c < 8; c++) m2m_one(Xp, Mp, Xc[c], Mc + c * g_P);
+    g_cycle *= 3;
+  }
+  free(Mp);
+  free(Mc);
+}
+
+long orc2_fmm(long n, const double *xyq, int P, int ncrit, double theta, int images, double cycle) {
   orc2_tree(n, xyq, ncrit);
   g_P = P;
   g_theta = theta;
+  g_images = images;
+  g_cycle = cycle;
   g_M = (cpx *)calloc((size_t)g_nc * P, sizeof(cpx));
   g_L = (cpx *)calloc((size_t)g_nc * P, sizeof(cpx));
   upward(0);
-  get_list(0, 0);
-  /* 2d/traverse_lazy.h:45-56 evaluate: per target cell, its M2L then its P2P list */
+  /* 2dp/traverse_lazy.h:124-141 horizontalPass: one walk per image of the
+   * first shell (iX0 outer, iX1 inner), or the plain walk */
+  if (images == 0) {
+    g_iX[0] = g_iX[1] = 0;
+    get_list(0, 0);
+  } else {
+    for (g_iX[0] = -1; g_iX[0] <= 1; g_iX[0]++)
+      for (g_iX[1] = -1; g_iX[1] <= 1; g_iX[1]++) get_list(0, 0);
+  }
+  /* 2d/traverse_lazy.h:45-56 evaluate: per target cell, its M2L then its P2P
+   * list, each entry at its image (2dp/traverse_lazy.h:54-65) */
   for (long c = 0; c < g_nc; c++) {
-    for (int k = 0; k < g_c[c].nm2l; k++) m2l(c, g_c[c].m2l[k]);
-    for (int k = 0; k < g_c[c].np2p; k++) {
+    for (int k = 0; k < g_c[c].nm2l; k += 2) {
+      g_iX[0] = g_c[c].m2l[k + 1] % 3 - 1;
+      g_iX[1] = g_c[c].m2l[k + 1] / 3 - 1;
+      m2l(c, g_c[c].m2l[k]);
+    }
+    for (int k = 0; k < g_c[c].np2p; k += 2) {
       const Cell2 *S = &g_c[g_c[c].p2p[k]];
+      g_iX[0] = g_c[c].p2p[k + 1] % 3 - 1;
+      g_iX[1] = g_c[c].p2p[k + 1] / 3 - 1;
       p2p(g_b + g_c[c].body, g_c[c].nbody, g_b + S->body, S->nbody);
     }
   }
+  if (images > 0) periodic();
+  g_cycle = cycle;
   downward(0);
   return g_nc;
 }
@@ -380,18 +445,24 @@ void orc2_get_cells(int *nchild, int *child, int *body, int *nbody, double *xr) 
 void orc2_count_lists(long *nm2l, long *np2p) {
   *nm2l = *np2p = 0;
   for (long c = 0; c < g_nc; c++) {
-    *nm2l += g_c[c].nm2l;
-    *np2p += g_c[c].np2p;
+    *nm2l += g_c[c].nm2l / 2;
+    *np2p += g_c[c].np2p / 2;
   }
 }
 
-void orc2_get_lists(int *m2l_off, int *m2l_src, int *p2p_off, int *p2p_src) {
+void orc2_get_lists(int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img) {
   int a = 0, b = 0;
   for (long c = 0; c < g_nc; c++) {
     m2l_off[c] = a;
     p2p_off[c] = b;
-    for (int k = 0; k < g_c[c].nm2l; k++) m2l_src[a++] = g_c[c].m2l[k];
-    for (int k = 0; k < g_c[c].np2p; k++) p2p_src[b++] = g_c[c].p2p[k];
+    for (int k = 0; k < g_c[c].nm2l; k += 2, a++) {
+      m2l_src[a] = g_c[c].m2l[k];
+      m2l_img[a] = g_c[c].m2l[k + 1];
+    }
+    for (int k = 0; k < g_c[c].np2p; k += 2, b++) {
+      p2p_src[b] = g_c[c].p2p[k];
+      p2p_img[b] = g_c[c].p2p[k + 1];
+    }
   }
   m2l_off[g_nc] = a;
   p2p_off[g_nc] = b;
@@ -402,11 +473,23 @@ void orc2_get_expansions(double *M, double *L) {
   memcpy(L, g_L, sizeof(cpx) * g_nc * g_P);
 }
 
-void orc2_direct(long nt, double *t6, long ns, const double *s6) {
+/* 2d/traverse_lazy.h:84-94 direct; 2dp/traverse_lazy.h:154-175 over the
+ * (2 prange + 1)^2 images, prange = sum_{i < images} 3^i (ix outer) */
+void orc2_direct(long nt, double *t6, long ns, const double *s6, int images, double cycle) {
   Body2 *T = (Body2 *)malloc(sizeof(Body2) * nt), *S = (Body2 *)malloc(sizeof(Body2) * ns);
   memcpy(T, t6, sizeof(Body2) * nt);
   memcpy(S, s6, sizeof(Body2) * ns);
-  p2p(T, nt, S, ns);
+  int prange = 0;
+  for (int i = 0, p3 = 1; i < images; i++, p3 *= 3) prange += p3;
+  const double save = g_cycle;
+  g_cycle = cycle;
+  for (int ix = -prange; ix <= prange; ix++)
+    for (int iy = -prange; iy <= prange; iy++) {
+      g_iX[0] = ix;
+      g_iX[1] = iy;
+      p2p(T, nt, S, ns);
+    }
+  g_cycle = save;
   memcpy(t6, T, sizeof(Body2) * nt);
   free(T);
   free(S);

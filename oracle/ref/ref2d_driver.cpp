@@ -1,9 +1,13 @@
-// Test infrastructure only: a C-ABI wrapper around the reference's OWN 2d
-// headers (minimal ExaFMM `2d/`, lazy traversal), compiled from where they
-// lie by oracle/Makefile into oracle/_ref/libref2d_lazy.so.  Nothing here
-// restates the algorithm: it calls the reference's buildTree / upwardPass /
+// Test infrastructure only: a C-ABI wrapper around the reference's OWN 2d or
+// 2dp headers (minimal ExaFMM `2d/` / `2dp/` with REF_PERIODIC, lazy
+// traversal), compiled from where they lie by oracle/Makefile into
+// oracle/_ref/libref2d_lazy.so and libref2dp_lazy.so.  Nothing here restates
+// the algorithm: it calls the reference's buildTree / upwardPass /
 // horizontalPass / downwardPass / direct and copies the results out for the
 // 2D oracle's parity tests and fixtures.  The product library never links it.
+#ifndef REF_PERIODIC
+#define REF_PERIODIC 0
+#endif
 #include <cstring>
 #include <omp.h>
 
@@ -49,9 +53,16 @@ long ref2_tree(long n, const double *xyq, int nc) {
   return (long)g_cells.size();
 }
 
-long ref2_fmm(long n, const double *xyq, int p, int nc, double th) {
+long ref2_fmm(long n, const double *xyq, int p, int nc, double th, int img, double cyc) {
   P = p;
   theta = th;
+#if REF_PERIODIC
+  images = img;
+  cycle = cyc;
+#else
+  if (img != 0) return -1;  // free-space build
+  (void)cyc;
+#endif
   ref2_tree(n, xyq, nc);
   upwardPass(g_cells);
   horizontalPass(g_cells, g_cells);
@@ -84,13 +95,28 @@ void ref2_count_lists(long *nm2l, long *np2p) {
   }
 }
 
-void ref2_get_lists(int *m2l_off, int *m2l_src, int *p2p_off, int *p2p_src) {
+void ref2_get_lists(int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img) {
   int a = 0, b = 0;
   for (size_t c = 0; c < g_cells.size(); c++) {
+    const Cell &C = g_cells[c];
     m2l_off[c] = a;
     p2p_off[c] = b;
-    for (Cell *s : g_cells[c].listM2L) m2l_src[a++] = (int)(s - &g_cells[0]);
-    for (Cell *s : g_cells[c].listP2P) p2p_src[b++] = (int)(s - &g_cells[0]);
+    for (size_t k = 0; k < C.listM2L.size(); k++, a++) {
+      m2l_src[a] = (int)(C.listM2L[k] - &g_cells[0]);
+#if REF_PERIODIC
+      m2l_img[a] = C.periodicM2L[k];
+#else
+      m2l_img[a] = 4;  // the central image
+#endif
+    }
+    for (size_t k = 0; k < C.listP2P.size(); k++, b++) {
+      p2p_src[b] = (int)(C.listP2P[k] - &g_cells[0]);
+#if REF_PERIODIC
+      p2p_img[b] = C.periodicP2P[k];
+#else
+      p2p_img[b] = 4;
+#endif
+    }
   }
   m2l_off[g_cells.size()] = a;
   p2p_off[g_cells.size()] = b;
@@ -103,7 +129,18 @@ void ref2_get_expansions(double *M, double *L) {
   }
 }
 
-void ref2_direct(long nt, double *t6, long ns, const double *s6) {
+// one thread: the periodic direct sum adds the images in parallel otherwise,
+// and its summation order (ix outer, iy inner) is only fixed on one thread
+void ref2_direct(long nt, double *t6, long ns, const double *s6, int img, double cyc) {
+#if REF_PERIODIC
+  images = img;
+  cycle = cyc;
+#else
+  (void)img;
+  (void)cyc;
+#endif
+  const int threads = omp_get_max_threads();
+  omp_set_num_threads(1);
   Bodies t(nt), s(ns);
   for (long i = 0; i < nt; i++) {
     t[i].X[0] = t6[6 * i];
@@ -120,6 +157,7 @@ void ref2_direct(long nt, double *t6, long ns, const double *s6) {
     s[j].p = s[j].F[0] = s[j].F[1] = 0;
   }
   direct(t, s);
+  omp_set_num_threads(threads);
   for (long i = 0; i < nt; i++) to6(t[i], t6 + 6 * i);
 }
 }

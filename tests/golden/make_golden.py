@@ -112,15 +112,19 @@ def main():
     print(kat)
 
 
-# 2D (minimal ExaFMM `2d/`): name -> (n, seed, P, ncrit, theta, clustered)
+# 2D (minimal ExaFMM `2d/`, and `2dp/` with images > 0):
+# name -> (n, seed, P, ncrit, theta, clustered, images)
 CASES_2D = {
-    "2d_n2000_p10": (2000, 0, 10, 8, 0.4, False),       # the 2d driver's parameters, small N
-    "2d_n5000_p14_nc4_th03": (5000, 2, 14, 4, 0.3, False),
-    "2d_clustered_n3000_p8": (3000, 5, 8, 8, 0.4, True),
-    "2d_n1": (1, 0, 10, 8, 0.4, False),
-    "2d_n8_single_leaf": (8, 0, 10, 8, 0.4, False),     # N = ncrit
-    "2d_n9": (9, 0, 10, 8, 0.4, False),                 # N = ncrit + 1
+    "2d_n2000_p10": (2000, 0, 10, 8, 0.4, False, 0),       # the 2d driver's parameters, small N
+    "2d_n5000_p14_nc4_th03": (5000, 2, 14, 4, 0.3, False, 0),
+    "2d_clustered_n3000_p8": (3000, 5, 8, 8, 0.4, True, 0),
+    "2d_n1": (1, 0, 10, 8, 0.4, False, 0),
+    "2d_n8_single_leaf": (8, 0, 10, 8, 0.4, False, 0),     # N = ncrit
+    "2d_n9": (9, 0, 10, 8, 0.4, False, 0),                 # N = ncrit + 1
+    "2dp_n2000_p10_img3": (2000, 0, 10, 8, 0.4, False, 3),  # the 2dp driver's parameters, small N
+    "2dp_n1500_p8_img2": (1500, 6, 8, 16, 0.5, False, 2),
 }
+CYCLE_2D = 2 * np.pi
 
 
 def bodies_2d(n, seed, clustered):
@@ -134,10 +138,11 @@ def bodies_2d(n, seed, clustered):
 
 
 def main_2d():
-    ref = oracle.Fmm2D("ref")
-    for name, (n, seed, P, ncrit, theta, clustered) in CASES_2D.items():
+    for name, (n, seed, P, ncrit, theta, clustered, images) in CASES_2D.items():
+        ref = oracle.Fmm2D("refp" if images else "ref")
+        cycle = CYCLE_2D if images else 0.0
         xyq = bodies_2d(n, seed, clustered)
-        ref.fmm(xyq, P, ncrit, theta)
+        ref.fmm(xyq, P, ncrit, theta, images, cycle)
         out = ref.bodies()
         cells = ref.cells()
         lists = ref.lists()
@@ -145,9 +150,9 @@ def main_2d():
         # direct sum onto up to 20 stride-sampled bodies (tree order, p = F = 0)
         tgt = out[:: max(1, n // 20)][:20].copy()
         tgt[:, 3:] = 0
-        direct = ref.direct(tgt, out)
-        np.savez_compressed(os.path.join(OUT, name + ".npz"), xyq=xyq, P=P, ncrit=ncrit, theta=theta, bodies=out,
-                            M=M, L=L, direct_targets=tgt, direct=direct, **cells, **lists)
+        direct = ref.direct(tgt, out, images, cycle)
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), xyq=xyq, P=P, ncrit=ncrit, theta=theta, images=images,
+                            cycle=cycle, bodies=out, M=M, L=L, direct_targets=tgt, direct=direct, **cells, **lists)
         print(name, "cells", ref.ncells, "m2l", len(lists["m2l_src"]), "p2p", len(lists["p2p_src"]))
 
 

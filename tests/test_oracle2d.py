@@ -1,9 +1,10 @@
 """The 2D oracle (oracle/fmm2d_oracle.c, a plain-C restatement of minimal
-ExaFMM's `2d/`) pinned against the reference: bit-identical quadtree, lists,
-expansions, potentials and forces on the committed fixtures (made from the
-reference's own 2d headers by tests/golden/make_golden.py) and on fresh
-cases against the compiled reference, and the reference 2d driver's printed
-errors reproduced."""
+ExaFMM's `2d/` and `2dp/`) pinned against the reference: bit-identical
+quadtree, lists (with periodic image indices), expansions, potentials,
+forces and direct sums on the committed fixtures (made from the reference's
+own 2d / 2dp headers by tests/golden/make_golden.py) and on fresh cases
+against the compiled reference, and the reference 2d driver's printed errors
+reproduced."""
 import ctypes
 import math
 import os
@@ -15,7 +16,7 @@ import pytest
 
 from tests.conftest import GOLDEN, ROOT, golden
 
-NAMES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.startswith("2d_") and f.endswith(".npz"))
+NAMES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.startswith(("2d_", "2dp_")) and f.endswith(".npz"))
 
 
 @pytest.fixture(scope="module")
@@ -34,26 +35,29 @@ def ref_available():
 @pytest.mark.parametrize("name", NAMES)
 def test_port_matches_reference_fixture_2d(port2, name):
     g = golden(name)
-    port2.fmm(g["xyq"], int(g["P"]), int(g["ncrit"]), float(g["theta"]))
+    images, cycle = int(g["images"]), float(g["cycle"])
+    port2.fmm(g["xyq"], int(g["P"]), int(g["ncrit"]), float(g["theta"]), images, cycle)
     cells, lists = port2.cells(), port2.lists()
     for k in ("nchild", "child", "body", "nbody", "xr"):
         assert np.array_equal(cells[k], g[k]), k
-    for k in ("m2l_off", "m2l_src", "p2p_off", "p2p_src"):
+    for k in ("m2l_off", "m2l_src", "m2l_img", "p2p_off", "p2p_src", "p2p_img"):
         assert np.array_equal(lists[k], g[k]), k
     M, L = port2.expansions()
     assert np.array_equal(M, g["M"]) and np.array_equal(L, g["L"])
     assert np.array_equal(port2.bodies(), g["bodies"])
-    assert np.array_equal(port2.direct(g["direct_targets"], g["bodies"]), g["direct"])
+    assert np.array_equal(port2.direct(g["direct_targets"], g["bodies"], images, cycle), g["direct"])
 
 
 # every case keeps the cell count at most N: the reference reserves N cells
 # (2d/build_tree.h:93) and its child pointers are only valid within that
-@pytest.mark.parametrize("n,P,ncrit,theta,seed,clustered", [
-    (4000, 4, 4, 0.5, 11, False),
-    (7000, 20, 16, 0.35, 12, False),
-    (5000, 12, 6, 0.45, 13, True),
+@pytest.mark.parametrize("n,P,ncrit,theta,seed,clustered,images", [
+    (4000, 4, 4, 0.5, 11, False, 0),
+    (7000, 20, 16, 0.35, 12, False, 0),
+    (5000, 12, 6, 0.45, 13, True, 0),
+    (3000, 10, 8, 0.4, 14, False, 4),
+    (2500, 16, 12, 0.3, 15, True, 2),
 ])
-def test_port_matches_compiled_reference_2d(port2, n, P, ncrit, theta, seed, clustered):
+def test_port_matches_compiled_reference_2d(port2, n, P, ncrit, theta, seed, clustered, images):
     if not ref_available():
         pytest.skip("the reference's 2d headers are not built here (oracle/_ref)")
     import oracle
@@ -61,9 +65,10 @@ def test_port_matches_compiled_reference_2d(port2, n, P, ncrit, theta, seed, clu
     from tests.golden.make_golden import bodies_2d
 
     xyq = bodies_2d(n, seed, clustered)
-    ref = oracle.Fmm2D("ref")
-    ref.fmm(xyq, P, ncrit, theta)
-    port2.fmm(xyq, P, ncrit, theta)
+    cycle = 2 * np.pi if images else 0.0
+    ref = oracle.Fmm2D("refp" if images else "ref")
+    ref.fmm(xyq, P, ncrit, theta, images, cycle)
+    port2.fmm(xyq, P, ncrit, theta, images, cycle)
     assert port2.ncells == ref.ncells
     for a, b in ((port2.cells(), ref.cells()), (port2.lists(), ref.lists())):
         for k in a:
