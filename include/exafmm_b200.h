@@ -82,7 +82,7 @@ EXAFMM_API int exafmm_b200_set_bodies(exafmm_b200 *h, const double *bodies8, int
 
 /* Phases of one evaluation, replacing the reference's buildTree
  * (3d/build_tree.h:88-96), the list recording of the lazy traversal
- * (3d/traverse_lazy.h:27-44 getList; 3dp/traverse_lazy.h:276-293 image loop),
+ * (3d/traverse_lazy.h:27-44 getList; 3dp/traverse_lazy.h:124-141 image loop),
  * upwardPass (3d/traverse_eager.h:127-144), horizontalPass
  * (3d/traverse_eager.h:147-172 M2L + P2P; 3dp/traverse_eager.h:95-110 with the
  * periodic root, :46-93) and downwardPass (3d/traverse_eager.h:175-190). */
@@ -116,7 +116,7 @@ EXAFMM_API int exafmm_b200_reevaluate(exafmm_b200 *h);
 EXAFMM_API int exafmm_b200_get_bodies(exafmm_b200 *h, double *bodies8, int where);
 EXAFMM_API int exafmm_b200_get_perm(exafmm_b200 *h, int64_t *perm, int where);
 
-/* Tree in the reference's cell order (3d/build_tree.h:117-131): per cell
+/* Tree in the reference's cell order (3d/build_tree.h:69-84): per cell
  * NCHILD, index of the first child (-1 for a leaf), index of the first body
  * in tree order, NBODY, level, and centre+radius as 4 doubles.  Host arrays
  * of exafmm_b200_num_cells() entries. */
@@ -192,10 +192,32 @@ EXAFMM_API int64_t exafmm_b200_last_launches(exafmm_b200 *h);
 EXAFMM_API int exafmm_b200_arch(void);
 
 /* Diagnostic with no reference counterpart: FMA-pipe throughput of the
- * handle's device in TFLOP/s (precision EXAFMM_FP64 or EXAFMM_MIXED = FP32),
- * measured with a dependent-chain FMA kernel; the denominator of the FP64 and
- * FP32 rooflines. */
+ * handle's device in TFLOP/s, measured with independent FMA chains; the
+ * denominator of the FP64 and FP32 rooflines.  precision EXAFMM_FP64: scalar
+ * FP64 FMAs; EXAFMM_MIXED: FP32, the larger of scalar FMAs and packed FP32x2
+ * FMAs (fma.rn.f32x2, two lanes per instruction); 2: scalar FP32 only; 3:
+ * packed FP32x2 only. */
 EXAFMM_API int exafmm_b200_fma_peak(exafmm_b200 *h, int precision, double *tflops);
+
+/* Tile shapes chosen at run time (no reference counterpart; the reference has
+ * no kernels to tile).  EXAFMM_TILE_M2L_FLUSH: groups of the tensor-core M2L
+ * (mixed form) accumulated in FP32 in tensor memory before the partial sum is
+ * folded into the compensated running sum: fewer groups per window means
+ * fewer FP32 additions between folds (a smaller accumulation error) and more
+ * fold work.  Values 1-64; 0 restores the default.  get_tile returns the value
+ * in effect.  exafmm_b200_autotune() chooses among candidates of it. */
+enum { EXAFMM_TILE_M2L_FLUSH = 0 };
+EXAFMM_API int exafmm_b200_set_tile(exafmm_b200 *h, int which, int value);
+EXAFMM_API int exafmm_b200_get_tile(exafmm_b200 *h, int which, int *value);
+
+/* Test hook with no reference counterpart: the next launch of the
+ * tensor-core M2L kernel on this handle (mixed form) first waits `ns`
+ * nanoseconds on a barrier that nothing arrives at, as if its inputs never
+ * came.  The wait runs out, the kernel's other roles stop waiting, copies and
+ * MMAs in flight are drained, tensor memory is freed, and the evaluation
+ * returns EXAFMM_ERR_TIMEOUT with its results discarded; the handle stays
+ * usable and the next evaluation runs normally.  ns = 0 clears the hook. */
+EXAFMM_API int exafmm_b200_test_stall_tc(exafmm_b200 *h, int64_t ns);
 
 /* Direct summation that allocates nothing.  No counterpart in the reference:
  * it exists for callers that may not allocate device memory -- programs that

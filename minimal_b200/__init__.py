@@ -38,7 +38,8 @@ API = [
     "exafmm_b200_get_lists", "exafmm_b200_get_expansions", "exafmm_b200_direct", "exafmm_b200_get_timings",
     "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak", "exafmm_b200_direct_static",
     "exafmm_b200_dipole_correction", "exafmm_b200_ewald", "exafmm_b200_set_batch", "exafmm_b200_autotune",
-    "exafmm_b200_set_charges", "exafmm_b200_reevaluate",
+    "exafmm_b200_set_charges", "exafmm_b200_reevaluate", "exafmm_b200_test_stall_tc",
+    "exafmm_b200_set_tile", "exafmm_b200_get_tile",
 ]
 
 PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
@@ -99,6 +100,9 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_autotune": (i, [vp, vp, i, i, vp, vp]),
         "exafmm_b200_set_charges": (i, [vp, vp, i]),
         "exafmm_b200_reevaluate": (i, [vp]),
+        "exafmm_b200_test_stall_tc": (i, [vp, i64]),
+        "exafmm_b200_set_tile": (i, [vp, i, i]),
+        "exafmm_b200_get_tile": (i, [vp, i, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -311,9 +315,23 @@ class FMM:
     def last_launches(self):
         return int(self.lib.exafmm_b200_last_launches(self.h))
 
+    TILES = {"m2l_flush": 0}
+
+    def set_tile(self, name, value):
+        """A run-time tile shape (include/exafmm_b200.h, EXAFMM_TILE_*); 0 = default."""
+        self._check(self.lib.exafmm_b200_set_tile(self.h, self.TILES[name], int(value)))
+
+    def get_tile(self, name):
+        v = np.zeros(1, dtype=np.int32)
+        self._check(self.lib.exafmm_b200_get_tile(self.h, self.TILES[name], _p(v)))
+        return int(v[0])
+
     def fma_peak(self, precision="fp64"):
+        """TFLOP/s of FMA chains: "fp64"; "fp32" (the larger of scalar and
+        packed FP32x2); "fp32_scalar"; "fp32x2"."""
+        kind = {"fp64": 0, "fp32": 1, "mixed": 1, "fp32_scalar": 2, "fp32x2": 3}[precision]
         t = np.zeros(1)
-        self._check(self.lib.exafmm_b200_fma_peak(self.h, FP64 if precision == "fp64" else MIXED, _p(t)))
+        self._check(self.lib.exafmm_b200_fma_peak(self.h, kind, _p(t)))
         return float(t[0])
 
 

@@ -12,6 +12,7 @@
 
 namespace fmm {
 double fma_peak_tflops(int precision);
+int m2l_flush_interval(const Handle &h);
 void m2l_set_attributes();
 void m2l_grouped_set_attributes();
 void p2p_set_attributes();
@@ -680,8 +681,32 @@ int64_t exafmm_b200_last_launches(exafmm_b200 *H) { return H ? H->h.launches : -
 int exafmm_b200_fma_peak(exafmm_b200 *H, int precision, double *tflops) {
   return guarded(H, [&](Handle &h) {
     if (!tflops) throw Error{EXAFMM_ERR_ARG, "null output"};
+    if (precision < 0 || precision > 3) throw Error{EXAFMM_ERR_ARG, "fma_peak: kind in [0, 3]"};
     FMM_CUDA(cudaSetDevice(h.prm.device));
     *tflops = fma_peak_tflops(precision);
+  });
+}
+
+int exafmm_b200_set_tile(exafmm_b200 *H, int which, int value) {
+  return guarded(H, [&](Handle &h) {
+    if (which != EXAFMM_TILE_M2L_FLUSH) throw Error{EXAFMM_ERR_ARG, "set_tile: unknown tile parameter"};
+    if (value < 0 || value > 64) throw Error{EXAFMM_ERR_ARG, "set_tile: M2L flush interval in [1, 64] (0: default)"};
+    h.tile_m2l_flush = value;
+  });
+}
+
+int exafmm_b200_get_tile(exafmm_b200 *H, int which, int *value) {
+  return guarded(H, [&](Handle &h) {
+    if (!value) throw Error{EXAFMM_ERR_ARG, "null output"};
+    if (which != EXAFMM_TILE_M2L_FLUSH) throw Error{EXAFMM_ERR_ARG, "get_tile: unknown tile parameter"};
+    *value = m2l_flush_interval(h);
+  });
+}
+
+int exafmm_b200_test_stall_tc(exafmm_b200 *H, int64_t ns) {
+  return guarded(H, [&](Handle &h) {
+    if (ns < 0 || ns > 1000000000LL) throw Error{EXAFMM_ERR_ARG, "test_stall_tc: ns in [0, 1e9]"};
+    h.tc_stall_ns = (long)ns;
   });
 }
 

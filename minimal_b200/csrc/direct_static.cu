@@ -15,12 +15,17 @@
 //    every GPU that loads the library until the process exits);
 //  - every call uses the same scratch array, and a call leaves its contents
 //    behind; each call re-initialises the part it uses before reading it;
-//  - calls run asynchronously on the caller's stream; two calls that overlap
-//    on the GPU (different streams, or different host threads) race on the
-//    scratch and must be serialised by the caller;
+//  - calls run asynchronously on the caller's stream, which must belong to
+//    the current device (a stream of another device is rejected); two calls
+//    that overlap on the GPU (different streams, or different host threads)
+//    race on the scratch and must be serialised by the caller;
 //  - the first call on each device looks up the device address of the
 //    scratch array (cudaGetSymbolAddress); make that first call before any
-//    stream capture.
+//    stream capture.  The address is kept for the life of the process: after
+//    cudaDeviceReset() on a device, this entry point must not be called on
+//    that device again;
+//  - any number of sources (the source chunks are looped over in the kernel).
+#include <algorithm>
 #include <mutex>
 
 #include "fmm.cuh"
@@ -46,31 +51,35 @@ __global__ void k_ds_pack(const double *targets8, long nt, double4 *xq, double4 
   pf[i] = make_double4(r[4], r[5], r[6], r[7]);  // accumulate onto the caller's p, F
 }
 
+// Block (x, y) sums source chunks y, y + gridDim.y, ... of DCHUNK sources
+// onto its DT targets.
 __global__ void __launch_bounds__(DT) k_ds_sum(const double4 *xq, long nt, const double *src8, long ns,
                                                double4 *pf) {
   __shared__ double4 tile[DT];
   const long i = (long)blockIdx.x * DT + threadIdx.x;
-  const long s0 = (long)blockIdx.y * DCHUNK, s1 = min(ns, s0 + DCHUNK);
   const double4 T = i < nt ? xq[i] : make_double4(0, 0, 0, 0);
   double p = 0, ax = 0, ay = 0, az = 0;
-  for (long b = s0; b < s1; b += DT) {
-    __syncthreads();
-    if (b + threadIdx.x < s1) {
-      const double *r = src8 + 8 * (b + threadIdx.x);
-      tile[threadIdx.x] = make_double4(r[0], r[1], r[2], r[3]);
-    }
-    __syncthreads();
-    const int m = (int)min((long)DT, s1 - b);
-    for (int k = 0; k < m; k++) {
-      const double4 s = tile[k];
-      const double dx = T.x - s.x, dy = T.y - s.y, dz = T.z - s.z;
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      const double ir = r2 > 0 ? rsqrt(r2) : 0.0;  // zero distance skipped (3d/kernel.h:135)
-      const double qir = s.w * ir, qir3 = qir * ir * ir;
-      p += qir;
-      ax += dx * qir3;
-      ay += dy * qir3;
-      az += dz * qir3;
+  for (long s0 = (long)blockIdx.y * DCHUNK; s0 < ns; s0 += (long)gridDim.y * DCHUNK) {
+    const long s1 = min(ns, s0 + DCHUNK);
+    for (long b = s0; b < s1; b += DT) {
+      __syncthreads();
+      if (b + threadIdx.x < s1) {
+        const double *r = src8 + 8 * (b + threadIdx.x);
+        tile[threadIdx.x] = make_double4(r[0], r[1], r[2], r[3]);
+      }
+      __syncthreads();
+      const int m = (int)min((long)DT, s1 - b);
+      for (int k = 0; k < m; k++) {
+        const double4 s = tile[k];
+        const double dx = T.x - s.x, dy = T.y - s.y, dz = T.z - s.z;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double ir = r2 > 0 ? rsqrt(r2) : 0.0;  // zero distance skipped (3d/kernel.h:135)
+        const double qir = s.w * ir, qir3 = qir * ir * ir;
+        p += qir;
+        ax += dx * qir3;
+        ay += dy * qir3;
+        az += dz * qir3;
+      }
     }
   }
   if (i < nt) {
@@ -130,9 +139,18 @@ extern "C" int exafmm_b200_direct_static(const double *sources8, int64_t ns, dou
   }
   double4 *xq = (double4 *)base, *pf = xq + MAXT;
   cudaStream_t s = (cudaStream_t)stream;
+  if (s) {  // the scratch address is this device's: the stream must be too
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess || sdev != dev) {
+      cudaGetLastError();
+      exafmm_b200_static_err = "direct_static: the stream does not belong to the current device";
+      return EXAFMM_ERR_ARG;
+    }
+  }
   const unsigned gt = (unsigned)((nt + DT - 1) / DT);
   k_ds_pack<<<gt, DT, 0, s>>>(targets8, nt, xq, pf);
-  dim3 grid(gt, (unsigned)((ns + DCHUNK - 1) / DCHUNK));
+  const long nchunk = (ns + DCHUNK - 1) / DCHUNK;
+  dim3 grid(gt, (unsigned)std::min<long>(nchunk, 1024));
   k_ds_sum<<<grid, DT, 0, s>>>(xq, nt, sources8, ns, pf);
   k_ds_unpack<<<gt, DT, 0, s>>>(pf, nt, targets8);
   cudaError_t e = cudaGetLastError();
@@ -140,5 +158,6 @@ extern "C" int exafmm_b200_direct_static(const double *sources8, int64_t ns, dou
     exafmm_b200_static_err = std::string("direct_static: launch failed: ") + cudaGetErrorString(e);
     return EXAFMM_ERR_CUDA;
   }
+  exafmm_b200_static_err.clear();  // as the handle calls do on success
   return EXAFMM_OK;
 }

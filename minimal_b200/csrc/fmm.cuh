@@ -81,6 +81,9 @@ struct DevCounters {
   int gcounts[4];      // grouped M2L: residual entries, flagged targets, groups, segments
   unsigned long long gfill;
   int tc_error;        // a bounded tensor-core wait ran out
+  // largest |scaled multipole| over the possible M2L sources, as the bits of
+  // a non-negative double (the FP16 split's power-of-two normalisation)
+  unsigned long long m16_max;
 };
 
 // Per-phase timing slots (CUDA events on the handle stream).
@@ -166,6 +169,11 @@ struct Handle {
     int P = 0, nres = 0;
   } g_plan;
   bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only
+  // tile shapes chosen at run time (exafmm_b200_set_tile; the autotuner)
+  int tile_m2l_flush = 0;  // tensor-core M2L groups per FP32 accumulator window (0: default)
+  // test hook (exafmm_b200_test_stall_tc): the next tensor-core M2L launch
+  // waits this long on a barrier nothing arrives at, then times out
+  long tc_stall_ns = 0;
 
   // phase state
   bool have_tree = false, have_lists = false, have_up = false, have_horiz = false, have_down = false;

@@ -55,6 +55,10 @@ constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
 // to the FP64 local expansion: keeps the FP32 accumulation short enough that
 // the mixed form's potential error stays within a few percent of FP64's.
 constexpr int TC_FLUSH_EVERY = 16;
+// Limit of every wait of the tensor-core kernel (the drain of copies and MMAs
+// already in flight gets twice as long): a wait that runs out flags
+// EXAFMM_ERR_TIMEOUT instead of hanging the GPU.
+constexpr long TC_WAIT_NS = 2000000000L;
 // group keys read back with the counts (more take a second read)
 constexpr int OP_KEYS_HOST = 8192;
 
@@ -236,10 +240,61 @@ __global__ void k_mscale(int ncells, int P, int KP, const double4 *xr, const dou
   Mt[i] = mscaled(c, k, tri(P), xr, M);
 }
 
-// Mixed form: the scaled multipoles split into FP16 hi and lo parts
-// (M16[c][0..KP) hi, M16[c][KP..2KP) lo), written directly; one thread per
-// coefficient (n, m) writes its real and imaginary parts.
-__global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const double2 *M, __half2 *M16) {
+// Degree n of coefficient index ci (tri(n) <= ci < tri(n + 1)) and 1 / R^n.
+__device__ __forceinline__ double mscale_factor(int ci, double R) {
+  int n = (int)((sqrtf(8.0f * ci + 1.0f) - 1.0f) * 0.5f);
+  while (tri(n) > ci) n--;
+  while (tri(n + 1) <= ci) n++;
+  const double inv = 1.0 / R;
+  double s = 1, b = inv;  // inv^n
+  for (int e = n; e; e >>= 1, b *= b)
+    if (e & 1) s *= b;
+  return s;
+}
+
+// Power-of-two exponent E of the FP16 split: the largest scaled multipole
+// times 2^E lies in [2^14, 2^15), so every source's leading coefficients are
+// normal FP16 numbers with an 11-bit lo part below them, whatever the scale
+// of the charges (charges of 1/N put a leaf's monopole below FP16's smallest
+// normal number), and nothing reaches FP16's largest (65504).
+__device__ __forceinline__ int m16_exponent(unsigned long long bits) {
+  const double mx = __longlong_as_double((long long)bits);
+  if (!(mx > 0.0) || !isfinite(mx)) return 0;
+  const int e = 14 - ilogb(mx);
+  return e < -500 ? -500 : (e > 500 ? 500 : e);
+}
+
+// Largest |real or imaginary part| of the scaled multipoles M_n / R^n over
+// the cells that can be M2L sources (every level but the roots'), into
+// *mx as double bits (non-negative doubles order like their bit patterns).
+__global__ void k_m16_max(int ncells, int P, const double4 *xr, const int *level, const double2 *M,
+                          unsigned long long *mx) {
+  const int NT = tri(P);
+  double v = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (long)ncells * NT;
+       i += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(i / NT), ci = (int)(i - (long)c * NT);
+    if (level[c] == 0) continue;
+    const double2 m = M[i];
+    const double s = mscale_factor(ci, xr[c].w);
+    v = fmax(v, fmax(fabs(m.x), fabs(m.y)) * s);
+  }
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __shared__ double wmax[TB / 32];
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, wmax[w]);
+    if (v > 0.0) atomicMax(mx, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// Mixed form: the scaled multipoles, times 2^E (m16_exponent), split into
+// FP16 hi and lo parts (M16[c][0..KP) hi, M16[c][KP..2KP) lo), written
+// directly; one thread per coefficient (n, m) writes its real and imaginary
+// parts.
+__global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const double2 *M,
+                           const unsigned long long *mx, __half2 *M16) {
   const int half_kp = KP / 2;
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long)ncells * half_kp) return;
@@ -247,13 +302,7 @@ __global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const d
   const int ci = (int)(i - c * half_kp), NT = tri(P);
   double2 v = make_double2(0, 0);
   if (ci < NT) {
-    int n = (int)((sqrtf(8.0f * ci + 1.0f) - 1.0f) * 0.5f);  // degree: tri(n) <= ci < tri(n + 1)
-    while (tri(n) > ci) n--;
-    while (tri(n + 1) <= ci) n++;
-    const double inv = 1.0 / xr[c].w;
-    double s = 1, b = inv;  // inv^n
-    for (int e = n; e; e >>= 1, b *= b)
-      if (e & 1) s *= b;
+    const double s = scalbn(mscale_factor(ci, xr[c].w), m16_exponent(*mx));
     const double2 m = M[c * NT + ci];
     v = make_double2(m.x * s, m.y * s);
   }
@@ -468,11 +517,12 @@ __device__ __forceinline__ void tc_zero(uint32_t cols, int cb, int ce) {
 }
 
 // Stores the running sum as the FP64 local expansion, unscaled
-// (L = L~ / R_t^(j+1)).  The tile is the only grouped writer of its targets.
-__device__ __forceinline__ void tc_store(uint32_t hi, uint32_t lo, int t, double inv, int cb, int ce, int NT,
-                                         double2 *L) {
+// (L = L~ / R_t^(j+1), and the split's 2^E removed: us = 2^-E).  The tile is
+// the only grouped writer of its targets.
+__device__ __forceinline__ void tc_store(uint32_t hi, uint32_t lo, int t, double inv, double us, int cb, int ce,
+                                         int NT, double2 *L) {
   int j = 0;
-  double sj = inv;  // inv^(j+1)
+  double sj = inv * us;  // us * inv^(j+1)
   for (int c0 = cb; c0 < ce; c0 += 16) {
     uint32_t h[16], l[16];
     tc::ld_32x32b_x16_async(hi + (uint32_t)c0, h);
@@ -496,10 +546,10 @@ __device__ __forceinline__ void tc_store(uint32_t hi, uint32_t lo, int t, double
 // Without room in TMEM for the running sum (KP > 128): the accumulator is
 // added into the FP64 L in global memory, eight independent
 // read-modify-writes at a time.
-__device__ __forceinline__ void tc_flush_global(uint32_t acc, int t, double inv, int cb, int ce, int NT,
+__device__ __forceinline__ void tc_flush_global(uint32_t acc, int t, double inv, double us, int cb, int ce, int NT,
                                                 double2 *L) {
   int j = 0;
-  double sj = inv;
+  double sj = inv * us;
   for (int c0 = cb; c0 < ce; c0 += 16) {
     float v[16];
     tc::ld_32x32b_x16(acc + (uint32_t)c0, v);
@@ -534,7 +584,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
                                                           const __half *M16, const double4 *xr, double2 *L, int P,
                                                           int KP, TcPlan pl,
                                                           int nstage, uint32_t half_cols, int fold, int flush_every,
-                                                          int *err, long spin) {
+                                                          const unsigned long long *m16_max, int *err, long wait_ns,
+                                                          long stall_ns) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   unsigned char *base = smraw + ((1024u - (tc::smem_u32(smraw) & 1023u)) & 1023u);  // swizzle atoms: 1024-aligned
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, tile = blockIdx.x;
@@ -545,7 +596,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
   uint64_t *empty = full + 4;                                          // [2] MMAs reading the stage finished
   uint64_t *accf = full + 6;                                           // [2] accumulator window complete
   uint64_t *acce = full + 8;                                           // [2] accumulator folded, reusable
-  uint32_t *tslot = (uint32_t *)(full + 10);
+  uint64_t *stall = full + 10;  // nothing arrives here (the stall test hook waits on it)
+  uint32_t *tslot = (uint32_t *)(full + 11);
+  volatile int *abort = (volatile int *)(tslot + 1);  // a role gave up: the others stop waiting
   // TMEM columns: accumulators [0, H) and [H, 2H); with `fold`, the running
   // sum hi at [2H, 3H) and lo at [3H, 4H)
   const uint32_t ncols = (fold ? 4u : 2u) * half_cols;
@@ -554,6 +607,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     for (int b = 0; b < 2; b++) tc::mbar_init(&full[b], TC_LOAD_WARPS * 32);
     for (int b = 2; b < 8; b++) tc::mbar_init(&full[b], 1);
     for (int b = 8; b < 10; b++) tc::mbar_init(&full[b], TC_EPI_WARPS);
+    tc::mbar_init(stall, 1);
+    *abort = 0;
   }
   tc::fence_before();
   __syncthreads();
@@ -567,6 +622,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     // ---- epilogue: warp w owns TMEM lanes 32w.. = targets 32w..
     const int t = tile_tgt[tile * TC_TILE + tid];
     const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
+    const double us = scalbn(1.0, -m16_exponent(*m16_max));
     const int NT = tri(P);
     const uint32_t lanes = tmem + ((uint32_t)(warp * 32) << 16);
     const uint32_t sum_hi = lanes + 2 * half_cols, sum_lo = lanes + 3 * half_cols;
@@ -577,20 +633,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     bool ok = true;
     for (int w = 0; w < nwin; w++) {
       const int a = w & 1;
-      ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[a], (uint32_t)(w >> 1) & 1u, spin));
+      ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[a], (uint32_t)(w >> 1) & 1u, wait_ns, abort));
       if (!ok) break;
       tc::fence_after();
       const uint32_t acc = lanes + (uint32_t)a * half_cols;
       if (fold) tc_fold(acc, sum_hi, sum_lo, 0, KP);
-      else tc_flush_global(acc, t, inv, 0, KP, NT, L);
+      else tc_flush_global(acc, t, inv, us, 0, KP, NT, L);
       tc::fence_before();
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&acce[a]);
     }
     if (!ok) {
+      *abort = 1;
       if (lane == 0) atomicExch(err, 1);
     } else if (fold && n > 0) {
-      tc_store(sum_hi, sum_lo, t, inv, 0, KP, NT, L);
+      tc_store(sum_hi, sum_lo, t, inv, us, 0, KP, NT, L);
     }
   } else if (warp < TC_LOAD_WARP + TC_LOAD_WARPS) {
     // ---- producers: thread r copies target row r of the tile -- the 16-byte
@@ -626,7 +683,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     int s_next = src_of(0);
     for (int k = 0; k < n; k++) {
       if (k >= nstage) {  // the stage is free once the MMAs of group k - nstage are done
-        ok = __all_sync(0xffffffffu, tc::mbar_wait(&empty[k % nstage], (uint32_t)(k / nstage - 1) & 1u, spin));
+        ok = __all_sync(0xffffffffu,
+                        tc::mbar_wait(&empty[k % nstage], (uint32_t)(k / nstage - 1) & 1u, wait_ns, abort));
         if (!ok) break;
       }
       issue(k, s_next);
@@ -634,9 +692,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
       last = k;
       s_next = src_of(k + 1);
     }
-    if (!ok && lane == 0) atomicExch(err, 1);
+    if (!ok) {
+      *abort = 1;
+      if (lane == 0) atomicExch(err, 1);
+    }
+    // drain this thread's copies; the operator's bulk copy completes by
+    // itself (bounded wait, no abort: the copy must land before exit)
     tc::cp_async_wait_all();
-    if (r == 0 && last >= 0) tc::mbar_wait(&bful[last % nstage], parity(last), spin);  // drain (bounded)
+    if (r == 0 && last >= 0) tc::mbar_wait(&bful[last % nstage], parity(last), 2 * wait_ns);
   } else if (warp == TC_MMA_WARP) {
     // ---- MMA issuer (one thread): per group and output block, K steps of
     // hi*hi + hi*lo + lo*hi into the window's accumulator
@@ -650,12 +713,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         boff[b] = b < pl.nb ? (uint32_t)pl.boff[b] : 0u;
         idesc[b] = tc::idesc_f16_f32(TC_TILE, rows[b] > 0 ? rows[b] : 16);
       }
-      bool ok = true;
+      // test hook: a wait on a barrier that nothing arrives at, as if the
+      // tensor core's inputs never came; it runs out after stall_ns
+      bool ok = stall_ns <= 0 || tc::mbar_wait(stall, 0u, stall_ns, abort);
       int last = -1;
-      for (int k = 0; k < n; k++) {
+      for (int k = 0; ok && k < n; k++) {
         const int st = k % nstage, w = k / flush_every, a = w & 1;
-        ok = tc::mbar_wait(&full[st], parity(k), spin) && tc::mbar_wait(&bful[st], parity(k), spin);
-        if (ok && k % flush_every == 0 && w >= 2) ok = tc::mbar_wait(&acce[a], (uint32_t)((w >> 1) - 1) & 1u, spin);
+        ok = tc::mbar_wait(&full[st], parity(k), wait_ns, abort) && tc::mbar_wait(&bful[st], parity(k), wait_ns, abort);
+        if (ok && k % flush_every == 0 && w >= 2)
+          ok = tc::mbar_wait(&acce[a], (uint32_t)((w >> 1) - 1) & 1u, wait_ns, abort);
         if (!ok) break;
         tc::fence_after();
         const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
@@ -679,8 +745,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         if (k % flush_every == flush_every - 1 || k == n - 1) tc::commit(&accf[a]);
         last = k;
       }
-      if (!ok) atomicExch(err, 1);
-      if (last >= 0) tc::mbar_wait(&empty[last % nstage], parity(last), spin);  // drain (bounded)
+      if (!ok) {
+        *abort = 1;
+        atomicExch(err, 1);
+      }
+      // drain: the MMAs already issued complete by themselves (no abort)
+      if (last >= 0) tc::mbar_wait(&empty[last % nstage], parity(last), 2 * wait_ns);
     }
     __syncwarp();
   }
@@ -759,6 +829,8 @@ bool tc_available(int P) {
 
 }  // namespace
 
+int m2l_flush_interval(const Handle &h) { return h.tile_m2l_flush > 0 ? h.tile_m2l_flush : TC_FLUSH_EVERY; }
+
 bool m2l_grouped_available(int P) {
   PlanCache &pc = plan_cache(P);
   return pc.host.P == P && gemm64_smem(pc.host) <= 200 * 1024;
@@ -787,8 +859,10 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
     k_m2l_tc<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
                                                     h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
                                                     h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
-                                                    tc_stages(tp), hc, 4 * hc <= 512 ? 1 : 0, TC_FLUSH_EVERY,
-                                                    &ctr->tc_error, 20000000L);
+                                                    tc_stages(tp), hc, 4 * hc <= 512 ? 1 : 0,
+                                                    m2l_flush_interval(h),
+                                                    &ctr->m16_max, &ctr->tc_error, TC_WAIT_NS, h.tc_stall_ns);
+    h.tc_stall_ns = 0;  // the test hook stalls one launch
     FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
     h.g_used_tc = true;
   } else {
@@ -818,8 +892,13 @@ void m2l_grouped_pass(Handle &h) {
   // scaled multipoles: FP64 (DMMA) or FP16 hi/lo (tensor core)
   if (tcore) {
     h.g_m16.need((size_t)C * 2 * KP16 * sizeof(__half));
+    u64 *m16_max = &h.counters.as<DevCounters>()->m16_max;
+    FMM_CUDA(cudaMemsetAsync(m16_max, 0, sizeof(u64), s));
+    k_m16_max<<<std::min<long>(grid_for((long)C * NT, TB), 148 * 8), TB, 0, s>>>(
+        C, P, h.c_xr.as<double4>(), h.c_level.as<int>(), h.M.as<double2>(), m16_max);
     k_mscale16<<<grid_for((long)C * (KP16 / 2), TB), TB, 0, s>>>(C, P, KP16, h.c_xr.as<double4>(),
-                                                                 h.M.as<double2>(), h.g_m16.as<__half2>());
+                                                                 h.M.as<double2>(), m16_max, h.g_m16.as<__half2>());
+    h.launches++;
   } else {
     h.g_mt.need((size_t)C * gp.KP * sizeof(double));
     k_mscale<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>(C, P, gp.KP, h.c_xr.as<double4>(), h.M.as<double2>(),

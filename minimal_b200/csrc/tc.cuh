@@ -93,11 +93,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: false if the barrier did not flip within `limit` polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long limit) {
-  for (long i = 0; i < limit; i++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait: false if the barrier did not flip within `limit_ns`
+// nanoseconds of the device's global timer, or -- when `abort` is given --
+// once another role of the CTA has set *abort (it gave up first, so this
+// wait would only run out in turn).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long limit_ns,
+                                          const volatile int *abort = nullptr) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
+    for (int i = 0; i < 16; i++)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (abort && *abort) return false;
+    if (globaltimer_ns() - t0 > (uint64_t)limit_ns) return false;
+  }
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {

@@ -351,7 +351,7 @@ __global__ void k_gather_cells(const u32 *pre_of_bfs, const int *bfs_of_pre, lon
 }
 
 // Reference cell number: 1 + (children allocated by parents earlier in
-// pre-order) + rank among siblings (3d/build_tree.h:117-131).
+// pre-order) + rank among siblings (3d/build_tree.h:69-84).
 __global__ void k_ref_index(BfsCells o, long c, const int *blockstart_pre, int *ref) {
   const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= c) return;

@@ -223,7 +223,7 @@ static void to_csr(const entry *e, long n, int **off, entry **csr) {
   free(fill);
 }
 
-/* 3dp/traverse_lazy.h:276-293 (horizontalPass list part): with images, one
+/* 3dp/traverse_lazy.h:124-141 (horizontalPass list part): with images, one
  * walk per first-shell shift, x outermost. */
 long orc_lists(double theta, int images, double cycle) {
   THETA_ = theta;

@@ -10,7 +10,7 @@
  *
  * The state is global (one problem at a time), as in the reference.  All
  * arrays in/out are caller-owned.  Cells are reported in the reference's cell
- * order (3d/build_tree.h:117-131: children appended as one block when the
+ * order (3d/build_tree.h:69-84: children appended as one block when the
  * parent is visited, depth first).  Bodies are reported in tree order.
  */
 #ifndef FMM_ORACLE_H

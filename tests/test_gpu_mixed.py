@@ -28,19 +28,45 @@ def errors(fmm, n, nt=1000):
     return rel(res[:, 4], d[:, 4]), rel(res[:, 5:], d[:, 5:]), out
 
 
+def make_bodies(n, dist):
+    """uniform: the reference driver's bodies (charges U[-0.5,0.5), neutral);
+    uniform_1e-6: the same with every charge times 1e-6; plummer: a Plummer
+    sphere with its own equal charges 1/N (the non-uniform benchmark's
+    bodies, positions and charges rounded to FP32 values); plummer_pm: the
+    same positions with charges U[-0.5,0.5)."""
+    from minimal_b200 import drand48_bodies, plummer_bodies
+
+    if dist.startswith("uniform"):
+        xq = drand48_bodies(n, 3)
+        if dist == "uniform_1e-6":
+            xq[:, 3] *= 1e-6
+        return xq
+    xq = plummer_bodies(n, 3).astype(np.float32).astype(np.float64)
+    if dist == "plummer_pm":
+        xq[:, 3] = np.random.default_rng(3).uniform(-0.5, 0.5, n)
+    return xq
+
+
 @pytest.mark.parametrize("n,P,theta,ncrit,dist", [
     (10000, 10, 0.4, 64, "uniform"),
     (200000, 10, 0.4, 64, "uniform"),
-    (100000, 8, 0.5, 32, "plummer"),
+    (100000, 8, 0.5, 32, "plummer_pm"),
     (60000, 12, 0.4, 64, "uniform"),
     (30000, 6, 0.5, 16, "uniform"),
+    (60000, 12, 0.4, 64, "uniform_1e-6"),
+    (200000, 10, 0.4, 64, "plummer"),
+    (200000, 12, 0.4, 64, "plummer"),
+    (100000, 8, 0.4, 64, "plummer"),
+    (100000, 6, 0.4, 64, "plummer"),
 ])
 def test_mixed_error_close_to_fp64(n, P, theta, ncrit, dist):
-    from minimal_b200 import FMM, drand48_bodies, plummer_bodies
+    """Charge scale does not matter: the FP16 split of the tensor-core M2L
+    normalises the multipoles by a power of two taken from their largest
+    magnitude, so charges of 1/N (or 1e-6 times the usual) keep the same
+    relative accuracy as charges of order one."""
+    from minimal_b200 import FMM
 
-    xq = drand48_bodies(n, 3) if dist == "uniform" else plummer_bodies(n, 3)
-    if dist == "plummer":
-        xq[:, 3] = np.random.default_rng(3).uniform(-0.5, 0.5, n)
+    xq = make_bodies(n, dist)
     res = {}
     for prec in ("fp64", "mixed"):
         f = FMM(P=P, ncrit=ncrit, theta=theta, precision=prec)

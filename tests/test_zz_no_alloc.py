@@ -46,10 +46,15 @@ def test_direct_static_matches_direct_twice():
         tgt[:, :4] = xq[::stride][:nt]
         want = fmm.direct(tgt)  # existing entry point, handle-based
         d_tgt = torch.from_numpy(tgt).to(dev)  # p, F start at zero
+        torch.cuda.synchronize(dev)
+        free_before = torch.cuda.mem_get_info(dev)[0]
         rc = lib.exafmm_b200_direct_static(ctypes.c_void_p(d_src.data_ptr()), len(src),
                                            ctypes.c_void_p(d_tgt.data_ptr()), nt, ctypes.c_void_p(stream))
         assert rc == 0, lib.exafmm_b200_last_error(None).decode()
+        assert lib.exafmm_b200_last_error(None).decode() == "", "a success leaves no error message"
         torch.cuda.synchronize(dev)
+        if call > 0:  # the first call may load the library's module (and its scratch) onto the GPU
+            assert torch.cuda.mem_get_info(dev)[0] == free_before, f"call {call}: device memory was allocated"
         got = d_tgt.cpu().numpy()
         assert np.array_equal(got[:, :4], tgt[:, :4]), f"call {call}: positions must be untouched"
         assert rel_l2(got[:, 4], want[:, 4]) < TOL, f"call {call}: potential"
@@ -69,3 +74,23 @@ def test_direct_static_rejects_oversize_without_launching():
                                        None)
     assert rc == -1
     assert "65536" in lib.exafmm_b200_last_error(None).decode()
+
+
+def test_direct_static_rejects_a_stream_of_another_device():
+    """The scratch address is per device, so the caller's stream must belong
+    to the current device: a stream of a second device is refused before
+    anything is launched (needs two GPUs; skipped on one)."""
+    import torch
+
+    import minimal_b200
+
+    lib = minimal_b200.load_library()
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    torch.cuda.set_device(0)
+    s1 = torch.cuda.Stream(device=1)
+    d = torch.zeros((8, 8), dtype=torch.float64, device="cuda:0")
+    rc = lib.exafmm_b200_direct_static(ctypes.c_void_p(d.data_ptr()), 8, ctypes.c_void_p(d.data_ptr()), 8,
+                                       ctypes.c_void_p(s1.cuda_stream))
+    assert rc == -1
+    assert "stream" in lib.exafmm_b200_last_error(None).decode()
