@@ -156,6 +156,50 @@ EXAFMM_API int exafmm_b200_dipole_correction(exafmm_b200 *h);
 EXAFMM_API int exafmm_b200_ewald(exafmm_b200 *h, int ksize, double alpha, double sigma, double cutoff,
                                  double *targets8, int64_t nt, int where);
 
+/* The Ewald parts one at a time (or any mask of them), as the reference's
+ * periodic driver calls them (3dp/fmm.cxx:85-93): EXAFMM_EWALD_WAVE replaces
+ * wavePart (3dp/ewald.h:130-143), EXAFMM_EWALD_REAL realPart
+ * (3dp/ewald.h:122-127; nearest image per axis, as above), EXAFMM_EWALD_SELF
+ * selfTerm (3dp/ewald.h:146-150: p -= 2/sqrt(pi) q alpha, which needs no
+ * loaded bodies).  Sources are the handle's bodies; p and F of the targets
+ * accumulate; exafmm_b200_ewald() is EXAFMM_EWALD_ALL. */
+enum { EXAFMM_EWALD_WAVE = 1, EXAFMM_EWALD_REAL = 2, EXAFMM_EWALD_SELF = 4, EXAFMM_EWALD_ALL = 7 };
+EXAFMM_API int exafmm_b200_ewald_parts(exafmm_b200 *h, int parts, int ksize, double alpha, double sigma,
+                                       double cutoff, double *targets8, int64_t nt, int where);
+
+/* Single operators: the reference's kernel functions one call at a time, on
+ * cells the caller describes (3d/kernel.h:122-323; the kernel test and the
+ * operator chain of 3d/kernel.cxx:4-91 and test/test_kernel.h:6-94 call them
+ * this way).  The order P is the handle's; no bodies need to be loaded.  A
+ * cell is its centre and radius, 4 doubles X[3], R (the layout of
+ * exafmm_b200_get_tree's xr; R is not read); an expansion is NTERM complex
+ * coefficients, re and im interleaved, index n(n+1)/2+m (3d/kernel.h:197);
+ * bodies are Body records.  Outputs accumulate, as the reference's += does.
+ * `where` says whether all the call's arrays are in host or device memory.
+ * shift3 (3 doubles, or NULL for none) is the periodic source offset iX*cycle
+ * of the 3dp variants: the pair offset is (Xi - Xj) - shift3
+ * (3dp/kernel.h:133, :200).  FP64, the same arithmetic as the FP64 form.
+ *   p2p  P2P(Ci, Cj) (3d/kernel.h:122-150): sources onto targets' p and F.
+ *   p2m  P2M(C) (3d/kernel.h:187-202): the cell's bodies into its M.
+ *   m2m  M2M(Ci) (3d/kernel.h:204-231): nchild children (centres
+ *        children4, multipoles Mchildren, nchild x NTERM) into the parent's M.
+ *   m2l  M2L(Ci, Cj) (3d/kernel.h:233-260): the source's M into the target's L.
+ *   l2l  L2L(Cj) (3d/kernel.h:262-291): the parent's L into each child's L
+ *        (Lchildren, nchild x NTERM).
+ *   l2p  L2P(C) (3d/kernel.h:293-323): the cell's L into its bodies' p and F. */
+EXAFMM_API int exafmm_b200_p2p(exafmm_b200 *h, double *targets8, int64_t nt, const double *sources8, int64_t ns,
+                               const double *shift3, int where);
+EXAFMM_API int exafmm_b200_p2m(exafmm_b200 *h, const double *cell4, const double *bodies8, int64_t nb, double *M,
+                               int where);
+EXAFMM_API int exafmm_b200_m2m(exafmm_b200 *h, const double *parent4, double *M, int nchild, const double *children4,
+                               const double *Mchildren, int where);
+EXAFMM_API int exafmm_b200_m2l(exafmm_b200 *h, const double *target4, double *L, const double *source4,
+                               const double *M, const double *shift3, int where);
+EXAFMM_API int exafmm_b200_l2l(exafmm_b200 *h, const double *parent4, const double *L, int nchild,
+                               const double *children4, double *Lchildren, int where);
+EXAFMM_API int exafmm_b200_l2p(exafmm_b200 *h, const double *cell4, const double *L, double *bodies8, int64_t nb,
+                               int where);
+
 /* Batch of independent free-space systems (no reference counterpart: the
  * reference evaluates one system per process).  bodies8 holds the systems'
  * Body records one after the other; system q owns records

@@ -22,16 +22,25 @@
  *                           bodies given to buildTree (the reference
  *                           accumulates, callers zero them first)
  *   direct(targets, sources) FP64 direct sum on the GPU, added into targets
+ *   P2P(Ci, Cj), P2M(C), M2M(Ci), M2L(Ci, Cj), L2L(Cj), L2P(C)
+ *                           the single operators of 3d/kernel.h:122-323 on the
+ *                           GPU (exafmm_b200_p2p ...), for drivers that call
+ *                           them one by one (3d/kernel.cxx, test/test_kernel.h);
+ *                           the 3dp shift iX * cycle is applied to P2P and M2L
+ *   wavePart(bodies, jbodies), realPart(Ci, Cj), selfTerm(bodies)
+ *                           the Ewald parts of 3dp/ewald.h:122-150 on the GPU
+ *                           (exafmm_b200_ewald_parts), with the globals ksize,
+ *                           alpha, sigma, cutoff
  *   start(event), stop(event) wall-clock timers printing as 3d/timer.h does
  *
  * Differences, by design: the handle keeps its own copy of the bodies from
  * buildTree (the passes do not read the caller's vector again); Cell::M and
  * Cell::L are filled after downwardPass only when `keep_expansions` is set
- * (they are large and no driver reads them); the operator-level kernels
- * (P2M(Cell*), M2L(Cell*, Cell*), ...) and the periodic Ewald parts
- * (wavePart, realPart, selfTerm) are not provided -- the GPU runs whole
- * passes, and exafmm_b200_ewald() sums all Ewald parts at once.  Errors of
- * the C ABI are thrown as exafmm::Error.
+ * (they are large and no driver reads them); the single operators run on a
+ * second handle, so they never disturb the tree of the first; realPart takes
+ * each source at its nearest periodic image inside the cutoff (the
+ * reference's neighbour search picks one image per pair of cells).  Errors
+ * of the C ABI are thrown as exafmm::Error.
  */
 #ifndef EXAFMM_B200_HPP
 #define EXAFMM_B200_HPP
@@ -86,6 +95,13 @@ inline real_t cycle = 0;
 inline int precision = EXAFMM_FP64;
 inline int device = 0;
 inline bool keep_expansions = false;
+// 3dp: the periodic image of the current P2P / M2L source (3dp/exafmm.h:46)
+// and the Ewald parameters (3dp/ewald.h:13-16)
+inline int iX[3] = {0, 0, 0};
+inline int ksize = 0;
+inline real_t alpha = 0;
+inline real_t sigma = 0;
+inline real_t cutoff = 0;
 
 struct Error : std::runtime_error {
   int code;
@@ -145,6 +161,44 @@ inline exafmm_b200 *handle() {
 inline exafmm_b200 *current() {
   if (!state().h || !state().bodies) throw Error(EXAFMM_ERR_STATE, "exafmm: buildTree() has not run");
   return state().h;
+}
+
+// The handle of the single operators and the self term (no bodies needed):
+// its own, so that they never reset the tree of the handle above.
+struct OpState {
+  exafmm_b200 *h = nullptr;
+  exafmm_params prm{};
+  ~OpState() {
+    if (h) exafmm_b200_destroy(h);
+  }
+};
+inline exafmm_b200 *op_handle() {
+  static OpState s;
+  const exafmm_params p = params();
+  if (!s.h) {
+    s.h = create();
+  } else if (p.P != s.prm.P || p.images != s.prm.images || p.cycle != s.prm.cycle || p.precision != s.prm.precision) {
+    check(exafmm_b200_set_params(s.h, &p), s.h);
+  }
+  s.prm = p;
+  return s.h;
+}
+
+inline void cell4(const Cell *c, double *x) {
+  for (int d = 0; d < 3; d++) x[d] = c->X[d];
+  x[3] = c->R;
+}
+
+// the 3dp source shift iX * cycle (3dp/kernel.h:133, :200)
+inline const double *image_shift(double *s) {
+  for (int d = 0; d < 3; d++) s[d] = iX[d] * cycle;
+  return s;
+}
+
+inline complex_t *terms(std::vector<complex_t> &v, const char *what) {
+  if (v.size() < (size_t)(P * (P + 1) / 2))
+    throw Error(EXAFMM_ERR_ARG, std::string("exafmm: ") + what + " needs NTERM coefficients (resize it first)");
+  return v.data();
 }
 
 }  // namespace shim
@@ -227,6 +281,114 @@ inline void direct(Bodies &targets, Bodies &sources) {
     throw;
   }
   exafmm_b200_destroy(h);
+}
+
+// ---- single operators (3d/kernel.h:122-323)
+inline void P2P(Cell *Ci, Cell *Cj) {
+  exafmm_b200 *h = shim::op_handle();
+  double s[3];
+  shim::check(exafmm_b200_p2p(h, (double *)Ci->BODY, Ci->NBODY, (const double *)Cj->BODY, Cj->NBODY,
+                              shim::image_shift(s), EXAFMM_HOST),
+              h);
+}
+
+inline void P2M(Cell *C) {
+  exafmm_b200 *h = shim::op_handle();
+  double c[4];
+  shim::cell4(C, c);
+  shim::check(exafmm_b200_p2m(h, c, (const double *)C->BODY, C->NBODY, (double *)shim::terms(C->M, "P2M: Cell::M"),
+                              EXAFMM_HOST),
+              h);
+}
+
+inline void M2M(Cell *Ci) {
+  exafmm_b200 *h = shim::op_handle();
+  const size_t nt = (size_t)P * (P + 1) / 2;
+  double c[4];
+  shim::cell4(Ci, c);
+  std::vector<double> kids(4 * (size_t)Ci->NCHILD);
+  std::vector<complex_t> Mk(nt * Ci->NCHILD);
+  for (int k = 0; k < Ci->NCHILD; k++) {
+    Cell *Cj = Ci->CHILD + k;
+    shim::cell4(Cj, &kids[4 * k]);
+    const complex_t *m = shim::terms(Cj->M, "M2M: child Cell::M");
+    for (size_t t = 0; t < nt; t++) Mk[k * nt + t] = m[t];
+  }
+  shim::check(exafmm_b200_m2m(h, c, (double *)shim::terms(Ci->M, "M2M: Cell::M"), Ci->NCHILD, kids.data(),
+                              (const double *)Mk.data(), EXAFMM_HOST),
+              h);
+}
+
+inline void M2L(Cell *Ci, Cell *Cj) {
+  exafmm_b200 *h = shim::op_handle();
+  double ci[4], cj[4], s[3];
+  shim::cell4(Ci, ci);
+  shim::cell4(Cj, cj);
+  shim::check(exafmm_b200_m2l(h, ci, (double *)shim::terms(Ci->L, "M2L: Cell::L"), cj,
+                              (const double *)shim::terms(Cj->M, "M2L: Cell::M"), shim::image_shift(s), EXAFMM_HOST),
+              h);
+}
+
+inline void L2L(Cell *Cj) {
+  exafmm_b200 *h = shim::op_handle();
+  const size_t nt = (size_t)P * (P + 1) / 2;
+  double c[4];
+  shim::cell4(Cj, c);
+  std::vector<double> kids(4 * (size_t)Cj->NCHILD);
+  std::vector<complex_t> Lk(nt * Cj->NCHILD);
+  for (int k = 0; k < Cj->NCHILD; k++) {
+    Cell *Ci = Cj->CHILD + k;
+    shim::cell4(Ci, &kids[4 * k]);
+    const complex_t *l = shim::terms(Ci->L, "L2L: child Cell::L");
+    for (size_t t = 0; t < nt; t++) Lk[k * nt + t] = l[t];
+  }
+  shim::check(exafmm_b200_l2l(h, c, (const double *)shim::terms(Cj->L, "L2L: Cell::L"), Cj->NCHILD, kids.data(),
+                              (double *)Lk.data(), EXAFMM_HOST),
+              h);
+  for (int k = 0; k < Cj->NCHILD; k++)
+    for (size_t t = 0; t < nt; t++) Cj->CHILD[k].L[t] = Lk[k * nt + t];
+}
+
+inline void L2P(Cell *Ci) {
+  exafmm_b200 *h = shim::op_handle();
+  double c[4];
+  shim::cell4(Ci, c);
+  shim::check(exafmm_b200_l2p(h, c, (const double *)shim::terms(Ci->L, "L2P: Cell::L"), (double *)Ci->BODY,
+                              Ci->NBODY, EXAFMM_HOST),
+              h);
+}
+
+// ---- Ewald parts (3dp/ewald.h:122-150): sources on a handle of their own
+namespace shim {
+inline void ewald_part(int part, const Body *sources, int64_t ns, Body *targets, int64_t nt) {
+  if (nt <= 0) return;
+  exafmm_b200 *h = create();
+  try {
+    check(exafmm_b200_set_bodies(h, (const double *)sources, ns, EXAFMM_HOST), h);
+    check(exafmm_b200_build_tree(h), h);
+    check(exafmm_b200_ewald_parts(h, part, ksize, alpha, sigma, cutoff, (double *)targets, nt, EXAFMM_HOST), h);
+  } catch (...) {
+    exafmm_b200_destroy(h);
+    throw;
+  }
+  exafmm_b200_destroy(h);
+}
+}  // namespace shim
+
+inline void wavePart(Bodies &bodies, Bodies &jbodies) {
+  shim::ewald_part(EXAFMM_EWALD_WAVE, jbodies.data(), (int64_t)jbodies.size(), bodies.data(), (int64_t)bodies.size());
+}
+
+inline void realPart(Cell *Ci, Cell *Cj) {
+  shim::ewald_part(EXAFMM_EWALD_REAL, Cj->BODY, Cj->NBODY, Ci->BODY, Ci->NBODY);
+}
+
+inline void selfTerm(Bodies &bodies) {
+  if (bodies.empty()) return;
+  exafmm_b200 *h = shim::op_handle();
+  shim::check(exafmm_b200_ewald_parts(h, EXAFMM_EWALD_SELF, ksize, alpha, sigma, cutoff, (double *)bodies.data(),
+                                      (int64_t)bodies.size(), EXAFMM_HOST),
+              h);
 }
 
 namespace shim {

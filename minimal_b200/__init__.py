@@ -40,6 +40,7 @@ API = [
     "exafmm_b200_dipole_correction", "exafmm_b200_ewald", "exafmm_b200_set_batch", "exafmm_b200_autotune",
     "exafmm_b200_set_charges", "exafmm_b200_reevaluate", "exafmm_b200_test_stall_tc",
     "exafmm_b200_set_tile", "exafmm_b200_get_tile",
+    "exafmm_b200_ewald_parts", "exafmm_b200_p2p", "exafmm_b200_p2m", "exafmm_b200_m2m", "exafmm_b200_m2l", "exafmm_b200_l2l", "exafmm_b200_l2p",
 ]
 
 PHASES = ["tree", "lists", "upward", "m2l", "p2p", "downward", "total"]
@@ -102,6 +103,13 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_reevaluate": (i, [vp]),
         "exafmm_b200_test_stall_tc": (i, [vp, i64]),
         "exafmm_b200_set_tile": (i, [vp, i, i]),
+        "exafmm_b200_ewald_parts": (i, [vp, i, i, d, d, d, vp, i64, i]),
+        "exafmm_b200_p2p": (i, [vp, vp, i64, vp, i64, vp, i]),
+        "exafmm_b200_p2m": (i, [vp, vp, vp, i64, vp, i]),
+        "exafmm_b200_m2m": (i, [vp, vp, vp, i, vp, vp, i]),
+        "exafmm_b200_m2l": (i, [vp, vp, vp, vp, vp, vp, i]),
+        "exafmm_b200_l2l": (i, [vp, vp, vp, i, vp, vp, i]),
+        "exafmm_b200_l2p": (i, [vp, vp, vp, vp, i64, i]),
         "exafmm_b200_get_tile": (i, [vp, i, vp]),
     }
     for name, (res, args) in sig.items():
@@ -293,6 +301,22 @@ class FMM:
                                                len(t), HOST))
         return t
 
+    EWALD_PARTS = {"wave": 1, "real": 2, "self": 4, "all": 7}
+
+    def ewald_parts(self, targets, parts, ksize=11, alpha=None, sigma=0.25 / np.pi, cutoff=None):
+        """Some of the Ewald parts ("wave", "real", "self", a list of them, or
+        "all") onto targets; defaults as in ewald()."""
+        mask = 0
+        for p in ([parts] if isinstance(parts, str) else parts):
+            mask |= self.EWALD_PARTS[p]
+        cyc = self.params.cycle
+        alpha = ksize / cyc if alpha is None else alpha
+        cutoff = cyc / 2 if cutoff is None else cutoff
+        t = as_records(targets).copy()
+        self._check(self.lib.exafmm_b200_ewald_parts(self.h, mask, int(ksize), float(alpha), float(sigma),
+                                                     float(cutoff), _p(t), len(t), HOST))
+        return t
+
     def autotune(self, candidates=None, repeats=2):
         """Pick the fastest leaf size ncrit for the loaded bodies (one system or
         a batch); returns (ncrit, ms per evaluation) and keeps it."""
@@ -314,6 +338,66 @@ class FMM:
 
     def last_launches(self):
         return int(self.lib.exafmm_b200_last_launches(self.h))
+
+    # ---- single operators (3d/kernel.h:122-323) on explicit cells.  cell:
+    # X[3], R; expansions: NTERM complex; bodies: N x 8 Body records.  Each
+    # returns the accumulated output as a new array (inputs are not modified).
+    def _nt(self):
+        return self.params.P * (self.params.P + 1) // 2
+
+    @staticmethod
+    def _c2(a, n):
+        a = np.zeros(n, complex) if a is None else np.asarray(a, complex).ravel()
+        return np.ascontiguousarray(np.stack([a.real, a.imag], -1))
+
+    @staticmethod
+    def _cell(c):
+        c = np.asarray(c, np.float64).ravel()
+        return np.ascontiguousarray(np.concatenate([c, np.zeros(4 - len(c))]) if len(c) < 4 else c[:4])
+
+    def p2p(self, targets, sources, shift=None):
+        t = np.array(as_records(targets), order="C")
+        s = as_records(sources)
+        sh = None if shift is None else np.ascontiguousarray(shift, np.float64)
+        self._check(self.lib.exafmm_b200_p2p(self.h, _p(t), len(t), _p(s), len(s), None if sh is None else _p(sh),
+                                             HOST))
+        return t
+
+    def p2m(self, cell, bodies, M=None):
+        m = self._c2(M, self._nt())
+        b = as_records(bodies)
+        self._check(self.lib.exafmm_b200_p2m(self.h, _p(self._cell(cell)), _p(b), len(b), _p(m), HOST))
+        return m[:, 0] + 1j * m[:, 1]
+
+    def m2m(self, parent, children, Mchildren, M=None):
+        nt = self._nt()
+        m = self._c2(M, nt)
+        ch = np.ascontiguousarray([self._cell(c) for c in children]).reshape(-1, 4)
+        mc = self._c2(Mchildren, nt * len(ch))
+        self._check(self.lib.exafmm_b200_m2m(self.h, _p(self._cell(parent)), _p(m), len(ch), _p(ch), _p(mc), HOST))
+        return m[:, 0] + 1j * m[:, 1]
+
+    def m2l(self, target, source, M, L=None, shift=None):
+        nt = self._nt()
+        lo, mm = self._c2(L, nt), self._c2(M, nt)
+        sh = None if shift is None else np.ascontiguousarray(shift, np.float64)
+        self._check(self.lib.exafmm_b200_m2l(self.h, _p(self._cell(target)), _p(lo), _p(self._cell(source)), _p(mm),
+                                             None if sh is None else _p(sh), HOST))
+        return lo[:, 0] + 1j * lo[:, 1]
+
+    def l2l(self, parent, L, children, Lchildren=None):
+        nt = self._nt()
+        ch = np.ascontiguousarray([self._cell(c) for c in children]).reshape(-1, 4)
+        lc = self._c2(Lchildren, nt * len(ch))
+        self._check(self.lib.exafmm_b200_l2l(self.h, _p(self._cell(parent)), _p(self._c2(L, nt)), len(ch), _p(ch),
+                                             _p(lc), HOST))
+        return (lc[:, 0] + 1j * lc[:, 1]).reshape(len(ch), nt)
+
+    def l2p(self, cell, L, bodies):
+        b = np.array(as_records(bodies), order="C")
+        self._check(self.lib.exafmm_b200_l2p(self.h, _p(self._cell(cell)), _p(self._c2(L, self._nt())), _p(b),
+                                             len(b), HOST))
+        return b
 
     TILES = {"m2l_flush": 0}
 

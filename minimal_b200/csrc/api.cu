@@ -13,6 +13,14 @@
 namespace fmm {
 double fma_peak_tflops(int precision);
 int m2l_flush_interval(const Handle &h);
+void ops_set_attributes();
+void op_p2p_call(Handle &h, double *t8, long nt, const double *s8, long ns, const double *shift3, int where);
+void op_p2m_call(Handle &h, const double *cell4, const double *b8, long nb, double *M, int where);
+void op_l2p_call(Handle &h, const double *cell4, const double *L, double *b8, long nb, int where);
+void op_shift_call(Handle &h, int kind, const double *parent4, const double *in, int nkid, const double *kids4,
+                   double *out, int where);
+void op_m2l_call(Handle &h, const double *t4, double *L, const double *s4, const double *M, const double *shift3,
+                 int where);
 void m2l_set_attributes();
 void m2l_grouped_set_attributes();
 void p2p_set_attributes();
@@ -300,6 +308,7 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     p2p_set_attributes();
     expansions_set_attributes();
     periodic_set_attributes();
+    ops_set_attributes();
     FMM_CUDA(cudaGetLastError());
   } catch (const Error &e) {
     exafmm_b200_static_err = e.msg;
@@ -324,7 +333,8 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
                  &h.leaves, &h.pre_tmp, &h.ctmp, &h.geom, &h.counters, &h.frontier[0], &h.frontier[1],
                  &h.m2l_raw, &h.m2l_key, &h.p2p_raw, &h.m2l_off, &h.m2l_ent, &h.p2p_off, &h.p2p_ent, &h.fill, &h.M, &h.L,
                  &h.m2l_units, &h.stage, &h.g_mt, &h.g_ekey, &h.g_occ, &h.g_cnt, &h.g_keyof, &h.g_ops,
-                 &h.g_tk, &h.g_tile, &h.g_seg, &h.g_tg, &h.g_m16, &h.g_slot, &h.g_pairs, &h.shift_ops, &h.shift_terms};
+                 &h.g_tk, &h.g_tile, &h.g_seg, &h.g_tg, &h.g_m16, &h.g_slot, &h.g_pairs, &h.shift_ops, &h.shift_terms,
+                 &h.op_scratch};
   for (Buf *b : bufs) b->release();
   if (h.ev_ok)
     for (int p = 0; p < PH_COUNT + 1; p++)
@@ -650,10 +660,20 @@ int exafmm_b200_dipole_correction(exafmm_b200 *H) {
 
 int exafmm_b200_ewald(exafmm_b200 *H, int ksize, double alpha, double sigma, double cutoff, double *targets,
                       int64_t nt, int where) {
+  return exafmm_b200_ewald_parts(H, EXAFMM_EWALD_ALL, ksize, alpha, sigma, cutoff, targets, nt, where);
+}
+
+int exafmm_b200_ewald_parts(exafmm_b200 *H, int parts, int ksize, double alpha, double sigma, double cutoff,
+                            double *targets, int64_t nt, int where) {
   return guarded(H, [&](Handle &h) {
-    need_tree(h);
-    need_single(h, "ewald()");
+    if (parts <= 0 || parts > EXAFMM_EWALD_ALL) throw Error{EXAFMM_ERR_ARG, "ewald: parts is a nonzero mask of WAVE, REAL, SELF"};
+    if (parts != EXAFMM_EWALD_SELF) {  // the self term reads only the targets
+      need_tree(h);
+      need_single(h, "ewald()");
+    }
     if (!targets || nt <= 0) throw Error{EXAFMM_ERR_ARG, "need targets"};
+    if (where != EXAFMM_HOST && where != EXAFMM_DEVICE) throw Error{EXAFMM_ERR_ARG, "where must be HOST or DEVICE"};
+    FMM_CUDA(cudaSetDevice(h.prm.device));
     if (ksize < 1 || ksize > 64 || !(alpha > 0) || !(sigma > 0) || !(cutoff > 0))
       throw Error{EXAFMM_ERR_ARG, "ewald: ksize in [1, 64] and positive alpha, sigma, cutoff required"};
     if (!(h.prm.cycle > 0)) throw Error{EXAFMM_ERR_STATE, "ewald() needs a periodic handle (cycle > 0)"};
@@ -661,7 +681,7 @@ int exafmm_b200_ewald(exafmm_b200 *H, int ksize, double alpha, double sigma, dou
     rec.need(nt * 64);
     FMM_CUDA(cudaMemcpyAsync(rec.p, targets, nt * 64, where == EXAFMM_HOST ? cudaMemcpyHostToDevice
                                                                           : cudaMemcpyDeviceToDevice, h.stream));
-    ewald(h, ksize, alpha, sigma, cutoff, h.prm.cycle, rec.as<double>(), nt);
+    ewald(h, parts, ksize, alpha, sigma, cutoff, h.prm.cycle, rec.as<double>(), nt);
     FMM_CUDA(cudaMemcpyAsync(targets, rec.p, nt * 64, where == EXAFMM_HOST ? cudaMemcpyDeviceToHost
                                                                           : cudaMemcpyDeviceToDevice, h.stream));
     FMM_CUDA(cudaStreamSynchronize(h.stream));
@@ -684,6 +704,52 @@ int exafmm_b200_fma_peak(exafmm_b200 *H, int precision, double *tflops) {
     if (precision < 0 || precision > 3) throw Error{EXAFMM_ERR_ARG, "fma_peak: kind in [0, 3]"};
     FMM_CUDA(cudaSetDevice(h.prm.device));
     *tflops = fma_peak_tflops(precision);
+  });
+}
+
+int exafmm_b200_p2p(exafmm_b200 *H, double *targets8, int64_t nt, const double *sources8, int64_t ns,
+                    const double *shift3, int where) {
+  return guarded(H, [&](Handle &h) {
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    op_p2p_call(h, targets8, nt, sources8, ns, shift3, where);
+  });
+}
+
+int exafmm_b200_p2m(exafmm_b200 *H, const double *cell4, const double *bodies8, int64_t nb, double *M, int where) {
+  return guarded(H, [&](Handle &h) {
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    op_p2m_call(h, cell4, bodies8, nb, M, where);
+  });
+}
+
+int exafmm_b200_m2m(exafmm_b200 *H, const double *parent4, double *M, int nchild, const double *children4,
+                    const double *Mchildren, int where) {
+  return guarded(H, [&](Handle &h) {
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    op_shift_call(h, 0, parent4, Mchildren, nchild, children4, M, where);
+  });
+}
+
+int exafmm_b200_m2l(exafmm_b200 *H, const double *target4, double *L, const double *source4, const double *M,
+                    const double *shift3, int where) {
+  return guarded(H, [&](Handle &h) {
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    op_m2l_call(h, target4, L, source4, M, shift3, where);
+  });
+}
+
+int exafmm_b200_l2l(exafmm_b200 *H, const double *parent4, const double *L, int nchild, const double *children4,
+                    double *Lchildren, int where) {
+  return guarded(H, [&](Handle &h) {
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    op_shift_call(h, 1, parent4, L, nchild, children4, Lchildren, where);
+  });
+}
+
+int exafmm_b200_l2p(exafmm_b200 *H, const double *cell4, const double *L, double *bodies8, int64_t nb, int where) {
+  return guarded(H, [&](Handle &h) {
+    FMM_CUDA(cudaSetDevice(h.prm.device));
+    op_l2p_call(h, cell4, L, bodies8, nb, where);
   });
 }
 

@@ -683,6 +683,22 @@ __global__ void __launch_bounds__(WARPS * 32) k_l2p(const int *leaves, int nleav
 
 }  // namespace
 
+// One cell's P2M or L2P with the FP64 pass kernels, for the single-operator
+// entry points: `mini` holds the one-cell tree (leaves = {0}, begin = {0},
+// count = {nb}) in device memory, xr the cell, src the bodies (x,y,z,q).
+void op_p2m(const int *mini, const double4 *xr, const double4 *src, double2 *M, int P, cudaStream_t s) {
+  const int nt = tri(P);
+  k_p2m<<<1, WARPS * 32, WARPS * nt * sizeof(double2), s>>>(mini, 1, mini + 1, mini + 2, xr, src, M, P);
+  FMM_LAUNCH();
+}
+
+void op_l2p(const int *mini, const double4 *xr, const double4 *src, const double2 *L, double4 *out, int P,
+            cudaStream_t s) {
+  const int nt = tri(P);
+  k_l2p<<<1, WARPS * 32, WARPS * nt * sizeof(double2), s>>>(mini, 1, mini + 1, mini + 2, xr, src, L, out, P);
+  FMM_LAUNCH();
+}
+
 void expansions_set_attributes() {
   double rc[2 * EXAFMM_MAX_P + 4];
   rc[0] = 0;

@@ -169,6 +169,7 @@ struct Handle {
     int P = 0, nres = 0;
   } g_plan;
   bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only
+  Buf op_scratch;  // single-operator entry points (ops.cu): staged arrays
   // tile shapes chosen at run time (exafmm_b200_set_tile; the autotuner)
   int tile_m2l_flush = 0;  // tensor-core M2L groups per FP32 accumulator window (0: default)
   // test hook (exafmm_b200_test_stall_tc): the next tensor-core M2L launch
@@ -211,7 +212,8 @@ void direct_sum(Handle &h, double4 *targets_pq /*x,y,z,q*/, double4 *out, long n
 void periodic_set_attributes();
 void periodic_pass(Handle &h);
 void dipole_correction(Handle &h);
-void ewald(Handle &h, int ksize, double alpha, double sigma, double cutoff, double cycle, double *rec_dev, long nt);
+void ewald(Handle &h, int parts, int ksize, double alpha, double sigma, double cutoff, double cycle, double *rec_dev,
+           long nt);
 
 inline int nterm_of(int P) { return P * (P + 1) / 2; }
 inline unsigned grid_for(long n, int block) { return (unsigned)((n + block - 1) / block); }

@@ -200,49 +200,59 @@ __global__ void k_ewald_dft(const int4 *waves, const double4 *src, long n, doubl
   }
 }
 
-// One block per target: real part over all sources (nearest image per axis,
-// 0 < R < cutoff) and the inverse DFT over all waves, then the self term;
-// p and F accumulate into the target record.
+// Real-space term of one source at the nearest image per axis, inside the
+// cutoff (3dp/ewald.h:82-102 realP2P).
+__device__ __forceinline__ void ewald_real_pair(double tx, double ty, double tz, const double4 &b, double c2,
+                                                double alpha, double a3, double half, double cycle, double &p,
+                                                double &fx, double &fy, double &fz) {
+  double dx = tx - b.x, dy = ty - b.y, dz = tz - b.z;
+  if (dx < -half) dx += cycle;
+  if (dx > half) dx -= cycle;
+  if (dy < -half) dy += cycle;
+  if (dy > half) dy -= cycle;
+  if (dz < -half) dz += cycle;
+  if (dz > half) dz -= cycle;
+  const double R2 = dx * dx + dy * dy + dz * dz;
+  if (0 < R2 && R2 < c2) {
+    const double R2s = R2 * alpha * alpha, Rs = sqrt(R2s);
+    const double invRs = 1 / Rs, invR2s = invRs * invRs, invR3s = invR2s * invRs;
+    const double ec = erfc(Rs);
+    const double dtmp = b.w * (M_2_SQRTPI * exp(-R2s) * invR2s + ec * invR3s) * a3;
+    p += b.w * ec * invRs * alpha;
+    fx -= dx * dtmp;
+    fy -= dy * dtmp;
+    fz -= dz * dtmp;
+  }
+}
+
+// Inverse DFT term of one wave at a target (3dp/ewald.h:36-51 idft).
+__device__ __forceinline__ void ewald_wave_term(double tx, double ty, double tz, const int4 &k, const double2 &a,
+                                                double scale, double &p, double &fx, double &fy, double &fz) {
+  const double th = k.x * tx * scale + k.y * ty * scale + k.z * tz * scale;
+  double s, c;
+  sincos(th, &s, &c);
+  const double dtmp = a.x * s - a.y * c;
+  p += a.x * c + a.y * s;
+  fx -= dtmp * k.x * scale;
+  fy -= dtmp * k.y * scale;
+  fz -= dtmp * k.z * scale;
+}
+
+// One block per target (few targets, many sources): the parts selected by
+// `parts` -- real part over all sources (nearest image per axis, 0 < R <
+// cutoff), the inverse DFT over all waves, the self term; p and F accumulate
+// into the target record.
 __global__ void k_ewald_target(const double4 *src, long n, const int4 *waves, const double2 *amp, int nw,
-                               double scale, double alpha, double cutoff, double cycle, double *rec) {
+                               double scale, double alpha, double cutoff, double cycle, int parts, double *rec) {
   __shared__ double red[4][EB];
   double *r = rec + 8 * (long)blockIdx.x;
   const double tx = r[0], ty = r[1], tz = r[2], tq = r[3];
   double p = 0, fx = 0, fy = 0, fz = 0;
   const double c2 = cutoff * cutoff, a3 = alpha * alpha * alpha, half = cycle / 2;
-  for (long i = threadIdx.x; i < n; i += EB) {
-    const double4 b = src[i];
-    double dx = tx - b.x, dy = ty - b.y, dz = tz - b.z;
-    if (dx < -half) dx += cycle;
-    if (dx > half) dx -= cycle;
-    if (dy < -half) dy += cycle;
-    if (dy > half) dy -= cycle;
-    if (dz < -half) dz += cycle;
-    if (dz > half) dz -= cycle;
-    const double R2 = dx * dx + dy * dy + dz * dz;
-    if (0 < R2 && R2 < c2) {
-      const double R2s = R2 * alpha * alpha, Rs = sqrt(R2s);
-      const double invRs = 1 / Rs, invR2s = invRs * invRs, invR3s = invR2s * invRs;
-      const double ec = erfc(Rs);
-      const double dtmp = b.w * (M_2_SQRTPI * exp(-R2s) * invR2s + ec * invR3s) * a3;
-      p += b.w * ec * invRs * alpha;
-      fx -= dx * dtmp;
-      fy -= dy * dtmp;
-      fz -= dz * dtmp;
-    }
-  }
-  for (int w = threadIdx.x; w < nw; w += EB) {
-    const int4 k = waves[w];
-    const double th = k.x * tx * scale + k.y * ty * scale + k.z * tz * scale;
-    double s, c;
-    sincos(th, &s, &c);
-    const double2 a = amp[w];
-    const double dtmp = a.x * s - a.y * c;
-    p += a.x * c + a.y * s;
-    fx -= dtmp * k.x * scale;
-    fy -= dtmp * k.y * scale;
-    fz -= dtmp * k.z * scale;
-  }
+  if (parts & EXAFMM_EWALD_REAL)
+    for (long i = threadIdx.x; i < n; i += EB) ewald_real_pair(tx, ty, tz, src[i], c2, alpha, a3, half, cycle, p, fx, fy, fz);
+  if (parts & EXAFMM_EWALD_WAVE)
+    for (int w = threadIdx.x; w < nw; w += EB) ewald_wave_term(tx, ty, tz, waves[w], amp[w], scale, p, fx, fy, fz);
   red[0][threadIdx.x] = p;
   red[1][threadIdx.x] = fx;
   red[2][threadIdx.x] = fy;
@@ -254,10 +264,54 @@ __global__ void k_ewald_target(const double4 *src, long n, const int4 *waves, co
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    r[4] += red[0][0] - M_2_SQRTPI * tq * alpha;
+    r[4] += red[0][0] - ((parts & EXAFMM_EWALD_SELF) ? M_2_SQRTPI * tq * alpha : 0.0);
     r[5] += red[1][0];
     r[6] += red[2][0];
     r[7] += red[3][0];
+  }
+}
+
+// One thread per target (many targets): sources and waves pass through
+// shared memory in tiles of EB, every thread sums its own target.
+__global__ void __launch_bounds__(EB) k_ewald_targets(const double4 *src, long n, const int4 *waves,
+                                                      const double2 *amp, int nw, double scale, double alpha,
+                                                      double cutoff, double cycle, int parts, double *rec, long nt) {
+  __shared__ double4 tile[EB];
+  __shared__ int4 wtile[EB];
+  __shared__ double2 atile[EB];
+  const long t = (long)blockIdx.x * EB + threadIdx.x;
+  double tx = 0, ty = 0, tz = 0, tq = 0;
+  if (t < nt) {
+    const double *r = rec + 8 * t;
+    tx = r[0]; ty = r[1]; tz = r[2]; tq = r[3];
+  }
+  double p = 0, fx = 0, fy = 0, fz = 0;
+  const double c2 = cutoff * cutoff, a3 = alpha * alpha * alpha, half = cycle / 2;
+  if (parts & EXAFMM_EWALD_REAL)
+    for (long b = 0; b < n; b += EB) {
+      __syncthreads();
+      if (b + threadIdx.x < n) tile[threadIdx.x] = src[b + threadIdx.x];
+      __syncthreads();
+      const int m = (int)min((long)EB, n - b);
+      for (int k = 0; k < m; k++) ewald_real_pair(tx, ty, tz, tile[k], c2, alpha, a3, half, cycle, p, fx, fy, fz);
+    }
+  if (parts & EXAFMM_EWALD_WAVE)
+    for (int w0 = 0; w0 < nw; w0 += EB) {
+      __syncthreads();
+      if (w0 + (int)threadIdx.x < nw) {
+        wtile[threadIdx.x] = waves[w0 + threadIdx.x];
+        atile[threadIdx.x] = amp[w0 + threadIdx.x];
+      }
+      __syncthreads();
+      const int m = min(EB, nw - w0);
+      for (int k = 0; k < m; k++) ewald_wave_term(tx, ty, tz, wtile[k], atile[k], scale, p, fx, fy, fz);
+    }
+  if (t < nt) {
+    double *r = rec + 8 * t;
+    r[4] += p - ((parts & EXAFMM_EWALD_SELF) ? M_2_SQRTPI * tq * alpha : 0.0);
+    r[5] += fx;
+    r[6] += fy;
+    r[7] += fz;
   }
 }
 
@@ -289,7 +343,8 @@ void dipole_correction(Handle &h) {
   part.release();
 }
 
-void ewald(Handle &h, int ksize, double alpha, double sigma, double cutoff, double cycle, double *rec_dev, long nt) {
+void ewald(Handle &h, int parts, int ksize, double alpha, double sigma, double cutoff, double cycle, double *rec_dev,
+           long nt) {
   // waves of initWaves (3dp/ewald.h:53-80)
   std::vector<int4> w;
   for (int l = 0; l <= ksize; l++) {
@@ -307,11 +362,20 @@ void ewald(Handle &h, int ksize, double alpha, double sigma, double cutoff, doub
   FMM_CUDA(cudaMemcpyAsync(wv.p, w.data(), nw * sizeof(int4), cudaMemcpyHostToDevice, h.stream));
   const double scale = 2 * M_PI / cycle;
   const double coef = 2 / sigma / cycle / cycle / cycle, coef2 = 1 / (4 * alpha * alpha);
-  k_ewald_dft<<<nw, EB, 0, h.stream>>>(wv.as<int4>(), h.src.as<double4>(), h.n, scale, coef, coef2,
-                                       amp.as<double2>());
-  k_ewald_target<<<(unsigned)nt, EB, 0, h.stream>>>(h.src.as<double4>(), h.n, wv.as<int4>(), amp.as<double2>(), nw,
-                                                    scale, alpha, cutoff, cycle, rec_dev);
-  h.launches += 2;
+  if (parts & EXAFMM_EWALD_WAVE) {
+    k_ewald_dft<<<nw, EB, 0, h.stream>>>(wv.as<int4>(), h.src.as<double4>(), h.n, scale, coef, coef2,
+                                         amp.as<double2>());
+    h.launches++;
+  }
+  const long n = (parts & (EXAFMM_EWALD_REAL | EXAFMM_EWALD_WAVE)) ? h.n : 0;
+  // a block per target while the targets cannot fill the GPU as threads
+  if (nt < 148L * 4 * EB)
+    k_ewald_target<<<(unsigned)nt, EB, 0, h.stream>>>(h.src.as<double4>(), n, wv.as<int4>(), amp.as<double2>(), nw,
+                                                      scale, alpha, cutoff, cycle, parts, rec_dev);
+  else
+    k_ewald_targets<<<grid_for(nt, EB), EB, 0, h.stream>>>(h.src.as<double4>(), n, wv.as<int4>(), amp.as<double2>(),
+                                                           nw, scale, alpha, cutoff, cycle, parts, rec_dev, nt);
+  h.launches++;
   FMM_LAUNCH();
   FMM_CUDA(cudaStreamSynchronize(h.stream));
   wv.release();

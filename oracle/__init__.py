@@ -105,9 +105,70 @@ class Port(_Common):
         L.orc_kernel_chain.restype = _d
         L.orc_kernel_chain.argtypes = [_i, _p]
         L.orc_reference_bodies.argtypes = [_l, _l, _i, _d, _p]
+        L.orc_op_p2m.argtypes = [_i, _p, _p, _l, _p]
+        L.orc_op_m2m.argtypes = [_i, _p, _p, _i, _p, _p]
+        L.orc_op_m2l.argtypes = [_i, _p, _p, _p, _p, _p, _d]
+        L.orc_op_l2l.argtypes = [_i, _p, _p, _i, _p, _p]
+        L.orc_op_l2p.argtypes = [_i, _p, _p, _p, _l]
+        L.orc_op_p2p.argtypes = [_p, _l, _p, _l, _p, _d]
+        for f in ("p2m", "m2m", "m2l", "l2l", "l2p", "p2p"):
+            getattr(L, "orc_op_" + f).restype = None
         self._bind_common("orc_")
         self.n = 0
         self.ncells = 0
+
+    # ---- single operators (3d/kernel.h:122-323) on caller data.  cell: X[3],
+    # R; expansions: NTERM complex; bodies: N x 8 Body records.  Each returns
+    # the accumulated output (a new array; the inputs are not modified).
+    @staticmethod
+    def _cplx(a, nt):
+        a = np.zeros(nt, complex) if a is None else np.asarray(a, complex).ravel()
+        return np.ascontiguousarray(np.stack([a.real, a.imag], -1))
+
+    def op_p2m(self, P, cell, bodies, M=None):
+        nt = P * (P + 1) // 2
+        m = self._cplx(M, nt)
+        b = np.ascontiguousarray(bodies, np.float64)
+        self.lib.orc_op_p2m(P, _ptr(np.asarray(cell, np.float64)), _ptr(b), len(b), _ptr(m))
+        return m[:, 0] + 1j * m[:, 1]
+
+    def op_m2m(self, P, parent, children, Mchildren, M=None):
+        nt = P * (P + 1) // 2
+        m = self._cplx(M, nt)
+        ch = np.ascontiguousarray(children, np.float64)
+        mc = self._cplx(Mchildren, nt * len(ch))
+        self.lib.orc_op_m2m(P, _ptr(np.asarray(parent, np.float64)), _ptr(m), len(ch), _ptr(ch), _ptr(mc))
+        return m[:, 0] + 1j * m[:, 1]
+
+    def op_m2l(self, P, target, source, M, L=None, ix=None, cycle=0.0):
+        nt = P * (P + 1) // 2
+        lo = self._cplx(L, nt)
+        mm = self._cplx(M, nt)
+        ixa = None if ix is None else np.ascontiguousarray(ix, np.int32)
+        self.lib.orc_op_m2l(P, _ptr(np.asarray(target, np.float64)), _ptr(lo), _ptr(np.asarray(source, np.float64)),
+                            _ptr(mm), None if ixa is None else _ptr(ixa), cycle)
+        return lo[:, 0] + 1j * lo[:, 1]
+
+    def op_l2l(self, P, parent, L, children, Lchildren=None):
+        nt = P * (P + 1) // 2
+        ch = np.ascontiguousarray(children, np.float64)
+        lc = self._cplx(Lchildren, nt * len(ch))
+        self.lib.orc_op_l2l(P, _ptr(np.asarray(parent, np.float64)), _ptr(self._cplx(L, nt)), len(ch), _ptr(ch),
+                            _ptr(lc))
+        return (lc[:, 0] + 1j * lc[:, 1]).reshape(len(ch), nt)
+
+    def op_l2p(self, P, cell, L, bodies):
+        nt = P * (P + 1) // 2
+        b = np.array(bodies, np.float64, order="C")
+        self.lib.orc_op_l2p(P, _ptr(np.asarray(cell, np.float64)), _ptr(self._cplx(L, nt)), _ptr(b), len(b))
+        return b
+
+    def op_p2p(self, targets, sources, ix=None, cycle=0.0):
+        t = np.array(targets, np.float64, order="C")
+        s = np.ascontiguousarray(sources, np.float64)
+        ixa = None if ix is None else np.ascontiguousarray(ix, np.int32)
+        self.lib.orc_op_p2p(_ptr(t), len(t), _ptr(s), len(s), None if ixa is None else _ptr(ixa), cycle)
+        return t
 
     def reference_bodies(self, n, seed=0, kind=0, cycle=2 * np.pi):
         xq = np.zeros((n, 4))

@@ -747,6 +747,12 @@ static void ewald_neighbor(int ci, int cj, double alpha, double cutoff, double c
  * wavePart), real part :122-127 (realPart, per target leaf), self term
  * :146-150. */
 void orc_ewald(int ksize, double alpha, double sigma, double cutoff, double cycle, double *out) {
+  orc_ewald_parts(7, ksize, alpha, sigma, cutoff, cycle, out);
+}
+
+/* The parts selected by the mask (1 wave, 2 real, 4 self), as the reference
+ * driver calls them one by one (3dp/fmm.cxx:85-93). */
+void orc_ewald_parts(int parts, int ksize, double alpha, double sigma, double cutoff, double cycle, double *out) {
   double *p = calloc(nb_, sizeof(double));
   double (*f)[3] = calloc(nb_, sizeof(*f));
   const double scale = 2 * M_PI / cycle;
@@ -768,6 +774,7 @@ void orc_ewald(int ksize, double alpha, double sigma, double cutoff, double cycl
     }
   }
   double *re = calloc(nw, sizeof(double)), *im = calloc(nw, sizeof(double));
+  if (!(parts & 1)) nw = 0;  /* no wave part */
 #pragma omp parallel for
   for (long w = 0; w < nw; w++) {
     double a = 0, b = 0;
@@ -813,9 +820,11 @@ void orc_ewald(int ksize, double alpha, double sigma, double cutoff, double cycl
   nleaf = 0;
   for (long c = 0; c < nc_; c++)
     if (nchild_[c] == 0) leaves[nleaf++] = (int)c;
+  if (!(parts & 2)) nleaf = 0;  /* no real part */
 #pragma omp parallel for schedule(dynamic)
   for (long k = 0; k < nleaf; k++) ewald_neighbor(leaves[k], 0, alpha, cutoff, cycle, p, f);
-  for (long i = 0; i < nb_; i++) p[i] -= M_2_SQRTPI * bq_[i] * alpha;
+  if (parts & 4)
+    for (long i = 0; i < nb_; i++) p[i] -= M_2_SQRTPI * bq_[i] * alpha;
   for (long b = 0; b < nb_; b++) {
     double *r = out + 8 * b;
     r[0] = bx_[b]; r[1] = by_[b]; r[2] = bz_[b]; r[3] = bq_[b];
@@ -874,6 +883,125 @@ double orc_kernel_chain(int P, double *ferr) {
   free(Y); free(dY); free(Y2);
   if (ferr) *ferr = sqrt(fd / fn);
   return sqrt(pd * pd / (pn * pn));
+}
+
+/* ------------------------------------------------------ single operators */
+
+/* A problem of nbodies bodies (Body records, or none) and ncells cells at
+ * order P, replacing the current one; cell c gets centre/radius cell4[c]. */
+static void op_problem(int P, long nbodies, const double *bodies8, int ncells, const double *cell4) {
+  free_bodies();
+  P_ = P;
+  NTERM_ = P * (P + 1) / 2;
+  CYCLE_ = 0;
+  nb_ = nbodies;
+  long nalloc = nbodies > 0 ? nbodies : 1;
+  bx_ = calloc(nalloc, sizeof(double)); by_ = calloc(nalloc, sizeof(double)); bz_ = calloc(nalloc, sizeof(double));
+  bq_ = calloc(nalloc, sizeof(double)); bp_ = calloc(nalloc, sizeof(double));
+  for (int d = 0; d < 3; d++) bf_[d] = calloc(nalloc, sizeof(double));
+  perm_ = calloc(nalloc, sizeof(long));
+  for (long b = 0; b < nbodies; b++) {
+    const double *r = bodies8 + 8 * b;
+    bx_[b] = r[0]; by_[b] = r[1]; bz_[b] = r[2]; bq_[b] = r[3];
+    bp_[b] = r[4]; bf_[0][b] = r[5]; bf_[1][b] = r[6]; bf_[2][b] = r[7];
+  }
+  nc_ = 0;
+  new_cells(ncells);
+  for (int c = 0; c < ncells; c++) {
+    cx_[c] = cell4[4 * c]; cy_[c] = cell4[4 * c + 1]; cz_[c] = cell4[4 * c + 2]; cr_[c] = cell4[4 * c + 3];
+    nchild_[c] = 0; child_[c] = -1; level_[c] = 0; body_[c] = 0; nbody_[c] = 0;
+  }
+  alloc_expansions();
+}
+
+static void op_bodies_out(double *bodies8, long nb) {
+  for (long b = 0; b < nb; b++) {
+    double *r = bodies8 + 8 * b;
+    r[4] = bp_[b]; r[5] = bf_[0][b]; r[6] = bf_[1][b]; r[7] = bf_[2][b];
+  }
+}
+
+/* P2M(C) (3d/kernel.h:187-202) on one cell: M (NTERM complex) accumulates. */
+void orc_op_p2m(int P, const double *cell4, const double *bodies8, long nb, double *M) {
+  op_problem(P, nb, bodies8, 1, cell4);
+  memcpy(M_, M, NTERM_ * sizeof(cplx));
+  body_[0] = 0; nbody_[0] = (int)nb;
+  cplx *Y = malloc(P * P * sizeof(cplx)), *dY = malloc(P * P * sizeof(cplx));
+  p2m(0, Y, dY);
+  memcpy(M, M_, NTERM_ * sizeof(cplx));
+  free(Y); free(dY);
+}
+
+/* M2M(Ci) (3d/kernel.h:204-231): the children's multipoles into the parent's
+ * M (accumulates). */
+void orc_op_m2m(int P, const double *parent4, double *M, int nchild, const double *child4, const double *Mchild) {
+  op_problem(P, 0, NULL, 1, parent4);
+  const int nt = P * (P + 1) / 2;
+  double (*kx)[3] = malloc((nchild > 0 ? nchild : 1) * sizeof(double[3]));
+  cplx **Mk = malloc((nchild > 0 ? nchild : 1) * sizeof(cplx *));
+  for (int k = 0; k < nchild; k++) {
+    for (int d = 0; d < 3; d++) kx[k][d] = child4[4 * k + d];
+    Mk[k] = (cplx *)(Mchild + 2 * (long)k * nt);
+  }
+  cplx *Y = malloc(P * P * sizeof(cplx)), *dY = malloc(P * P * sizeof(cplx));
+  m2m_into(parent4, (cplx *)M, nchild, (const double(*)[3])kx, Mk, Y, dY);
+  free(Y); free(dY); free(kx); free(Mk);
+}
+
+/* M2L(Ci, Cj) (3d/kernel.h:233-260; 3dp/kernel.h:198-200 with the periodic
+ * shift iX * cycle): the source multipole into the target's L (accumulates). */
+void orc_op_m2l(int P, const double *target4, double *L, const double *source4, const double *M, const int *ix,
+                double cycle) {
+  op_problem(P, 0, NULL, 1, target4);
+  const int ix0[3] = {0, 0, 0};
+  cplx *Y2 = malloc(4 * P * P * sizeof(cplx));
+  m2l_into(target4, source4, (const cplx *)M, (cplx *)L, ix ? ix : ix0, ix ? cycle : 0.0, Y2);
+  free(Y2);
+}
+
+/* L2L(Cj) (3d/kernel.h:262-291): the parent's L into each child's L
+ * (Lchild: nchild x NTERM complex, accumulates). */
+void orc_op_l2l(int P, const double *parent4, const double *L, int nchild, const double *child4, double *Lchild) {
+  double *cells = malloc(4 * (1 + (long)nchild) * sizeof(double));
+  memcpy(cells, parent4, 4 * sizeof(double));
+  memcpy(cells + 4, child4, 4 * (long)nchild * sizeof(double));
+  op_problem(P, 0, NULL, 1 + nchild, cells);
+  free(cells);
+  nchild_[0] = nchild; child_[0] = 1;
+  memcpy(L_, L, NTERM_ * sizeof(cplx));
+  memcpy(L_ + NTERM_, Lchild, (long)nchild * NTERM_ * sizeof(cplx));
+  cplx *Y = malloc(P * P * sizeof(cplx)), *dY = malloc(P * P * sizeof(cplx));
+  l2l(0, Y, dY);
+  memcpy(Lchild, L_ + NTERM_, (long)nchild * NTERM_ * sizeof(cplx));
+  free(Y); free(dY);
+}
+
+/* L2P(C) (3d/kernel.h:293-323): the cell's local expansion at its bodies
+ * (Body records; p and F accumulate). */
+void orc_op_l2p(int P, const double *cell4, const double *L, double *bodies8, long nb) {
+  op_problem(P, nb, bodies8, 1, cell4);
+  memcpy(L_, L, NTERM_ * sizeof(cplx));
+  body_[0] = 0; nbody_[0] = (int)nb;
+  cplx *Y = malloc(P * P * sizeof(cplx)), *dY = malloc(P * P * sizeof(cplx));
+  l2p(0, Y, dY);
+  op_bodies_out(bodies8, nb);
+  free(Y); free(dY);
+}
+
+/* P2P(Ci, Cj) (3d/kernel.h:122-150; 3dp/kernel.h:133 with the periodic shift
+ * iX * cycle): sources onto targets (Body records; p and F accumulate). */
+void orc_op_p2p(double *targets8, long nt, const double *sources8, long ns, const int *ix, double cycle) {
+  double *all = malloc(8 * (nt + ns) * sizeof(double));
+  memcpy(all, targets8, 8 * nt * sizeof(double));
+  memcpy(all + 8 * nt, sources8, 8 * ns * sizeof(double));
+  const double c0[4] = {0, 0, 0, 0};
+  op_problem(1, nt + ns, all, 1, c0);
+  free(all);
+  const int ix0[3] = {0, 0, 0};
+  CYCLE_ = ix ? cycle : 0.0;
+  p2p(0, nt, nt, ns, ix ? ix : ix0);
+  CYCLE_ = 0;
+  op_bodies_out(targets8, nt);
 }
 
 /* --------------------------------------------------------------- bodies */

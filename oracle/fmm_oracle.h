@@ -49,10 +49,26 @@ void orc_dipole_correction(double cycle);
 /* Ewald sum of the current bodies (wave + real + self parts), written as
  * 8 doubles per body in tree order. */
 void orc_ewald(int ksize, double alpha, double sigma, double cutoff, double cycle, double *out8);
+/* ... only the parts in the mask: 1 wave, 2 real, 4 self (orc_ewald = 7). */
+void orc_ewald_parts(int parts, int ksize, double alpha, double sigma, double cutoff, double cycle, double *out8);
 
 /* Operator chain known-answer test (test/test_kernel.h): relative potential
  * error, force error through *ferr. */
 double orc_kernel_chain(int P, double *ferr);
+
+/* Single operators on caller data, the reference's kernel functions one call
+ * at a time (3d/kernel.h:122-323).  Each replaces the oracle's current
+ * problem.  Cells are centre + radius (4 doubles), expansions NTERM complex
+ * values (re, im interleaved), bodies Body records; outputs accumulate, as
+ * the reference's += does.  ix (3 ints, or NULL) and cycle give the 3dp
+ * periodic shift iX * cycle of P2P and M2L (3dp/kernel.h:133,200). */
+void orc_op_p2m(int P, const double *cell4, const double *bodies8, long nb, double *M);
+void orc_op_m2m(int P, const double *parent4, double *M, int nchild, const double *child4, const double *Mchild);
+void orc_op_m2l(int P, const double *target4, double *L, const double *source4, const double *M, const int *ix,
+                double cycle);
+void orc_op_l2l(int P, const double *parent4, const double *L, int nchild, const double *child4, double *Lchild);
+void orc_op_l2p(int P, const double *cell4, const double *L, double *bodies8, long nb);
+void orc_op_p2p(double *targets8, long nt, const double *sources8, long ns, const int *ix, double cycle);
 
 /* n bodies as the reference drivers make them: srand48(seed); per body
  * x,y,z from drand48() and q = drand48()-0.5, then q -= mean.  kind 0 is the

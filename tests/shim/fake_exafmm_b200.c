@@ -8,6 +8,7 @@
  *
  * The oracle keeps one problem in global state; every call that reads it
  * first makes sure it holds this handle's problem. */
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -138,5 +139,95 @@ int exafmm_b200_direct(exafmm_b200 *h, double *targets8, int64_t nt, int where) 
   for (long i = 0; i < h->n; i++) memcpy(src + 8 * i, h->xq + 4 * i, 4 * sizeof(double));
   orc_direct(nt, targets8, h->n, src, h->prm.images, h->prm.cycle);
   free(src);
+  return EXAFMM_OK;
+}
+
+/* Single operators on the oracle's restated operators (host arrays only). */
+/* The shift iX * cycle of a periodic call back to the oracle's (iX, cycle),
+ * with the handle's cycle. */
+static const int *ix_of(const exafmm_b200 *h, const double *shift3, int ix[3], double *cycle) {
+  *cycle = h->prm.cycle;
+  if (!shift3 || !(h->prm.cycle > 0)) return NULL;
+  for (int d = 0; d < 3; d++) ix[d] = (int)lround(shift3[d] / h->prm.cycle);
+  return ix;
+}
+
+int exafmm_b200_p2p(exafmm_b200 *h, double *t8, int64_t nt, const double *s8, int64_t ns, const double *shift3,
+                    int where) {
+  if (where != EXAFMM_HOST) return fail(h, EXAFMM_ERR_ARG, "host arrays only");
+  int ix[3];
+  double cyc = 0;
+  const int *pix = ix_of(h, shift3, ix, &cyc);
+  owner = NULL;
+  orc_op_p2p(t8, nt, s8, ns, pix, cyc);
+  return EXAFMM_OK;
+}
+
+int exafmm_b200_p2m(exafmm_b200 *h, const double *cell4, const double *b8, int64_t nb, double *M, int where) {
+  if (where != EXAFMM_HOST) return fail(h, EXAFMM_ERR_ARG, "host arrays only");
+  owner = NULL;
+  orc_op_p2m(h->prm.P, cell4, b8, nb, M);
+  return EXAFMM_OK;
+}
+
+int exafmm_b200_m2m(exafmm_b200 *h, const double *parent4, double *M, int nchild, const double *child4,
+                    const double *Mchild, int where) {
+  if (where != EXAFMM_HOST) return fail(h, EXAFMM_ERR_ARG, "host arrays only");
+  owner = NULL;
+  orc_op_m2m(h->prm.P, parent4, M, nchild, child4, Mchild);
+  return EXAFMM_OK;
+}
+
+int exafmm_b200_m2l(exafmm_b200 *h, const double *t4, double *L, const double *s4, const double *M,
+                    const double *shift3, int where) {
+  if (where != EXAFMM_HOST) return fail(h, EXAFMM_ERR_ARG, "host arrays only");
+  int ix[3];
+  double cyc = 0;
+  const int *pix = ix_of(h, shift3, ix, &cyc);
+  owner = NULL;
+  orc_op_m2l(h->prm.P, t4, L, s4, M, pix, cyc);
+  return EXAFMM_OK;
+}
+
+int exafmm_b200_l2l(exafmm_b200 *h, const double *parent4, const double *L, int nchild, const double *child4,
+                    double *Lchild, int where) {
+  if (where != EXAFMM_HOST) return fail(h, EXAFMM_ERR_ARG, "host arrays only");
+  owner = NULL;
+  orc_op_l2l(h->prm.P, parent4, L, nchild, child4, Lchild);
+  return EXAFMM_OK;
+}
+
+int exafmm_b200_l2p(exafmm_b200 *h, const double *cell4, const double *L, double *b8, int64_t nb, int where) {
+  if (where != EXAFMM_HOST) return fail(h, EXAFMM_ERR_ARG, "host arrays only");
+  owner = NULL;
+  orc_op_l2p(h->prm.P, cell4, L, b8, nb);
+  return EXAFMM_OK;
+}
+
+/* Ewald parts of the handle's bodies onto targets.  The oracle evaluates its
+ * bodies onto themselves, so the stand-in takes targets that are the
+ * handle's bodies in tree order (the periodic driver's case: the same bodies,
+ * tree-sorted twice); the self term alone takes any targets. */
+int exafmm_b200_ewald_parts(exafmm_b200 *h, int parts, int ksize, double alpha, double sigma, double cutoff,
+                            double *t8, int64_t nt, int where) {
+  if (where != EXAFMM_HOST) return fail(h, EXAFMM_ERR_ARG, "host arrays only");
+  if (parts == EXAFMM_EWALD_SELF) {
+    for (int64_t i = 0; i < nt; i++) t8[8 * i + 4] -= M_2_SQRTPI * t8[8 * i + 3] * alpha;
+    return EXAFMM_OK;
+  }
+  if (!h->tree) return fail(h, EXAFMM_ERR_STATE, "no tree");
+  hold(h, 0);
+  if (nt != h->n) return fail(h, EXAFMM_ERR_ARG, "stand-in: targets must be the handle's bodies");
+  double *out = (double *)calloc(8 * nt, sizeof(double));
+  orc_ewald_parts(parts, ksize, alpha, sigma, cutoff, h->prm.cycle, out);
+  for (int64_t i = 0; i < nt; i++) {
+    for (int d = 0; d < 4; d++)
+      if (out[8 * i + d] != t8[8 * i + d]) {
+        free(out);
+        return fail(h, EXAFMM_ERR_ARG, "stand-in: targets must be the handle's bodies in tree order");
+      }
+    for (int d = 4; d < 8; d++) t8[8 * i + d] += out[8 * i + d];
+  }
+  free(out);
   return EXAFMM_OK;
 }

@@ -51,6 +51,37 @@ def test_test_fmm_through_the_shim_gives_the_known_answers():
     assert e10 == pytest.approx(kat["fmm_p10"], rel=1e-8) and e20 == pytest.approx(kat["fmm_p20"], rel=1e-8)
 
 
+def kernel_errors(text):
+    """(p, F) of the operator chain from 3d/kernel.cxx's two printed lines."""
+    return errors(text)
+
+
+@pytest.mark.parametrize("P", [10, 20, 30])
+def test_kernel_cxx_through_the_shim_prints_the_reference_results(P):
+    """The single operators (P2M, M2M, M2L, L2L, L2P, P2P one call each)
+    through the shim give the reference's known answers."""
+    ref = subprocess.run([binary("kernel_ref"), str(P)], capture_output=True, text=True, timeout=60)
+    shim = subprocess.run([binary("kernel_cpu"), str(P)], capture_output=True, text=True, timeout=60)
+    assert ref.returncode == 0 and shim.returncode == 0, shim.stderr[-2000:]
+    assert kernel_errors(shim.stdout) == kernel_errors(ref.stdout)
+
+
+def test_test_kernel_through_the_shim_gives_the_known_answers(kat):
+    r = run(binary("test_kernel_cpu"))
+    assert r.returncode == 0, r.stderr[-2000:]
+    e = list(map(float, re.search(r"test_kernel (\S+) (\S+) (\S+)", r.stdout).groups()))
+    assert e == pytest.approx([kat["kernel_p10"], kat["kernel_p20"], kat["kernel_p30"]], rel=1e-8)
+
+
+def test_periodic_fmm_cxx_through_the_shim_prints_the_reference_results():
+    """3dp/fmm.cxx (1000 bodies, images = 4, dipole correction, then the Ewald
+    parts wavePart, realPart, selfTerm one by one) through the shim."""
+    ref, shim = run(binary("fmm3dp_ref")), run(binary("fmm3dp_cpu"))
+    assert ref.returncode == 0 and shim.returncode == 0, shim.stderr[-2000:]
+    (p, f), (rp, rf) = errors(shim.stdout), errors(ref.stdout)
+    assert p == pytest.approx(rp, rel=1e-4) and f == pytest.approx(rf, rel=1e-4)
+
+
 def test_drivers_linked_against_the_library_reach_it():
     r = run(binary("fmm_gpu"))
     if r.returncode != 0:  # no GPU here: the library's own error, thrown by the shim
