@@ -392,10 +392,15 @@ def batched_leg(FMM, torch, dev, local_rank, nsys=2048):
 
 def periodic_leg(FMM, torch, dev, local_rank, n):
     """Periodic configuration: N bodies uniform in a cube of side 2 pi
-    (neutralised), P=10, theta=0.4, ncrit=64, 3 image layers, mixed form
-    (root images in FP64); after the dipole correction, checked against the
-    GPU FP64 Ewald sum (ksize=11, alpha=ksize/cycle, cutoff=cycle/2) on 1000
-    sampled bodies, by the reference's measures (energy sum, force L2)."""
+    (neutralised), P=10, theta=0.4, ncrit=64, 3 image layers, both forms
+    (root images in FP64).  After the dipole correction each form is checked
+    by the reference's own measures (3dp/fmm.cxx:96-111) over ALL N bodies:
+    the relative error of the energy sum q.p and the relative L2 error of
+    the forces, against one GPU FP64 Ewald sum of all N bodies (ksize=11,
+    sigma=1/(4 pi), cutoff=cycle/2, alpha=ksize/cycle as the reference's
+    driver sets it, 3dp/fmm.cxx:20-23).  A second Ewald sum with the
+    alpha=10/(2 pi) of the benchmark's configuration shows how far the Ewald
+    check itself moves with alpha."""
     from minimal_b200 import drand48_bodies
 
     cyc = 2 * np.pi
@@ -403,7 +408,8 @@ def periodic_leg(FMM, torch, dev, local_rank, n):
     rec = np.zeros((n, 8))
     rec[:, :4] = xq
     d = torch.from_numpy(rec).to(dev)
-    res = {}
+    res, outs = {}, {}
+    ewald_handle = None
     for prec in ("mixed", "fp64"):
         f = FMM(P=10, ncrit=64, theta=0.4, images=3, cycle=cyc, precision=prec, device=local_rank)
         f.set_bodies_device(d.data_ptr(), n)
@@ -413,18 +419,39 @@ def periodic_leg(FMM, torch, dev, local_rank, n):
             f.evaluate()
             ts.append(f.timings()["total"])
         f.dipole_correction()
-        out = f.bodies()
-        sample = np.arange(0, n, max(1, n // 1000))[:1000]
-        tgt = out[sample].copy()
-        tgt[:, 4:] = 0
-        ew = f.ewald(tgt, ksize=11)
-        o = out[sample]
-        ep = abs((o[:, 4] * o[:, 3]).sum() - (ew[:, 4] * ew[:, 3]).sum()) / abs((ew[:, 4] * ew[:, 3]).sum())
-        ef = float(np.sqrt(((o[:, 5:] - ew[:, 5:]) ** 2).sum() / (ew[:, 5:] ** 2).sum()))
-        res[prec] = {"ms_per_eval": statistics.mean(ts), "evals_per_s": 1e3 / statistics.mean(ts),
-                     "energy_rel_err_vs_ewald": float(ep), "force_rel_l2_vs_ewald": ef}
-        f.close()
-    res["workload"] = f"{n} bodies uniform in a cube of side 2 pi, P=10, theta=0.4, ncrit=64, images=3"
+        outs[prec] = f.bodies()
+        res[prec] = {"ms_per_eval": statistics.mean(ts), "evals_per_s": 1e3 / statistics.mean(ts)}
+        if prec == "fp64":
+            ewald_handle = f
+        else:
+            f.close()
+    assert np.array_equal(outs["mixed"][:, :4], outs["fp64"][:, :4])  # same tree, same body order
+    tgt = outs["fp64"].copy()
+    tgt[:, 4:] = 0
+    ewald = {}
+    for name, alpha in (("alpha_ksize_over_cycle", 11 / cyc), ("alpha_10_over_2pi", 10 / cyc)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ewald[name] = ewald_handle.ewald(tgt, ksize=11, alpha=alpha)
+        ewald[name + "_s"] = time.perf_counter() - t0
+    ewald_handle.close()
+
+    def measures(o, ew):
+        e, e0 = float((o[:, 4] * o[:, 3]).sum()), float((ew[:, 4] * ew[:, 3]).sum())
+        return {"energy_rel_err": abs(e - e0) / abs(e0),
+                "force_rel_l2": float(np.sqrt(((o[:, 5:] - ew[:, 5:]) ** 2).sum() / (ew[:, 5:] ** 2).sum()))}
+
+    ew = ewald["alpha_ksize_over_cycle"]
+    for prec in ("mixed", "fp64"):
+        m = measures(outs[prec], ew)
+        res[prec]["energy_rel_err_vs_ewald"] = m["energy_rel_err"]
+        res[prec]["force_rel_l2_vs_ewald"] = m["force_rel_l2"]
+    res["mixed_over_fp64_speedup"] = res["fp64"]["ms_per_eval"] / res["mixed"]["ms_per_eval"]
+    res["ewald"] = {"targets": n, "alpha": 11 / cyc, "ksize": 11, "cutoff": cyc / 2,
+                    "seconds": ewald["alpha_ksize_over_cycle_s"],
+                    "vs_alpha_10_over_2pi": measures(ewald["alpha_10_over_2pi"], ew)}
+    res["workload"] = (f"{n} bodies uniform in a cube of side 2 pi, P=10, theta=0.4, ncrit=64, images=3; errors "
+                       "over all bodies against the GPU FP64 Ewald sum, as 3dp/fmm.cxx:96-111 measures them")
     return res
 
 

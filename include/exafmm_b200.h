@@ -64,7 +64,21 @@ typedef struct exafmm_params {
   double cycle;    /* period of the periodic box (3dp) */
   int precision;   /* EXAFMM_FP64 or EXAFMM_MIXED */
   int device;      /* CUDA device ordinal */
+  int dim;         /* 3 (or 0): the 3d/3dp variants; 2: the 2d/2dp variants */
 } exafmm_params;
+
+/* The 2D variants (2d/, 2dp/: the log kernel, complex power series of P
+ * terms, quadtree; 2d/kernel.h:12-126) run on the same handle with dim = 2,
+ * FP64 only, P >= 2.  What changes at the boundary: bodies are the 2D Body
+ * record, 6 doubles X[2], q, p, F[2] (2d/exafmm.h:14-19), in set_bodies,
+ * get_bodies, set_charges (N doubles, as in 3D) and direct; get_tree's xr is
+ * x, y, 0, R; expansions are P complex coefficients per cell
+ * (2d/kernel.h:34-45); list image indices are the 2D periodic1D
+ * (ix+1) + 3 (iy+1) (2dp/traverse_lazy.h:27-30; 4 = no shift); with
+ * images > 0 the walk repeats over the 9 in-plane images and the root adds
+ * the far images of 2dp/traverse_eager.h:46-93; direct() sums the
+ * (2r+1)^2 images of 2dp/traverse_eager.h:124-143.  Batches, the mixed form,
+ * the single operators, the dipole correction and Ewald are 3D only. */
 
 typedef struct exafmm_b200 exafmm_b200;
 

@@ -111,7 +111,8 @@ struct Error : std::runtime_error {
 namespace shim {
 
 inline exafmm_params params() {
-  exafmm_params p;
+  exafmm_params p{};
+  p.dim = 3;
   p.P = P;
   p.ncrit = ncrit;
   p.theta = theta;

@@ -55,7 +55,7 @@ class FMMError(RuntimeError):
 class Params(ctypes.Structure):
     _fields_ = [("P", ctypes.c_int), ("ncrit", ctypes.c_int), ("theta", ctypes.c_double),
                 ("images", ctypes.c_int), ("cycle", ctypes.c_double), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("dim", ctypes.c_int)]
 
 
 _lib = None
@@ -124,14 +124,16 @@ def _p(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-def as_records(bodies):
-    """N x 4 (x,y,z,q) or N x 8 Body records -> contiguous N x 8 float64."""
+def as_records(bodies, dim=3):
+    """3D: N x 4 (x,y,z,q) or N x 8 Body records -> contiguous N x 8 float64.
+    2D: N x 3 (x,y,q) or N x 6 Body records (2d/exafmm.h:14-19) -> N x 6."""
     b = np.asarray(bodies, dtype=np.float64)
-    if b.ndim != 2 or b.shape[1] not in (4, 8):
-        raise ValueError("bodies must be N x 4 (x,y,z,q) or N x 8 (X,q,p,F)")
-    if b.shape[1] == 4:
-        r = np.zeros((len(b), 8))
-        r[:, :4] = b
+    short, full = (3, 6) if dim == 2 else (4, 8)
+    if b.ndim != 2 or b.shape[1] not in (short, full):
+        raise ValueError(f"bodies must be N x {short} (X, q) or N x {full} (X, q, p, F)")
+    if b.shape[1] == short:
+        r = np.zeros((len(b), full))
+        r[:, :short] = b
         return r
     return np.ascontiguousarray(b)
 
@@ -139,9 +141,10 @@ def as_records(bodies):
 class FMM:
     """One FMM problem on one GPU (a handle of the C ABI)."""
 
-    def __init__(self, P=10, ncrit=64, theta=0.4, images=0, cycle=0.0, precision="fp64", device=0):
+    def __init__(self, P=10, ncrit=64, theta=0.4, images=0, cycle=0.0, precision="fp64", device=0, dim=3):
         self.lib = load_library()
-        self.params = Params(P, ncrit, theta, images, cycle, MIXED if precision == "mixed" else FP64, device)
+        self.dim = dim
+        self.params = Params(P, ncrit, theta, images, cycle, MIXED if precision == "mixed" else FP64, device, dim)
         h = ctypes.c_void_p()
         rc = self.lib.exafmm_b200_create(ctypes.byref(self.params), ctypes.byref(h))
         if rc != 0:
@@ -172,8 +175,14 @@ class FMM:
             setattr(self.params, k, v)
         self._check(self.lib.exafmm_b200_set_params(self.h, ctypes.byref(self.params)))
 
+    def _rec(self, bodies):
+        return as_records(bodies, self.dim)
+
+    def _len(self):
+        return 6 if self.dim == 2 else 8
+
     def set_bodies(self, bodies):
-        rec = as_records(bodies)
+        rec = self._rec(bodies)
         self.n = len(rec)
         self._check(self.lib.exafmm_b200_set_bodies(self.h, _p(rec), self.n, HOST))
 
@@ -237,7 +246,7 @@ class FMM:
 
     # ---- results
     def bodies(self):
-        out = np.zeros((self.n, 8))
+        out = np.zeros((self.n, self._len()))
         self._check(self.lib.exafmm_b200_get_bodies(self.h, _p(out), HOST))
         return out
 
@@ -272,7 +281,8 @@ class FMM:
         return dict(m2l_off=mo, m2l_src=ms[:na], m2l_img=mi[:na], p2p_off=po, p2p_src=ps[:nb], p2p_img=pi[:nb])
 
     def expansions(self):
-        c, nt = self.num_cells(), self.params.P * (self.params.P + 1) // 2
+        c = self.num_cells()
+        nt = self.params.P if self.dim == 2 else self.params.P * (self.params.P + 1) // 2
         M = np.zeros((c, nt, 2))
         L = np.zeros((c, nt, 2))
         self._check(self.lib.exafmm_b200_get_expansions(self.h, _p(M), _p(L)))
@@ -280,7 +290,7 @@ class FMM:
 
     def direct(self, targets):
         """FP64 direct sum of all loaded bodies onto targets (Body records; p, F accumulate)."""
-        t = as_records(targets).copy()
+        t = self._rec(targets).copy()
         self._check(self.lib.exafmm_b200_direct(self.h, _p(t), len(t), HOST))
         return t
 
@@ -355,6 +365,8 @@ class FMM:
         c = np.asarray(c, np.float64).ravel()
         return np.ascontiguousarray(np.concatenate([c, np.zeros(4 - len(c))]) if len(c) < 4 else c[:4])
 
+    # every array handed to the library is bound to a local first: _p() keeps
+    # only the address, so an inline temporary could be freed before the call
     def p2p(self, targets, sources, shift=None):
         t = np.array(as_records(targets), order="C")
         s = as_records(sources)
@@ -366,7 +378,8 @@ class FMM:
     def p2m(self, cell, bodies, M=None):
         m = self._c2(M, self._nt())
         b = as_records(bodies)
-        self._check(self.lib.exafmm_b200_p2m(self.h, _p(self._cell(cell)), _p(b), len(b), _p(m), HOST))
+        c = self._cell(cell)
+        self._check(self.lib.exafmm_b200_p2m(self.h, _p(c), _p(b), len(b), _p(m), HOST))
         return m[:, 0] + 1j * m[:, 1]
 
     def m2m(self, parent, children, Mchildren, M=None):
@@ -374,29 +387,33 @@ class FMM:
         m = self._c2(M, nt)
         ch = np.ascontiguousarray([self._cell(c) for c in children]).reshape(-1, 4)
         mc = self._c2(Mchildren, nt * len(ch))
-        self._check(self.lib.exafmm_b200_m2m(self.h, _p(self._cell(parent)), _p(m), len(ch), _p(ch), _p(mc), HOST))
+        c = self._cell(parent)
+        self._check(self.lib.exafmm_b200_m2m(self.h, _p(c), _p(m), len(ch), _p(ch), _p(mc), HOST))
         return m[:, 0] + 1j * m[:, 1]
 
     def m2l(self, target, source, M, L=None, shift=None):
         nt = self._nt()
         lo, mm = self._c2(L, nt), self._c2(M, nt)
         sh = None if shift is None else np.ascontiguousarray(shift, np.float64)
-        self._check(self.lib.exafmm_b200_m2l(self.h, _p(self._cell(target)), _p(lo), _p(self._cell(source)), _p(mm),
-                                             None if sh is None else _p(sh), HOST))
+        t, s = self._cell(target), self._cell(source)
+        self._check(self.lib.exafmm_b200_m2l(self.h, _p(t), _p(lo), _p(s), _p(mm), None if sh is None else _p(sh),
+                                             HOST))
         return lo[:, 0] + 1j * lo[:, 1]
 
     def l2l(self, parent, L, children, Lchildren=None):
         nt = self._nt()
         ch = np.ascontiguousarray([self._cell(c) for c in children]).reshape(-1, 4)
         lc = self._c2(Lchildren, nt * len(ch))
-        self._check(self.lib.exafmm_b200_l2l(self.h, _p(self._cell(parent)), _p(self._c2(L, nt)), len(ch), _p(ch),
-                                             _p(lc), HOST))
+        lp = self._c2(L, nt)
+        c = self._cell(parent)
+        self._check(self.lib.exafmm_b200_l2l(self.h, _p(c), _p(lp), len(ch), _p(ch), _p(lc), HOST))
         return (lc[:, 0] + 1j * lc[:, 1]).reshape(len(ch), nt)
 
     def l2p(self, cell, L, bodies):
         b = np.array(as_records(bodies), order="C")
-        self._check(self.lib.exafmm_b200_l2p(self.h, _p(self._cell(cell)), _p(self._c2(L, self._nt())), _p(b),
-                                             len(b), HOST))
+        lc = self._c2(L, self._nt())
+        c = self._cell(cell)
+        self._check(self.lib.exafmm_b200_l2p(self.h, _p(c), _p(lc), _p(b), len(b), HOST))
         return b
 
     TILES = {"m2l_flush": 0}

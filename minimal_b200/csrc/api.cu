@@ -63,13 +63,25 @@ void check_params(const exafmm_params &p) {
   if (p.images < 0 || p.images > 12) throw Error{EXAFMM_ERR_ARG, "images must be in [0, 12]"};
   if (p.images > 0 && !(p.cycle > 0)) throw Error{EXAFMM_ERR_ARG, "cycle must be positive when images > 0"};
   if (p.precision != EXAFMM_FP64 && p.precision != EXAFMM_MIXED) throw Error{EXAFMM_ERR_ARG, "unknown precision"};
+  if (p.dim != 0 && p.dim != 2 && p.dim != 3) throw Error{EXAFMM_ERR_ARG, "dim must be 2 or 3 (0 = 3)"};
+  if (p.dim == 2 && p.precision != EXAFMM_FP64) throw Error{EXAFMM_ERR_ARG, "the 2D variants are FP64 only"};
+  if (p.dim == 2 && p.P < 2) throw Error{EXAFMM_ERR_ARG, "the 2D variants need P >= 2"};
 }
 
-__global__ void k_pack_in(const double *rec, long n, double4 *in, int *bad) {
+bool is2d(const Handle &h) { return h.prm.dim == 2; }
+int rec_len(const Handle &h) { return is2d(h) ? 6 : 8; }  // doubles per Body record
+
+void need_3d(Handle &h, const char *what) {
+  if (is2d(h)) throw Error{EXAFMM_ERR_STATE, std::string(what) + " is for the 3D variants (dim = 3)"};
+}
+
+// Body records (8 doubles in 3D, 6 in 2D: X[dim], q, p, F[dim]) -> x, y, z, q
+// (z = 0 in 2D).
+__global__ void k_pack_in(const double *rec, long n, int len, double4 *in, int *bad) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double *r = rec + 8 * i;
-  const double4 v = make_double4(r[0], r[1], r[2], r[3]);
+  const double *r = rec + len * i;
+  const double4 v = len == 8 ? make_double4(r[0], r[1], r[2], r[3]) : make_double4(r[0], r[1], 0.0, r[2]);
   if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) *bad = 1;
   in[i] = v;
 }
@@ -88,28 +100,42 @@ __global__ void k_set_charges(const double *q, long n, double4 *in, const int *p
   if (src) src[i].w = q[perm[i]];
 }
 
-__global__ void k_unpack_out(const double4 *src, const double4 *out, long n, double *rec) {
+__global__ void k_unpack_out(const double4 *src, const double4 *out, long n, int len, double *rec) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 a = src[i], b = out[i];
-  double *r = rec + 8 * i;
-  r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
-  r[4] = b.x; r[5] = b.y; r[6] = b.z; r[7] = b.w;
+  double *r = rec + len * i;
+  if (len == 8) {
+    r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
+    r[4] = b.x; r[5] = b.y; r[6] = b.z; r[7] = b.w;
+  } else {
+    r[0] = a.x; r[1] = a.y; r[2] = a.w;
+    r[3] = b.x; r[4] = b.y; r[5] = b.z;
+  }
 }
 
-__global__ void k_direct_prep(const double *rec, long n, double4 *xq, double4 *pf) {
+__global__ void k_direct_prep(const double *rec, long n, int len, double4 *xq, double4 *pf) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double *r = rec + 8 * i;
-  xq[i] = make_double4(r[0], r[1], r[2], r[3]);
-  pf[i] = make_double4(r[4], r[5], r[6], r[7]);
+  const double *r = rec + len * i;
+  if (len == 8) {
+    xq[i] = make_double4(r[0], r[1], r[2], r[3]);
+    pf[i] = make_double4(r[4], r[5], r[6], r[7]);
+  } else {
+    xq[i] = make_double4(r[0], r[1], 0.0, r[2]);
+    pf[i] = make_double4(r[3], r[4], r[5], 0.0);
+  }
 }
 
-__global__ void k_direct_back(const double4 *pf, long n, double *rec) {
+__global__ void k_direct_back(const double4 *pf, long n, int len, double *rec) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double *r = rec + 8 * i;
-  r[4] = pf[i].x; r[5] = pf[i].y; r[6] = pf[i].z; r[7] = pf[i].w;
+  double *r = rec + len * i;
+  if (len == 8) {
+    r[4] = pf[i].x; r[5] = pf[i].y; r[6] = pf[i].z; r[7] = pf[i].w;
+  } else {
+    r[3] = pf[i].x; r[4] = pf[i].y; r[5] = pf[i].z;
+  }
 }
 
 // A phase: CUDA events on its stream (the timings), and an NVTX range on
@@ -288,7 +314,7 @@ int exafmm_b200_create(const exafmm_params *params, exafmm_b200 **out) {
     FMM_CUDA(cudaSetDevice(params->device));
     Handle &h = H->h;
     h.prm = *params;
-    h.nterm = nterm_of(params->P);
+    h.nterm = params->dim == 2 ? params->P : nterm_of(params->P);
     int least = 0, greatest = 0;
     FMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     FMM_CUDA(cudaStreamCreateWithPriority(&h.stream, cudaStreamNonBlocking, greatest));
@@ -363,8 +389,11 @@ int exafmm_b200_set_params(exafmm_b200 *H, const exafmm_params *params) {
     if (h.nsys > 1 && params->images != 0)
       throw Error{EXAFMM_ERR_STATE, "batches of systems are free-space only (images = 0)"};
     if (params->device != h.prm.device) throw Error{EXAFMM_ERR_ARG, "a handle stays on its device"};
+    if ((params->dim == 2) != is2d(h) && h.n > 0)
+      throw Error{EXAFMM_ERR_STATE, "dim changes the Body record: load the bodies again after set_params"};
+    if (params->dim == 2 && h.nsys > 1) throw Error{EXAFMM_ERR_STATE, "batches of systems are 3D only"};
     h.prm = *params;
-    h.nterm = nterm_of(params->P);
+    h.nterm = params->dim == 2 ? params->P : nterm_of(params->P);
     h.have_tree = h.have_lists = h.have_up = h.have_horiz = h.have_down = false;
   });
 }
@@ -379,14 +408,15 @@ int exafmm_b200_set_bodies(exafmm_b200 *H, const double *rec, int64_t n, int whe
     h.in.need(n * sizeof(double4));
     h.counters.need(sizeof(DevCounters));
     const double *drec = rec;
+    const int len = rec_len(h);
     if (where == EXAFMM_HOST) {
-      h.stage.need(n * 8 * sizeof(double));
-      FMM_CUDA(cudaMemcpyAsync(h.stage.p, rec, n * 8 * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+      h.stage.need(n * len * sizeof(double));
+      FMM_CUDA(cudaMemcpyAsync(h.stage.p, rec, n * len * sizeof(double), cudaMemcpyHostToDevice, h.stream));
       drec = h.stage.as<double>();
     }
     int *bad = &h.counters.as<DevCounters>()->overflow;
     FMM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), h.stream));
-    k_pack_in<<<grid_for(n, 256), 256, 0, h.stream>>>(drec, n, h.in.as<double4>(), bad);
+    k_pack_in<<<grid_for(n, 256), 256, 0, h.stream>>>(drec, n, len, h.in.as<double4>(), bad);
     h.launches++;
     FMM_LAUNCH();
     int hb = 0;
@@ -416,6 +446,10 @@ int exafmm_b200_set_batch(exafmm_b200 *H, const double *rec, const int64_t *offs
     }
   if (H->h.prm.images != 0) {
     H->h.err = "batches of systems are free-space only (images = 0)";
+    return EXAFMM_ERR_STATE;
+  }
+  if (is2d(H->h)) {
+    H->h.err = "batches of systems are for the 3D variants (dim = 3)";
     return EXAFMM_ERR_STATE;
   }
   const int rc = exafmm_b200_set_bodies(H, rec, offsets[nsys], where);
@@ -536,14 +570,15 @@ int exafmm_b200_get_bodies(exafmm_b200 *H, double *rec, int where) {
     if (!rec) throw Error{EXAFMM_ERR_ARG, "null output"};
     if (!h.have_down) throw Error{EXAFMM_ERR_STATE, "no completed evaluation"};
     double *drec = rec;
+    const int len = rec_len(h);
     if (where == EXAFMM_HOST) {
-      h.stage.need(h.n * 8 * sizeof(double));
+      h.stage.need(h.n * len * sizeof(double));
       drec = h.stage.as<double>();
     }
-    k_unpack_out<<<grid_for(h.n, 256), 256, 0, h.stream>>>(h.src.as<double4>(), h.out.as<double4>(), h.n, drec);
+    k_unpack_out<<<grid_for(h.n, 256), 256, 0, h.stream>>>(h.src.as<double4>(), h.out.as<double4>(), h.n, len, drec);
     FMM_LAUNCH();
     if (where == EXAFMM_HOST)
-      FMM_CUDA(cudaMemcpyAsync(rec, drec, h.n * 8 * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+      FMM_CUDA(cudaMemcpyAsync(rec, drec, h.n * len * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
     FMM_CUDA(cudaStreamSynchronize(h.stream));
   });
 }
@@ -629,19 +664,23 @@ int exafmm_b200_direct(exafmm_b200 *H, double *targets, int64_t nt, int where) {
     need_tree(h);
     need_single(h, "direct()");
     if (!targets || nt <= 0) throw Error{EXAFMM_ERR_ARG, "need targets"};
+    const int len = rec_len(h);
+    const size_t bytes = (size_t)nt * len * sizeof(double);
     Buf rec, xq, pf;
-    rec.need(nt * 64);
+    rec.need(bytes);
     xq.need(nt * sizeof(double4));
     pf.need(nt * sizeof(double4));
-    FMM_CUDA(cudaMemcpyAsync(rec.p, targets, nt * 64, where == EXAFMM_HOST ? cudaMemcpyHostToDevice
-                                                                          : cudaMemcpyDeviceToDevice, h.stream));
-    k_direct_prep<<<grid_for(nt, 256), 256, 0, h.stream>>>(rec.as<double>(), nt, xq.as<double4>(), pf.as<double4>());
+    FMM_CUDA(cudaMemcpyAsync(rec.p, targets, bytes, where == EXAFMM_HOST ? cudaMemcpyHostToDevice
+                                                                        : cudaMemcpyDeviceToDevice, h.stream));
+    k_direct_prep<<<grid_for(nt, 256), 256, 0, h.stream>>>(rec.as<double>(), nt, len, xq.as<double4>(),
+                                                          pf.as<double4>());
     FMM_LAUNCH();
-    direct_sum(h, xq.as<double4>(), pf.as<double4>(), nt);
-    k_direct_back<<<grid_for(nt, 256), 256, 0, h.stream>>>(pf.as<double4>(), nt, rec.as<double>());
+    if (is2d(h)) direct_sum_2d(h, xq.as<double4>(), pf.as<double4>(), nt);
+    else direct_sum(h, xq.as<double4>(), pf.as<double4>(), nt);
+    k_direct_back<<<grid_for(nt, 256), 256, 0, h.stream>>>(pf.as<double4>(), nt, len, rec.as<double>());
     FMM_LAUNCH();
-    FMM_CUDA(cudaMemcpyAsync(targets, rec.p, nt * 64, where == EXAFMM_HOST ? cudaMemcpyDeviceToHost
-                                                                          : cudaMemcpyDeviceToDevice, h.stream));
+    FMM_CUDA(cudaMemcpyAsync(targets, rec.p, bytes, where == EXAFMM_HOST ? cudaMemcpyDeviceToHost
+                                                                        : cudaMemcpyDeviceToDevice, h.stream));
     FMM_CUDA(cudaStreamSynchronize(h.stream));
     rec.release();
     xq.release();
@@ -652,6 +691,7 @@ int exafmm_b200_direct(exafmm_b200 *H, double *targets, int64_t nt, int where) {
 int exafmm_b200_dipole_correction(exafmm_b200 *H) {
   return guarded(H, [&](Handle &h) {
     need_single(h, "dipole_correction()");
+    need_3d(h, "dipole_correction()");
     if (!h.have_down) throw Error{EXAFMM_ERR_STATE, "dipole_correction() needs the results of evaluate()"};
     if (h.prm.images <= 0) throw Error{EXAFMM_ERR_STATE, "dipole_correction() is for periodic systems (images > 0)"};
     dipole_correction(h);
@@ -667,6 +707,7 @@ int exafmm_b200_ewald_parts(exafmm_b200 *H, int parts, int ksize, double alpha, 
                             double *targets, int64_t nt, int where) {
   return guarded(H, [&](Handle &h) {
     if (parts <= 0 || parts > EXAFMM_EWALD_ALL) throw Error{EXAFMM_ERR_ARG, "ewald: parts is a nonzero mask of WAVE, REAL, SELF"};
+    need_3d(h, "ewald()");
     if (parts != EXAFMM_EWALD_SELF) {  // the self term reads only the targets
       need_tree(h);
       need_single(h, "ewald()");
@@ -710,6 +751,7 @@ int exafmm_b200_fma_peak(exafmm_b200 *H, int precision, double *tflops) {
 int exafmm_b200_p2p(exafmm_b200 *H, double *targets8, int64_t nt, const double *sources8, int64_t ns,
                     const double *shift3, int where) {
   return guarded(H, [&](Handle &h) {
+    need_3d(h, "the single operators");
     FMM_CUDA(cudaSetDevice(h.prm.device));
     op_p2p_call(h, targets8, nt, sources8, ns, shift3, where);
   });
@@ -717,6 +759,7 @@ int exafmm_b200_p2p(exafmm_b200 *H, double *targets8, int64_t nt, const double *
 
 int exafmm_b200_p2m(exafmm_b200 *H, const double *cell4, const double *bodies8, int64_t nb, double *M, int where) {
   return guarded(H, [&](Handle &h) {
+    need_3d(h, "the single operators");
     FMM_CUDA(cudaSetDevice(h.prm.device));
     op_p2m_call(h, cell4, bodies8, nb, M, where);
   });
@@ -725,6 +768,7 @@ int exafmm_b200_p2m(exafmm_b200 *H, const double *cell4, const double *bodies8, 
 int exafmm_b200_m2m(exafmm_b200 *H, const double *parent4, double *M, int nchild, const double *children4,
                     const double *Mchildren, int where) {
   return guarded(H, [&](Handle &h) {
+    need_3d(h, "the single operators");
     FMM_CUDA(cudaSetDevice(h.prm.device));
     op_shift_call(h, 0, parent4, Mchildren, nchild, children4, M, where);
   });
@@ -733,6 +777,7 @@ int exafmm_b200_m2m(exafmm_b200 *H, const double *parent4, double *M, int nchild
 int exafmm_b200_m2l(exafmm_b200 *H, const double *target4, double *L, const double *source4, const double *M,
                     const double *shift3, int where) {
   return guarded(H, [&](Handle &h) {
+    need_3d(h, "the single operators");
     FMM_CUDA(cudaSetDevice(h.prm.device));
     op_m2l_call(h, target4, L, source4, M, shift3, where);
   });
@@ -741,6 +786,7 @@ int exafmm_b200_m2l(exafmm_b200 *H, const double *target4, double *L, const doub
 int exafmm_b200_l2l(exafmm_b200 *H, const double *parent4, const double *L, int nchild, const double *children4,
                     double *Lchildren, int where) {
   return guarded(H, [&](Handle &h) {
+    need_3d(h, "the single operators");
     FMM_CUDA(cudaSetDevice(h.prm.device));
     op_shift_call(h, 1, parent4, L, nchild, children4, Lchildren, where);
   });
@@ -748,6 +794,7 @@ int exafmm_b200_l2l(exafmm_b200 *H, const double *parent4, const double *L, int 
 
 int exafmm_b200_l2p(exafmm_b200 *H, const double *cell4, const double *L, double *bodies8, int64_t nb, int where) {
   return guarded(H, [&](Handle &h) {
+    need_3d(h, "the single operators");
     FMM_CUDA(cudaSetDevice(h.prm.device));
     op_l2p_call(h, cell4, L, bodies8, nb, where);
   });

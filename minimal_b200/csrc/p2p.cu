@@ -648,6 +648,7 @@ void p2p_set_attributes() {
 }
 
 void p2p_pass(Handle &h, cudaStream_t s) {
+  if (h.prm.dim == 2) return p2p_pass_2d(h, s);
   h.out.need((size_t)h.n * sizeof(double4));
   const double cyc = h.prm.images ? h.prm.cycle : 0.0;
   const bool cta = h.prm.ncrit <= CT_MAXTGT;  // every leaf fits two targets per thread and the buffer

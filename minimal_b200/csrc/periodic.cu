@@ -322,6 +322,7 @@ void periodic_set_attributes() {
 }
 
 void periodic_pass(Handle &h) {
+  if (h.prm.dim == 2) return periodic_pass_2d(h);
   if (h.prm.images < 2) return;
   const int P = h.prm.P, nt = tri(P), T = periodic_threads(P);
   k_periodic<<<1, PT, ((size_t)T + 3) * nt * sizeof(double2), h.stream>>>(h.M.as<double2>(), h.L.as<double2>(), P,

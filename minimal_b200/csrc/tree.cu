@@ -523,6 +523,9 @@ void build_tree(Handle &h) {
     FMM_LAUNCH();
     break;
   }
+  // 2D bodies lie at z = 0: the octree is the quadtree (the z digit is the
+  // same for every body of a level); its cells go to the plane z = 0
+  if (h.prm.dim == 2) flatten_tree_2d(h);
 }
 
 }  // namespace fmm

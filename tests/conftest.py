@@ -28,3 +28,10 @@ def port():
 @pytest.fixture(scope="session")
 def kat():
     return {k: float(v) for k, v in np.load(os.path.join(GOLDEN, "kat.npz")).items()}
+
+
+@pytest.fixture(scope="session")
+def port2d():
+    import oracle
+
+    return oracle.Fmm2D("port")

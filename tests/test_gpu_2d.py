@@ -1,0 +1,111 @@
+"""The 2D variants on the GPU (dim = 2): minimal ExaFMM's `2d/` and `2dp/`
+(log kernel, complex power series of P terms, quadtree; 2dp: 9-image walk and
+the far images at the root) against the committed fixtures, which the
+reference's own 2d / 2dp headers produced (tests/golden/make_golden.py):
+quadtree and interaction lists (with image indices) bit-exact, bodies in the
+reference's tree order, multipole and local expansions, potentials and
+forces within 1e-12 relative, direct sums within 1e-13 (1e-10 over the
+periodic images)."""
+import os
+
+import numpy as np
+import pytest
+
+from tests.conftest import GOLDEN, golden
+
+pytestmark = pytest.mark.gpu
+
+NAMES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.startswith(("2d_", "2dp_")) and f.endswith(".npz"))
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    nb = float(np.sqrt((np.abs(b) ** 2).sum()))
+    d = float(np.sqrt((np.abs(a - b) ** 2).sum()))
+    return d / nb if nb > 0 else d
+
+
+def run(g):
+    from minimal_b200 import FMM
+
+    f = FMM(P=int(g["P"]), ncrit=int(g["ncrit"]), theta=float(g["theta"]), images=int(g["images"]),
+            cycle=float(g["cycle"]), dim=2)
+    f.set_bodies(g["xyq"])
+    f.evaluate()
+    return f
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_tree_and_lists_bit_exact(name):
+    g = golden(name)
+    f = run(g)
+    t = f.tree()
+    for k in ("nchild", "child", "body", "nbody"):
+        assert np.array_equal(t[k], g[k]), k
+    assert np.array_equal(t["xr"][:, [0, 1, 3]], g["xr"])
+    assert not t["xr"][:, 2].any()  # the plane z = 0
+    lists = f.lists()
+    for k in ("m2l_off", "m2l_src", "m2l_img", "p2p_off", "p2p_src", "p2p_img"):
+        assert np.array_equal(lists[k], g[k]), k
+    out = f.bodies()
+    assert out.shape[1] == 6
+    assert np.array_equal(out[:, :3], g["bodies"][:, :3])  # the reference's tree order
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_expansions_and_results_within_1e12(name):
+    g = golden(name)
+    f = run(g)
+    M, L = f.expansions()
+    assert M.shape == g["M"].shape
+    assert rel(M, g["M"]) < 1e-12 and rel(L, g["L"]) < 1e-12
+    out = f.bodies()
+    assert rel(out[:, 3], g["bodies"][:, 3]) < 1e-12
+    assert rel(out[:, 4:], g["bodies"][:, 4:]) < 1e-12
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_direct_sum(name):
+    g = golden(name)
+    f = run(g)
+    tgt = g["direct_targets"].copy()
+    d = f.direct(tgt)
+    tol = 1e-10 if int(g["images"]) > 0 else 1e-13
+    assert rel(d[:, 3], g["direct"][:, 3]) < tol and rel(d[:, 4:], g["direct"][:, 4:]) < tol
+
+
+def test_larger_2d_system_against_the_oracle(port2d):
+    """100,000 bodies (the reference 2d driver's N, P = 10, ncrit = 8) and a
+    2dp system with images = 3: trees and lists bit-exact, results within
+    1e-12 of the restatement of the reference."""
+    from minimal_b200 import FMM
+    import oracle
+
+    for images, n in ((0, 100000), (3, 20000)):
+        xyq = oracle.reference_bodies_2d(n, 0)
+        cyc = 2 * np.pi
+        f = FMM(P=10, ncrit=8, theta=0.4, images=images, cycle=cyc if images else 0.0, dim=2)
+        f.set_bodies(xyq)
+        f.evaluate()
+        port2d.fmm(xyq, 10, 8, 0.4, images, cyc if images else 0.0)
+        c = port2d.cells()
+        t = f.tree()
+        for k in ("nchild", "child", "body", "nbody"):
+            assert np.array_equal(t[k], c[k]), k
+        lo, lp = f.lists(), port2d.lists()
+        for k in lp:
+            assert np.array_equal(lo[k], lp[k]), k
+        out, ref = f.bodies(), port2d.bodies()
+        assert rel(out[:, 3], ref[:, 3]) < 1e-12 and rel(out[:, 4:], ref[:, 4:]) < 1e-12
+
+
+def test_2d_argument_checks():
+    from minimal_b200 import FMM, FMMError
+
+    with pytest.raises(FMMError):
+        FMM(P=10, precision="mixed", dim=2)  # FP64 only
+    with pytest.raises(FMMError):
+        FMM(P=1, dim=2)  # the M2L needs two terms
+    f = FMM(P=8, dim=2, images=1, cycle=1.0)
+    with pytest.raises(FMMError):
+        f.ewald(np.zeros((1, 8)))  # 3D only
