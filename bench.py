@@ -455,6 +455,53 @@ def periodic_leg(FMM, torch, dev, local_rank, n):
     return res
 
 
+def two_d_leg(FMM, torch, flush, local_rank, n=1 << 20, P=10, ncrit=8, steps=3, warmup=2):
+    """The 2D variant (2d/: log kernel, complex series of P terms,
+    quadtree), FP64: N bodies as the reference's 2d driver makes them
+    (drand48 seed 0, uniform in [-pi, pi]^2, 2d/fmm.cxx:21-35), its P = 10 and
+    ncrit = 8, theta = 0.4.  Device ms per evaluation, error against the GPU
+    FP64 direct sum on 1000 targets, and the reference's own 2d build (lazy
+    traversal, all host cores) on the same bodies, timed here on the host."""
+    import oracle
+
+    xyq = oracle.reference_bodies_2d(n, 0)
+    f = FMM(P=P, ncrit=ncrit, theta=0.4, dim=2, device=local_rank)
+    f.set_bodies(xyq)
+    ts = []
+    for s in range(warmup + steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        f.evaluate()
+        if s >= warmup:
+            ts.append(f.timings()["total"])
+    out = f.bodies()
+    sample = np.arange(0, n, max(1, n // 1000))[:1000]
+    tgt = out[sample].copy()
+    tgt[:, 3:] = 0
+    d = f.direct(tgt)
+    err = {"p": float(np.sqrt(((out[sample, 3] - d[:, 3]) ** 2).sum() / (d[:, 3] ** 2).sum())),
+           "F": float(np.sqrt(((out[sample, 4:] - d[:, 4:]) ** 2).sum() / (d[:, 4:] ** 2).sum()))}
+    f.close()
+    ms = statistics.mean(ts)
+    res = {"workload": f"2d: {n} bodies (drand48 seed 0) in [-pi,pi]^2, P={P}, ncrit={ncrit}, theta=0.4, FP64",
+           "ms_per_eval": ms, "evals_per_s": 1e3 / ms, "error_vs_direct": err}
+    threads = os.cpu_count() or 1
+    try:
+        ref = oracle.Fmm2D("ref")
+        t0 = time.perf_counter()
+        ref.fmm(xyq, P, ncrit, 0.4, 0, 0.0)
+        dt = time.perf_counter() - t0
+        rb = ref.bodies()
+        res["cpu_reference"] = {"value": 1.0 / dt, "unit": "evals/s", "cores": threads, "kind": "reference",
+                                "sample": f"one evaluation of the same {n}-body 2d workload (reference lazy "
+                                          f"traversal, OpenMP {threads} threads), {dt:.2f} s"}
+        res["gpu_over_cpu_reference"] = dt * 1e3 / ms
+        res["rel_l2_p_vs_reference_fmm"] = float(np.sqrt(((out[:, 3] - rb[:, 3]) ** 2).sum() / (rb[:, 3] ** 2).sum()))
+    except Exception as e:  # the reference build missing is reported, not hidden
+        res["cpu_reference"] = {"unavailable": str(e)}
+    return res
+
+
 def run_ours(a, rank, world, local_rank):
     import torch
 
@@ -592,6 +639,10 @@ def run_ours(a, rank, world, local_rank):
             extra["plummer_4M"] = plummer_leg(FMM, flush, torch, local_rank)
         except Exception as e:
             extra["plummer_4M"] = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            extra["two_d"] = two_d_leg(FMM, torch, flush, local_rank)
+        except Exception as e:
+            extra["two_d"] = {"error": f"{type(e).__name__}: {e}"}
 
     cpu = None
     if not a.no_cpu_baseline and world == 1:

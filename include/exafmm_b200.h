@@ -232,7 +232,9 @@ EXAFMM_API int exafmm_b200_set_batch(exafmm_b200 *h, const double *bodies8, cons
  * 3d/fmm.cxx:14).  Times evaluate() on the bodies now loaded (one system or a
  * batch) for each candidate leaf size ncrit (NULL = 32, 48, 64, 96, 128,
  * 192, 256), `repeats` timed runs each after one warm-up, keeps the fastest
- * in the handle's parameters and leaves its results in the handle.  ncrit
+ * in the handle's parameters, then at that leaf size times the near-field
+ * source tiles (EXAFMM_TILE_P2P_STAGE 1024, 1536, 2048) and keeps the
+ * fastest, and leaves the results of the chosen setting in the handle.  ncrit
  * shapes the tree, so results after tuning are those of the chosen ncrit,
  * not of the reference's; the plain drop-in configuration keeps ncrit = 64. */
 EXAFMM_API int exafmm_b200_autotune(exafmm_b200 *h, const int *ncrit_candidates, int ncand, int repeats,
@@ -262,9 +264,13 @@ EXAFMM_API int exafmm_b200_fma_peak(exafmm_b200 *h, int precision, double *tflop
  * (mixed form) accumulated in FP32 in tensor memory before the partial sum is
  * folded into the compensated running sum: fewer groups per window means
  * fewer FP32 additions between folds (a smaller accumulation error) and more
- * fold work.  Values 1-64; 0 restores the default.  get_tile returns the value
- * in effect.  exafmm_b200_autotune() chooses among candidates of it. */
-enum { EXAFMM_TILE_M2L_FLUSH = 0 };
+ * fold work (the default: 2 for P <= 10, 1 above).  Values 1-64; 0 restores
+ * the default.  EXAFMM_TILE_P2P_STAGE: bodies of source leaves the near-field
+ * kernel stages in shared memory per chunk (the source tile), 1024, 1536 or
+ * 2048 (default: 1536 mixed, 1024 FP64); a speed choice: the sums change only
+ * by rounding (the chunks group the sources differently).  get_tile returns the value in effect.  exafmm_b200_autotune()
+ * chooses the source tile after the leaf size. */
+enum { EXAFMM_TILE_M2L_FLUSH = 0, EXAFMM_TILE_P2P_STAGE = 1 };
 EXAFMM_API int exafmm_b200_set_tile(exafmm_b200 *h, int which, int value);
 EXAFMM_API int exafmm_b200_get_tile(exafmm_b200 *h, int which, int *value);
 

@@ -416,7 +416,7 @@ class FMM:
         self._check(self.lib.exafmm_b200_l2p(self.h, _p(c), _p(lc), _p(b), len(b), HOST))
         return b
 
-    TILES = {"m2l_flush": 0}
+    TILES = {"m2l_flush": 0, "p2p_stage": 1}
 
     def set_tile(self, name, value):
         """A run-time tile shape (include/exafmm_b200.h, EXAFMM_TILE_*); 0 = default."""

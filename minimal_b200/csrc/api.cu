@@ -13,6 +13,7 @@
 namespace fmm {
 double fma_peak_tflops(int precision);
 int m2l_flush_interval(const Handle &h);
+int p2p_tile(const Handle &h);
 void ops_set_attributes();
 void op_p2p_call(Handle &h, double *t8, long nt, const double *s8, long ns, const double *shift3, int where);
 void op_p2m_call(Handle &h, const double *cell4, const double *b8, long nb, double *M, int where);
@@ -559,6 +560,23 @@ int exafmm_b200_autotune(exafmm_b200 *H, const int *candidates, int ncand, int r
     }
     h.prm.ncrit = best;
     h.key_levels = 0;
+    // then the near-field source tile at that leaf size (a speed choice:
+    // the sums change only by rounding)
+    if (best <= 256) {
+      const int saved = h.tile_p2p_stage;
+      int best_tile = saved;
+      for (int tile : {1024, 1536, 2048}) {
+        h.tile_p2p_stage = tile;
+        run();
+        double t = run();
+        for (int r = 1; r < repeats; r++) t = std::min(t, run());
+        if (t < tbest) {
+          tbest = t;
+          best_tile = tile;
+        }
+      }
+      h.tile_p2p_stage = best_tile;
+    }
     run();  // leave the results of the chosen setting
     if (best_ncrit) *best_ncrit = best;
     if (best_ms) *best_ms = tbest;
@@ -802,17 +820,25 @@ int exafmm_b200_l2p(exafmm_b200 *H, const double *cell4, const double *L, double
 
 int exafmm_b200_set_tile(exafmm_b200 *H, int which, int value) {
   return guarded(H, [&](Handle &h) {
-    if (which != EXAFMM_TILE_M2L_FLUSH) throw Error{EXAFMM_ERR_ARG, "set_tile: unknown tile parameter"};
-    if (value < 0 || value > 64) throw Error{EXAFMM_ERR_ARG, "set_tile: M2L flush interval in [1, 64] (0: default)"};
-    h.tile_m2l_flush = value;
+    if (which == EXAFMM_TILE_M2L_FLUSH) {
+      if (value < 0 || value > 64) throw Error{EXAFMM_ERR_ARG, "set_tile: M2L flush interval in [1, 64] (0: default)"};
+      h.tile_m2l_flush = value;
+    } else if (which == EXAFMM_TILE_P2P_STAGE) {
+      if (value != 0 && value != 1024 && value != 1536 && value != 2048)
+        throw Error{EXAFMM_ERR_ARG, "set_tile: near-field source tile 1024, 1536 or 2048 (0: default)"};
+      h.tile_p2p_stage = value;
+    } else {
+      throw Error{EXAFMM_ERR_ARG, "set_tile: unknown tile parameter"};
+    }
   });
 }
 
 int exafmm_b200_get_tile(exafmm_b200 *H, int which, int *value) {
   return guarded(H, [&](Handle &h) {
     if (!value) throw Error{EXAFMM_ERR_ARG, "null output"};
-    if (which != EXAFMM_TILE_M2L_FLUSH) throw Error{EXAFMM_ERR_ARG, "get_tile: unknown tile parameter"};
-    *value = m2l_flush_interval(h);
+    if (which == EXAFMM_TILE_M2L_FLUSH) *value = m2l_flush_interval(h);
+    else if (which == EXAFMM_TILE_P2P_STAGE) *value = p2p_tile(h);
+    else throw Error{EXAFMM_ERR_ARG, "get_tile: unknown tile parameter"};
   });
 }
 

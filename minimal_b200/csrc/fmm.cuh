@@ -158,6 +158,8 @@ struct Handle {
   // op_layout (0: FP64 row blocks, 1: tensor-core FP16 images)
   std::unordered_map<int, int> op_slot;
   int op_P = -1, op_layout = -1;
+  double op_cycle = 0, op_R0 = 0;  // image-key operators: the geometry they were built for
+  int op_depth = -1;
   std::vector<int> op_host_keys, op_host_slots, op_host_new_keys, op_host_new_slots;
   int *keys_host = nullptr;  // pinned: the group keys read with the counts
   int g_ntiles = 0, g_ngroups = 0, g_nseg = 0;
@@ -172,6 +174,7 @@ struct Handle {
   Buf op_scratch;  // single-operator entry points (ops.cu): staged arrays
   // tile shapes chosen at run time (exafmm_b200_set_tile; the autotuner)
   int tile_m2l_flush = 0;  // tensor-core M2L groups per FP32 accumulator window (0: default)
+  int tile_p2p_stage = 0;  // near-field source tile: bodies staged per chunk (0: default)
   // test hook (exafmm_b200_test_stall_tc): the next tensor-core M2L launch
   // waits this long on a barrier nothing arrives at, then times out
   long tc_stall_ns = 0;

@@ -41,7 +41,8 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
                                             int2 *fout, unsigned long long *nout, unsigned long long *nnext,
                                             u64 fcap, int2 *m2l, unsigned long long *nm2l, u64 mcap, int2 *p2p,
                                             unsigned long long *np2p, u64 pcap, double theta, double cycle,
-                                            int *overflow, int *m2l_key, int *occ, int *gflag, int *nres) {
+                                            int depth, int *overflow, int *m2l_key, int *occ, int *gflag,
+                                            int *nres) {
   constexpr int NW = TB / 32;
   __shared__ int s_tot[NW], s_totk[NW];    // every warp's packed list counts and frontier count
   __shared__ unsigned long long s_base[3];  // the block's M2L, P2P and frontier ranges
@@ -81,6 +82,7 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
         // the group key of the grouped M2L (radii are R0 / 2^level exactly,
         // so their exponents give the level difference)
         if (img == 13) key = m2l_group_key(a, b, ilogb(b.w) - ilogb(a.w));
+        else key = m2l_image_key(a, b, ilogb(b.w) - ilogb(a.w), img, cv.xr[0].w, cycle, depth);
         if (key >= 0) m2l_mark_key(key, i, occ, gflag);
         else res++;
       } else if (ci == 0 && cj == 0) {
@@ -298,7 +300,8 @@ void build_lists(Handle &h) {
   h.m2l_cap = std::max<size_t>(h.m2l_cap, (size_t)C * 200 + 1024);
   h.p2p_cap = std::max<size_t>(h.p2p_cap, (size_t)h.nleaves * 90 + 1024);
   const int images = h.prm.images;
-  h.g_occ.need((size_t)KEY_SPACE * sizeof(int) * 2 + 64);  // key occupancy, then its scan
+  const long ks = key_space(images, h.depth);
+  h.g_occ.need((size_t)ks * sizeof(int) * 2 + 64);  // key occupancy, then its scan
   h.g_cnt.need((size_t)C * sizeof(int) * 2 + 64);           // targets with grouped entries, then tile slots
   int *occ = h.g_occ.as<int>(), *gflag = h.g_cnt.as<int>();
   for (int attempt = 0;; attempt++) {
@@ -311,7 +314,7 @@ void build_lists(Handle &h) {
     FMM_CUDA(cudaMemsetAsync(&ctr->walk_resid, 0, sizeof(int), s));
     // group keys of the M2L entries, and the keys and targets that occur
     h.m2l_key.need(h.m2l_cap * sizeof(int));
-    FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
+    FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)ks * sizeof(int), s));
     FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
     k_seed<<<grid_for(std::max(h.nsys, 32), 256), 256, 0, s>>>(h.frontier[0].as<int2>(), &ctr->frontier[0], images,
                                                                 h.nsys, h.prm.dim == 2 ? 2 : 3);
@@ -326,7 +329,7 @@ void build_lists(Handle &h) {
       k_walk<<<148 * WALK_BLOCKS_PER_SM, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[st % 3], h.frontier[b].as<int2>(),
                                     &ctr->frontier[(st + 1) % 3], &ctr->frontier[(st + 2) % 3], h.frontier_cap,
                                     h.m2l_raw.as<int2>(), &ctr->n_m2l, h.m2l_cap, h.p2p_raw.as<int2>(), &ctr->n_p2p,
-                                    h.p2p_cap, h.prm.theta, images ? h.prm.cycle : 0.0, &ctr->list_overflow,
+                                    h.p2p_cap, h.prm.theta, images ? h.prm.cycle : 0.0, h.depth, &ctr->list_overflow,
                                     h.m2l_key.as<int>(), occ, gflag, &ctr->walk_resid);
       h.launches++;
       FMM_LAUNCH();

@@ -71,13 +71,14 @@ constexpr int OP_KEYS_HOST = 8192;
 // marks the keys that occur and the targets that have grouped entries.  (The
 // walk does the same for its raw entries.)
 __global__ void k_gkeys(long n, const int2 *pairs, const double4 *xr, const int *level, int *ekey, int *occ,
-                        int *gflag, int *nres) {
+                        int *gflag, int *nres, double cycle, int depth) {
   const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
   int key = -1;
   if (e < n) {
     const int2 pr = pairs[e];
     const int t = pr.x & (int)IDX_MASK, img = (int)((u32)pr.x >> IMG_SHIFT), s = pr.y;
     if (img == 13) key = m2l_group_key(xr[t], xr[s], level[t] - level[s]);
+    else key = m2l_image_key(xr[t], xr[s], level[t] - level[s], img, xr[0].w, cycle, depth);
     if (key >= 0) m2l_mark_key(key, t, occ, gflag);
     ekey[e] = key;
   }
@@ -95,9 +96,9 @@ __global__ void k_csr_pairs(int ncells, const int *off, const u32 *ent, int2 *pa
   }
 }
 
-__global__ void k_key_of_gid(const int *occ, const int *gidx, int *key_of) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < KEY_SPACE && occ[k]) key_of[gidx[k]] = k;
+__global__ void k_key_of_gid(long nkeys, const int *occ, const int *gidx, int *key_of) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nkeys && occ[k]) key_of[gidx[k]] = (int)k;
 }
 
 struct PlanDev {
@@ -105,13 +106,22 @@ struct PlanDev {
   const int *woff, *jmin, *pieces, *prank;
 };
 
-// Irregular harmonics of the group's integer offset into shared memory
-// (threads m < P build column m); returns the level difference.
-__device__ int group_harmonics(int key, int P, double2 *Zsh) {
-  const int dl = (key >> 18) - KEY_DL;
-  const int vx = ((key >> 12) & 63) - KEY_V, vy = ((key >> 6) & 63) - KEY_V, vz = (key & 63) - KEY_V;
+// Geometry an operator key needs: the root radius and the period (image
+// keys), the tree depth (image key slots).
+struct KeyGeom {
+  const double4 *xr;  // xr[0].w: root radius
+  double cycle;
+  int depth;
+};
+
+// Irregular harmonics of the group's offset (an integer vector, or for an
+// image key its exact fractional offset) into shared memory (threads m < P
+// build column m); returns the level difference.
+__device__ int group_harmonics(int key, int P, double2 *Zsh, KeyGeom kg) {
+  double vx, vy, vz;
+  const int dl = m2l_key_offset(key, key < KEY_SPACE ? 1.0 : kg.xr[0].w, kg.cycle, kg.depth, vx, vy, vz);
   if (threadIdx.x < P) {
-    const Sph sg = sph_of((double)vx, (double)vy, (double)vz);
+    const Sph sg = sph_of(vx, vy, vz);
     const int m = threadIdx.x;
     irregular_column(m, P, sg.r, sg, [&](int n, double2 z) { Zsh[tri(n) + m] = z; });
   }
@@ -154,9 +164,9 @@ __device__ double op_value(int row, int col, int P, int NT, int dl, const double
 }
 
 // One CTA per group: the realified, scaled operator in row-block layout.
-__global__ void k_gops(const int *keys, const int *slots, PlanDev pd, double *ops) {
+__global__ void k_gops(const int *keys, const int *slots, PlanDev pd, double *ops, KeyGeom kg) {
   extern __shared__ double2 Zsh[];  // NT irregular harmonics of v
-  const int dl = group_harmonics(keys[blockIdx.x], pd.P, Zsh);
+  const int dl = group_harmonics(keys[blockIdx.x], pd.P, Zsh, kg);
   double *W = ops + (size_t)slots[blockIdx.x] * pd.wsize;
   for (int i = threadIdx.x; i < pd.wsize; i += blockDim.x) {
     int rb = 0;
@@ -202,10 +212,10 @@ TcPlan make_tc_plan(int P, int KP) {
 
 // One CTA per group: the operator split into FP16 hi + lo parts, written as
 // the byte image the MMA reads from shared memory (hi image, then lo image).
-__global__ void k_gops16(const int *keys, const int *slots, int P, TcPlan pl, __half *ops16) {
+__global__ void k_gops16(const int *keys, const int *slots, int P, TcPlan pl, __half *ops16, KeyGeom kg) {
   extern __shared__ double2 Zsh[];
   const int NT = tri(P);
-  const int dl = group_harmonics(keys[blockIdx.x], P, Zsh);
+  const int dl = group_harmonics(keys[blockIdx.x], P, Zsh, kg);
   const int nh = pl.bimg / 2;  // halves per image
   __half *Wh = ops16 + (size_t)slots[blockIdx.x] * 2 * nh, *Wl = Wh + nh;
   for (int e = threadIdx.x; e < nh; e += blockDim.x) {
@@ -931,7 +941,9 @@ void m2l_grouped_pass(Handle &h) {
   // reads) with their keys computed here
   const int2 *pairs = h.m2l_raw.as<int2>();
   const int *ekey = h.m2l_key.as<int>();
-  int *occ = h.g_occ.as<int>(), *gidx = occ + KEY_SPACE;  // sized by build_lists
+  const long ks = key_space(h.prm.images, h.depth);
+  const double cyc = h.prm.images ? h.prm.cycle : 0.0;
+  int *occ = h.g_occ.as<int>(), *gidx = occ + ks;  // sized by build_lists
   int *gflag = h.g_cnt.as<int>(), *tslot = gflag + C;
   DevCounters *ctr = h.counters.as<DevCounters>();
   int *counts = ctr->gcounts;
@@ -942,19 +954,19 @@ void m2l_grouped_pass(Handle &h) {
                                                           h.g_pairs.as<int2>());
     pairs = h.g_pairs.as<int2>();
     h.g_ekey.need(nent * sizeof(int));
-    FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)KEY_SPACE * sizeof(int), s));
+    FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)ks * sizeof(int), s));
     FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
     k_gkeys<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.c_xr.as<double4>(), h.c_level.as<int>(),
-                                              h.g_ekey.as<int>(), occ, gflag, &counts[0]);
+                                              h.g_ekey.as<int>(), occ, gflag, &counts[0], cyc, h.depth);
     ekey = h.g_ekey.as<int>();
     h.launches += 2;
   }
   // dense group ids, the key of each, the flagged targets in tile order;
   // then one read of the counts and of the keys (for the operator cache)
-  scan_exclusive_int(h, occ, gidx, KEY_SPACE, &counts[2]);
-  const long keys_cap = std::max<long>(OP_KEYS_HOST, std::min<long>(KEY_SPACE, nent));
+  scan_exclusive_int(h, occ, gidx, ks, &counts[2]);
+  const long keys_cap = std::max<long>(OP_KEYS_HOST, std::min<long>(ks, nent));
   h.g_keyof.need((size_t)keys_cap * sizeof(int));
-  k_key_of_gid<<<grid_for(KEY_SPACE, TB), TB, 0, s>>>(occ, gidx, h.g_keyof.as<int>());
+  k_key_of_gid<<<grid_for(ks, TB), TB, 0, s>>>(ks, occ, gidx, h.g_keyof.as<int>());
   h.g_tk.need((size_t)C * 2 * (sizeof(u64) + sizeof(u32)) + 64);
   u64 *tk = h.g_tk.as<u64>(), *tk2 = tk + C;
   u32 *tv = (u32 *)(tk2 + C), *tv2 = tv + C;
@@ -963,6 +975,8 @@ void m2l_grouped_pass(Handle &h) {
   if (!h.keys_host) FMM_CUDA(cudaMallocHost((void **)&h.keys_host, OP_KEYS_HOST * sizeof(int)));
   FMM_CUDA(cudaMemcpyAsync(&h.hc, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
   FMM_CUDA(cudaMemcpyAsync(h.keys_host, h.g_keyof.p, OP_KEYS_HOST * sizeof(int), cudaMemcpyDeviceToHost, s));
+  double4 root{};
+  FMM_CUDA(cudaMemcpyAsync(&root, h.c_xr.p, sizeof(double4), cudaMemcpyDeviceToHost, s));
   FMM_CUDA(cudaStreamSynchronize(s));
   const int nres = h.m2l_ordered ? h.hc.gcounts[0] : h.hc.walk_resid;
   const int nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
@@ -977,10 +991,17 @@ void m2l_grouped_pass(Handle &h) {
     // operators: cached per handle by group key (they depend only on the key
     // and P); only keys not seen before are built
     const int layout = tcore ? 1 : 0;
-    if (h.op_P != P || h.op_layout != layout) {
+    // image keys also depend on the period, the root radius and the depth
+    const bool img_geom_changed = h.prm.images > 0 && (h.op_cycle != cyc || h.op_R0 != root.w || h.op_depth != h.depth);
+    if (h.op_P != P || h.op_layout != layout || img_geom_changed) {
       h.op_slot.clear();
       h.op_P = P;
       h.op_layout = layout;
+    }
+    if (h.prm.images > 0) {
+      h.op_cycle = cyc;
+      h.op_R0 = root.w;
+      h.op_depth = h.depth;
     }
     const size_t op_bytes = tcore ? (size_t)2 * tp.bimg : (size_t)gp.wsize * sizeof(double);
     std::vector<int> &key_of = h.op_host_keys;
@@ -1023,12 +1044,13 @@ void m2l_grouped_pass(Handle &h) {
       FMM_CUDA(cudaMemcpyAsync(d_new_keys, new_keys.data(), new_keys.size() * sizeof(int), cudaMemcpyHostToDevice, s));
       FMM_CUDA(cudaMemcpyAsync(d_new_slots, new_slots.data(), new_slots.size() * sizeof(int), cudaMemcpyHostToDevice,
                                s));
+      const KeyGeom kg{h.c_xr.as<double4>(), cyc, h.depth};
       if (tcore)
         k_gops16<<<(int)new_keys.size(), 256, NT * sizeof(double2), s>>>(d_new_keys, d_new_slots, P, tp,
-                                                                          h.g_ops.as<__half>());
+                                                                          h.g_ops.as<__half>(), kg);
       else
         k_gops<<<(int)new_keys.size(), 128, NT * sizeof(double2), s>>>(d_new_keys, d_new_slots, pd,
-                                                                        h.g_ops.as<double>());
+                                                                        h.g_ops.as<double>(), kg);
       h.launches++;
     }
     // tiles of targets

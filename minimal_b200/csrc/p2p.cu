@@ -324,8 +324,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_f32(const int *leaves, int n
 // the zero-distance check; every group takes its share of both parts, so the
 // warps stay converged.  FP64 form: list order, every pair checked.
 constexpr int CT = 128;           // threads per CTA
-// bodies staged at once: FP32 1536 (7 CTAs per SM, register-bound), FP64
-// 1024 (5 CTAs per SM); tuned on B200 at 1M bodies
+// bodies staged at once (the source tile): a template parameter, chosen at
+// run time among 1024, 1536 and 2048 (exafmm_b200_set_tile / the
+// autotuner); the defaults, FP32 1536 (7 CTAs per SM, register-bound) and
+// FP64 1024 (5 CTAs per SM), were tuned on B200 at 1M uniform bodies
 template <bool F32>
 constexpr int ct_cap() { return F32 ? 1536 : 1024; }
 constexpr int CT_MAXTGT = 256;    // target-leaf bodies: two per thread
@@ -348,14 +350,14 @@ struct NearBody<true> {
   typedef float R;
 };
 
-template <bool F32>
+template <bool F32, int CAP>
 __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, const int *begin, const int *count,
                                                 const int *off, const u32 *ent, const double4 *xr,
                                                 const typename NearBody<F32>::T *bodies, double4 *out,
                                                 double cycle) {
   typedef typename NearBody<F32>::T BT;
   typedef typename NearBody<F32>::R RT;
-  constexpr int CAP = ct_cap<F32>(), CT_UNROLL = ct_unroll<F32>();
+  constexpr int CT_UNROLL = ct_unroll<F32>();
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char stage_raw[];  // CAP bodies
   BT *stage = (BT *)stage_raw;
@@ -640,11 +642,33 @@ void make_srcf(Handle &h) {
   h.srcf_ready = true;
 }
 
+// The near-field CTA kernel with source tile `cap` (1024, 1536 or 2048).
+template <bool F32, class... A>
+void launch_p2p_cta(int cap, int nleaves, cudaStream_t s, A... args) {
+  typedef typename NearBody<F32>::T BT;
+  switch (cap) {
+    case 1024: k_p2p_cta<F32, 1024><<<nleaves, CT, 1024 * sizeof(BT), s>>>(args...); break;
+    case 2048: k_p2p_cta<F32, 2048><<<nleaves, CT, 2048 * sizeof(BT), s>>>(args...); break;
+    default: k_p2p_cta<F32, 1536><<<nleaves, CT, 1536 * sizeof(BT), s>>>(args...);
+  }
+}
+
+template <bool F32>
+void set_p2p_attributes() {
+  typedef typename NearBody<F32>::T BT;
+  cudaFuncSetAttribute(k_p2p_cta<F32, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1024 * (int)sizeof(BT));
+  cudaFuncSetAttribute(k_p2p_cta<F32, 1536>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1536 * (int)sizeof(BT));
+  cudaFuncSetAttribute(k_p2p_cta<F32, 2048>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2048 * (int)sizeof(BT));
+}
+
 void p2p_set_attributes() {
-  cudaFuncSetAttribute(k_p2p_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       ct_cap<false>() * (int)sizeof(double4));
-  cudaFuncSetAttribute(k_p2p_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       ct_cap<true>() * (int)sizeof(float4));
+  set_p2p_attributes<false>();
+  set_p2p_attributes<true>();
+}
+
+int p2p_tile(const Handle &h) {
+  if (h.tile_p2p_stage > 0) return h.tile_p2p_stage;
+  return h.prm.precision == EXAFMM_MIXED ? ct_cap<true>() : ct_cap<false>();
 }
 
 void p2p_pass(Handle &h, cudaStream_t s) {
@@ -656,9 +680,9 @@ void p2p_pass(Handle &h, cudaStream_t s) {
     if (s != h.stream && !h.srcf_ready) throw Error{EXAFMM_ERR_STATE, "near field on a side stream before its sources"};
     make_srcf(h);
     if (cta)
-      k_p2p_cta<true><<<h.nleaves, CT, ct_cap<true>() * sizeof(float4), s>>>(
-          h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
-          h.c_xr.as<double4>(), h.srcf.as<float4>(), h.out.as<double4>(), cyc);
+      launch_p2p_cta<true>(p2p_tile(h), h.nleaves, s, h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(),
+                           h.p2p_off.as<int>(), h.p2p_ent.as<u32>(), h.c_xr.as<double4>(), h.srcf.as<float4>(),
+                           h.out.as<double4>(), cyc);
     else
       k_p2p_f32<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, s>>>(
           h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
@@ -668,9 +692,9 @@ void p2p_pass(Handle &h, cudaStream_t s) {
     return;
   }
   if (cta)
-    k_p2p_cta<false><<<h.nleaves, CT, ct_cap<false>() * sizeof(double4), s>>>(
-        h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(), h.p2p_ent.as<u32>(),
-        h.c_xr.as<double4>(), h.src.as<double4>(), h.out.as<double4>(), cyc);
+    launch_p2p_cta<false>(p2p_tile(h), h.nleaves, s, h.leaves.as<int>(), h.c_begin.as<int>(), h.c_count.as<int>(),
+                          h.p2p_off.as<int>(), h.p2p_ent.as<u32>(), h.c_xr.as<double4>(), h.src.as<double4>(),
+                          h.out.as<double4>(), cyc);
   else
     k_p2p<<<grid_for(h.nleaves, WARPS), WARPS * 32, 0, s>>>(
         h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.p2p_off.as<int>(),
