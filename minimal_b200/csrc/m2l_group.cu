@@ -56,9 +56,11 @@ constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
 // accumulation truncates toward zero, so with same-signed contributions (all
 // charges positive) its error is a bias that grows with the MMAs per window:
 // measured on 200,000 Plummer bodies at P = 12, the local expansions' mean
-// relative error was -1.6e-6 over 16 groups and -2.9e-7 over one.  The default
-// keeps a window at one or two groups (P > 10: one); a wider window, set with
-// exafmm_b200_set_tile, trades that accuracy for fewer folds.
+// relative error was -1.6e-6 over 16 groups, -4.1e-7 over two and -2.9e-7
+// over one (potential error 2.7x, 1.22x and 1.15x FP64's).  The default keeps
+// a window at two groups for P <= 10 and one above; a wider window, set with
+// exafmm_b200_set_tile, trades that accuracy for fewer folds (at 1M uniform
+// bodies, P = 10: 3.39 ms per evaluation with 16 groups, 3.45 with 2).
 int default_flush(int P) { return P > 10 ? 1 : 2; }
 // Limit of every wait of the tensor-core kernel (the drain of copies and MMAs
 // already in flight gets twice as long): a wait that runs out flags
@@ -744,24 +746,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         const uint64_t lo_a = abytes >> 4, lo_b = bimg >> 4;  // descriptor start fields count 16 bytes
         const bool fresh = k % flush_every == 0;
         const uint32_t acc = tmem + (uint32_t)a * half_cols;
-        // The tensor core truncates each accumulation toward zero, relative
-        // to the accumulator's magnitude: per group the small hi*lo and lo*hi
-        // products go first (while a fresh accumulator is still small), then
-        // the hi*hi products, so fewer truncations happen at full size.
+        // per K step: hi*hi, then hi*lo with the same A, then lo*hi (issuing
+        // the small products first lowered the truncation bias by a third
+        // but cost 15% of the M2L time: consecutive MMAs on one A are faster)
 #pragma unroll
         for (int b = 0; b < 4; b++) {
           if (b >= pl.nb) break;
-          const uint32_t d = acc + 64u * (uint32_t)b;
           for (int ks = 0; ks < ksteps[b]; ks++) {
             const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
             const uint64_t bo = ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * rows[b] * 128 + (uint64_t)(ks & 3) * 32) >> 4;
-            tc::mma_f16(d, dA + ao, dB + lo_b + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
+            const uint32_t d = acc + 64u * (uint32_t)b;
+            tc::mma_f16(d, dA + ao, dB + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
+            tc::mma_f16(d, dA + ao, dB + lo_b + bo, idesc[b], 1u);
             tc::mma_f16(d, dA + lo_a + ao, dB + bo, idesc[b], 1u);
-          }
-          for (int ks = 0; ks < ksteps[b]; ks++) {
-            const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
-            const uint64_t bo = ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * rows[b] * 128 + (uint64_t)(ks & 3) * 32) >> 4;
-            tc::mma_f16(d, dA + ao, dB + bo, idesc[b], 1u);
           }
         }
         tc::commit(&empty[st]);
