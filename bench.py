@@ -658,9 +658,7 @@ def run_ours(a, rank, world, local_rank):
             "config": dict(workload(a), parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                            precision=a.precision),
             "e2e": {"value": world * 1e3 / e2e_ms, "unit": "evals/s", "ms_per_step": e2e_ms,
-                    # set_bodies uploads X and q of each 64-byte Body record (32 bytes);
-                    # get_bodies returns whole records (positions in tree order, p, F)
-                    "h2d_bytes_per_step": a.n * 32, "d2h_bytes_per_step": a.n * 64},
+                    "h2d_bytes_per_step": a.n * 64, "d2h_bytes_per_step": a.n * 64},
             "gpu_launches": launches, "roofline": roof, "roofline_m2l": roof_m2l, "cpu_baseline": cpu,
             "clocks": clk, "phases_ms": {k: statistics.mean(v) for k, v in phase.items()},
             "wall_ms_per_step": wall * 1e3 / a.steps, "error_vs_direct": err,

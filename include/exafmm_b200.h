@@ -264,7 +264,7 @@ EXAFMM_API int exafmm_b200_fma_peak(exafmm_b200 *h, int precision, double *tflop
  * (mixed form) accumulated in FP32 in tensor memory before the partial sum is
  * folded into the compensated running sum: fewer groups per window means
  * fewer FP32 additions between folds (a smaller accumulation error) and more
- * fold work (the default: 2 for P <= 10, 1 above).  Values 1-64; 0 restores
+ * fold work (the default: 2 for P <= 10, 1 for P = 11 and 12, 4 above).  Values 1-64; 0 restores
  * the default.  EXAFMM_TILE_P2P_STAGE: bodies of source leaves the near-field
  * kernel stages in shared memory per chunk (the source tile), 1024, 1536 or
  * 2048 (default: 1536 mixed, 1024 FP64); a speed choice: the sums change only

@@ -87,13 +87,6 @@ __global__ void k_pack_in(const double *rec, long n, int len, double4 *in, int *
   in[i] = v;
 }
 
-__global__ void k_check_bodies(const double4 *in, long n, int *bad) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double4 v = in[i];
-  if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) *bad = 1;
-}
-
 __global__ void k_check_finite(const double *q, long n, int *bad) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && !isfinite(q[i])) *bad = 1;
@@ -419,20 +412,14 @@ int exafmm_b200_set_bodies(exafmm_b200 *H, const double *rec, int64_t n, int whe
     const int len = rec_len(h);
     int *bad = &h.counters.as<DevCounters>()->overflow;
     FMM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), h.stream));
-    if (where == EXAFMM_HOST && len == 8) {
-      // only X and q cross the bus: the first 32 bytes of every 64-byte
-      // record, straight into the packed (x, y, z, q) array
-      FMM_CUDA(cudaMemcpy2DAsync(h.in.p, sizeof(double4), rec, 8 * sizeof(double), sizeof(double4), n,
-                                 cudaMemcpyHostToDevice, h.stream));
-      k_check_bodies<<<grid_for(n, 256), 256, 0, h.stream>>>(h.in.as<double4>(), n, bad);
-    } else {
-      if (where == EXAFMM_HOST) {
-        h.stage.need(n * len * sizeof(double));
-        FMM_CUDA(cudaMemcpyAsync(h.stage.p, rec, n * len * sizeof(double), cudaMemcpyHostToDevice, h.stream));
-        drec = h.stage.as<double>();
-      }
-      k_pack_in<<<grid_for(n, 256), 256, 0, h.stream>>>(drec, n, len, h.in.as<double4>(), bad);
+    // whole records cross the bus (a strided copy of only X and q, half the
+    // bytes, measured slower: the copy engine moves 32-byte rows poorly)
+    if (where == EXAFMM_HOST) {
+      h.stage.need(n * len * sizeof(double));
+      FMM_CUDA(cudaMemcpyAsync(h.stage.p, rec, n * len * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+      drec = h.stage.as<double>();
     }
+    k_pack_in<<<grid_for(n, 256), 256, 0, h.stream>>>(drec, n, len, h.in.as<double4>(), bad);
     h.launches++;
     FMM_LAUNCH();
     int hb = 0;

@@ -57,11 +57,14 @@ constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
 // charges positive) its error is a bias that grows with the MMAs per window:
 // measured on 200,000 Plummer bodies at P = 12, the local expansions' mean
 // relative error was -1.6e-6 over 16 groups, -4.1e-7 over two and -2.9e-7
-// over one (potential error 2.7x, 1.22x and 1.15x FP64's).  The default keeps
-// a window at two groups for P <= 10 and one above; a wider window, set with
-// exafmm_b200_set_tile, trades that accuracy for fewer folds (at 1M uniform
-// bodies, P = 10: 3.39 ms per evaluation with 16 groups, 3.45 with 2).
-int default_flush(int P) { return P > 10 ? 1 : 2; }
+// over one (potential error 2.7x, 1.22x and 1.15x FP64's).  Defaults, from
+// measurements at 1M uniform bodies: P <= 10 (two accumulators in tensor
+// memory) two groups, 3.45 ms per evaluation at P = 10 against 3.39 with 16;
+// P = 11, 12 (one accumulator and the running sum in tensor memory) one
+// group, 4.59 ms at P = 12 against 4.53; larger P (windows added to L in
+// global memory, where every window costs a read-modify-write) four.  A
+// wider window, set with exafmm_b200_set_tile, trades accuracy for time.
+int default_flush(int P) { return P <= 10 ? 2 : (P <= 12 ? 1 : 4); }
 // Limit of every wait of the tensor-core kernel (the drain of copies and MMAs
 // already in flight gets twice as long): a wait that runs out flags
 // EXAFMM_ERR_TIMEOUT instead of hanging the GPU.
@@ -596,11 +599,22 @@ __device__ __forceinline__ void tc_flush_global(uint32_t acc, int t, double inv,
   }
 }
 
+// Tensor-memory layout of the accumulators (columns; 128 lanes = targets):
+// nacc accumulators of KP columns `stride` apart, alternating per window
+// (two: the tensor core fills one while the epilogue folds the other; one:
+// the tensor core waits for each fold); with `fold`, the double-FP32 running
+// sum at columns [hi, hi + KP) and [lo, lo + KP), else windows are added to L
+// in global memory.  ncols is the allocation (a power of two).
+struct TcAcc {
+  int nacc, fold;
+  uint32_t stride, hi, lo, ncols;
+};
+
 __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, const int *tg_off, const int *tg_gid,
                                                           const int *tg_src, const unsigned char *ops,
                                                           const __half *M16, const double4 *xr, double2 *L, int P,
                                                           int KP, TcPlan pl,
-                                                          int nstage, uint32_t half_cols, int fold, int flush_every,
+                                                          int nstage, TcAcc ta, int flush_every,
                                                           const unsigned long long *m16_max, int *err, long wait_ns,
                                                           long stall_ns) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -616,9 +630,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
   uint64_t *stall = full + 10;  // nothing arrives here (the stall test hook waits on it)
   uint32_t *tslot = (uint32_t *)(full + 11);
   volatile int *abort = (volatile int *)(tslot + 1);  // a role gave up: the others stop waiting
-  // TMEM columns: accumulators [0, H) and [H, 2H); with `fold`, the running
-  // sum hi at [2H, 3H) and lo at [3H, 4H)
-  const uint32_t ncols = (fold ? 4u : 2u) * half_cols;
+  const uint32_t ncols = ta.ncols;
+  const int fold = ta.fold;
+  // window w's accumulator, and the phase of its barriers
+  auto acc_of = [&](int w) { return ta.nacc == 2 ? (w & 1) : 0; };
+  auto phase_of = [&](int w) { return (uint32_t)(ta.nacc == 2 ? (w >> 1) : w) & 1u; };
   if (warp == TC_MMA_WARP) tc::alloc(tslot, ncols);
   if (tid == 0) {
     for (int b = 0; b < 2; b++) tc::mbar_init(&full[b], TC_LOAD_WARPS * 32);
@@ -642,18 +658,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     const double us = scalbn(1.0, -m16_exponent(*m16_max));
     const int NT = tri(P);
     const uint32_t lanes = tmem + ((uint32_t)(warp * 32) << 16);
-    const uint32_t sum_hi = lanes + 2 * half_cols, sum_lo = lanes + 3 * half_cols;
+    const uint32_t sum_hi = lanes + ta.hi, sum_lo = lanes + ta.lo;
     if (fold) {
       tc_zero(sum_hi, 0, KP);
       tc_zero(sum_lo, 0, KP);
     }
     bool ok = true;
     for (int w = 0; w < nwin; w++) {
-      const int a = w & 1;
-      ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[a], (uint32_t)(w >> 1) & 1u, wait_ns, abort));
+      const int a = acc_of(w);
+      ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[a], phase_of(w), wait_ns, abort));
       if (!ok) break;
       tc::fence_after();
-      const uint32_t acc = lanes + (uint32_t)a * half_cols;
+      const uint32_t acc = lanes + (uint32_t)a * ta.stride;
       if (fold) tc_fold(acc, sum_hi, sum_lo, 0, KP);
       else tc_flush_global(acc, t, inv, us, 0, KP, NT, L);
       tc::fence_before();
@@ -735,17 +751,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
       bool ok = stall_ns <= 0 || tc::mbar_wait(stall, 0u, stall_ns, abort);
       int last = -1;
       for (int k = 0; ok && k < n; k++) {
-        const int st = k % nstage, w = k / flush_every, a = w & 1;
+        const int st = k % nstage, w = k / flush_every, a = acc_of(w);
         ok = tc::mbar_wait(&full[st], parity(k), wait_ns, abort) && tc::mbar_wait(&bful[st], parity(k), wait_ns, abort);
-        if (ok && k % flush_every == 0 && w >= 2)
-          ok = tc::mbar_wait(&acce[a], (uint32_t)((w >> 1) - 1) & 1u, wait_ns, abort);
+        // a new window reuses accumulator a once the epilogue has folded
+        // window w - nacc, its previous user
+        if (ok && k % flush_every == 0 && w >= ta.nacc)
+          ok = tc::mbar_wait(&acce[a], phase_of(w - ta.nacc), wait_ns, abort);
         if (!ok) break;
         tc::fence_after();
         const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
         const uint64_t dA = tc::smem_desc_sw128(sA), dB = tc::smem_desc_sw128(sB);
         const uint64_t lo_a = abytes >> 4, lo_b = bimg >> 4;  // descriptor start fields count 16 bytes
         const bool fresh = k % flush_every == 0;
-        const uint32_t acc = tmem + (uint32_t)a * half_cols;
+        const uint32_t acc = tmem + (uint32_t)a * ta.stride;
         // per K step: hi*hi, then hi*lo with the same A, then lo*hi (issuing
         // the small products first lowered the truncation bias by a third
         // but cost 15% of the M2L time: consecutive MMAs on one A are faster)
@@ -842,6 +860,17 @@ uint32_t tc_half_cols(int KP) {
   return c;
 }
 
+// Two double-buffered accumulators and the running sum where they fit (KP up
+// to 128: P <= 10), else one accumulator and the running sum (3 x KP
+// rounded to 32 columns within 512: P = 11, 12), else windows added to L in
+// global memory.
+TcAcc tc_acc_layout(int KP) {
+  const uint32_t hc = tc_half_cols(KP), k32 = ((uint32_t)KP + 31u) / 32u * 32u;
+  if (4 * hc <= 512) return TcAcc{2, 1, hc, 2 * hc, 3 * hc, 4 * hc};
+  if (3 * k32 <= 512) return TcAcc{1, 1, 0, k32, 2 * k32, 512};
+  return TcAcc{2, 0, hc, 0, 0, 2 * hc};
+}
+
 bool tc_available(int P) {
   const int KP = tc_kp(P);
   return KP <= 256 && tc_smem(make_tc_plan(P, KP)) <= TC_SMEM_MAX;
@@ -875,12 +904,10 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
   DevCounters *ctr = h.counters.as<DevCounters>();
   if (tcore) {
     FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
-    const uint32_t hc = tc_half_cols(KP16);
     k_m2l_tc<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
                                                     h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
                                                     h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
-                                                    tc_stages(tp), hc, 4 * hc <= 512 ? 1 : 0,
-                                                    m2l_flush_interval(h),
+                                                    tc_stages(tp), tc_acc_layout(KP16), m2l_flush_interval(h),
                                                     &ctr->m16_max, &ctr->tc_error, TC_WAIT_NS, h.tc_stall_ns);
     h.tc_stall_ns = 0;  // the test hook stalls one launch
     FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));

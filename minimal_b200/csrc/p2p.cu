@@ -618,13 +618,15 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
       for (int q = 0; q < 4; q++) red[(g * CT_TPT * H + i + u * H) * 4 + q] = (double)sacc[u][q] + (double)eacc[u][q];
   }
   __syncthreads();
-  if (tid < tn) {
+  // a target leaf holds up to CT_TPT * CT bodies: every thread writes
+  // targets tid, tid + CT, ...
+  for (int t = tid; t < tn; t += CT) {
     double r[4] = {0, 0, 0, 0};
     for (int gg = 0; gg < G; gg++)
 #pragma unroll
-      for (int q = 0; q < 4; q++) r[q] += red[(gg * CT_TPT * H + tid) * 4 + q];
+      for (int q = 0; q < 4; q++) r[q] += red[(gg * CT_TPT * H + t) * 4 + q];
     const double s1 = scale, s2 = s1 * s1;  // back to the input units
-    out[tb + tid] = make_double4(r[0] * s1, -r[1] * s2, -r[2] * s2, -r[3] * s2);
+    out[tb + t] = make_double4(r[0] * s1, -r[1] * s2, -r[2] * s2, -r[3] * s2);
   }
 }
 

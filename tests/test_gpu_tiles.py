@@ -37,7 +37,7 @@ def test_m2l_flush_default_and_range():
     from minimal_b200 import FMM, FMMError, drand48_bodies
 
     xq = drand48_bodies(30000, 5)
-    for P, want in ((8, 2), (10, 2), (12, 1)):
+    for P, want in ((8, 2), (10, 2), (11, 1), (12, 1), (14, 4)):
         f = FMM(P=P, precision="mixed")
         assert f.get_tile("m2l_flush") == want
     f = FMM(P=10, precision="mixed")
