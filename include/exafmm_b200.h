@@ -274,6 +274,11 @@ enum { EXAFMM_TILE_M2L_FLUSH = 0, EXAFMM_TILE_P2P_STAGE = 1 };
 EXAFMM_API int exafmm_b200_set_tile(exafmm_b200 *h, int which, int value);
 EXAFMM_API int exafmm_b200_get_tile(exafmm_b200 *h, int which, int *value);
 
+/* Diagnostic with no reference counterpart: the grouped M2L of the last
+ * evaluation -- operator groups, (tile, group) segments contracted, entries
+ * left to the direct-form kernel, target tiles (4 values). */
+EXAFMM_API int exafmm_b200_m2l_stats(exafmm_b200 *h, int64_t *stats4);
+
 /* Test hook with no reference counterpart: the next launch of the
  * tensor-core M2L kernel on this handle (mixed form) first waits `ns`
  * nanoseconds on a barrier that nothing arrives at, as if its inputs never

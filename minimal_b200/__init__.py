@@ -39,7 +39,7 @@ API = [
     "exafmm_b200_last_launches", "exafmm_b200_arch", "exafmm_b200_fma_peak", "exafmm_b200_direct_static",
     "exafmm_b200_dipole_correction", "exafmm_b200_ewald", "exafmm_b200_set_batch", "exafmm_b200_autotune",
     "exafmm_b200_set_charges", "exafmm_b200_reevaluate", "exafmm_b200_test_stall_tc",
-    "exafmm_b200_set_tile", "exafmm_b200_get_tile",
+    "exafmm_b200_set_tile", "exafmm_b200_get_tile", "exafmm_b200_m2l_stats",
     "exafmm_b200_ewald_parts", "exafmm_b200_p2p", "exafmm_b200_p2m", "exafmm_b200_m2m", "exafmm_b200_m2l", "exafmm_b200_l2l", "exafmm_b200_l2p",
 ]
 
@@ -103,6 +103,7 @@ def load_library(path=LIB_PATH):
         "exafmm_b200_reevaluate": (i, [vp]),
         "exafmm_b200_test_stall_tc": (i, [vp, i64]),
         "exafmm_b200_set_tile": (i, [vp, i, i]),
+        "exafmm_b200_m2l_stats": (i, [vp, vp]),
         "exafmm_b200_ewald_parts": (i, [vp, i, i, d, d, d, vp, i64, i]),
         "exafmm_b200_p2p": (i, [vp, vp, i64, vp, i64, vp, i]),
         "exafmm_b200_p2m": (i, [vp, vp, vp, i64, vp, i]),
@@ -415,6 +416,12 @@ class FMM:
         c = self._cell(cell)
         self._check(self.lib.exafmm_b200_l2p(self.h, _p(c), _p(lc), _p(b), len(b), HOST))
         return b
+
+    def m2l_stats(self):
+        """Grouped M2L of the last evaluation: groups, segments, residual entries, tiles."""
+        v = np.zeros(4, dtype=np.int64)
+        self._check(self.lib.exafmm_b200_m2l_stats(self.h, _p(v)))
+        return dict(zip(("groups", "segments", "residual", "tiles"), v.tolist()))
 
     TILES = {"m2l_flush": 0, "p2p_stage": 1}
 

@@ -361,7 +361,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
                  &h.m2l_raw, &h.m2l_key, &h.p2p_raw, &h.m2l_off, &h.m2l_ent, &h.p2p_off, &h.p2p_ent, &h.fill, &h.M, &h.L,
                  &h.m2l_units, &h.stage, &h.g_mt, &h.g_ekey, &h.g_occ, &h.g_cnt, &h.g_keyof, &h.g_ops,
                  &h.g_tk, &h.g_tile, &h.g_seg, &h.g_tg, &h.g_m16, &h.g_slot, &h.g_pairs, &h.shift_ops, &h.shift_terms,
-                 &h.op_scratch};
+                 &h.op_scratch, &h.g_gmark};
   for (Buf *b : bufs) b->release();
   if (h.ev_ok)
     for (int p = 0; p < PH_COUNT + 1; p++)
@@ -841,6 +841,19 @@ int exafmm_b200_get_tile(exafmm_b200 *H, int which, int *value) {
     if (which == EXAFMM_TILE_M2L_FLUSH) *value = m2l_flush_interval(h);
     else if (which == EXAFMM_TILE_P2P_STAGE) *value = p2p_tile(h);
     else throw Error{EXAFMM_ERR_ARG, "get_tile: unknown tile parameter"};
+  });
+}
+
+int exafmm_b200_m2l_stats(exafmm_b200 *H, int64_t *stats4) {
+  return guarded(H, [&](Handle &h) {
+    if (!stats4) throw Error{EXAFMM_ERR_ARG, "null output"};
+    stats4[0] = h.g_ngroups;
+    int nseg = 0;  // the exact count, from the segment scan's total
+    if (h.g_plan.valid && h.g_ngroups > 0)
+      FMM_CUDA(cudaMemcpy(&nseg, &h.counters.as<DevCounters>()->gcounts[3], sizeof(int), cudaMemcpyDeviceToHost));
+    stats4[1] = nseg;
+    stats4[2] = h.g_plan.valid ? h.g_plan.nres : 0;
+    stats4[3] = h.g_ntiles;
   });
 }
 

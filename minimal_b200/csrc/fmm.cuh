@@ -84,6 +84,7 @@ struct DevCounters {
   // largest |scaled multipole| over the possible M2L sources, as the bits of
   // a non-negative double (the FP16 split's power-of-two normalisation)
   unsigned long long m16_max;
+  int nghost;  // ghost sources of image entries (mixed form, periodic)
 };
 
 // Per-phase timing slots (CUDA events on the handle stream).
@@ -154,6 +155,8 @@ struct Handle {
 
   // grouped M2L (m2l_group.cu)
   Buf g_mt, g_ekey, g_occ, g_cnt, g_keyof, g_ops, g_tk, g_tile, g_seg, g_tg, g_m16, g_slot, g_pairs;
+  Buf g_gmark;      // ghost slots: marks, their scan, the slot of every ghost
+  int g_nghost = 0;  // ghost multipole rows after the cells' in g_m16
   // operator cache: group key -> slot in g_ops, for order op_P and layout
   // op_layout (0: FP64 row blocks, 1: tensor-core FP16 images)
   std::unordered_map<int, int> op_slot;

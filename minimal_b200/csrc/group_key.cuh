@@ -94,6 +94,42 @@ __device__ __forceinline__ int m2l_key_offset(int key, double R0, double cycle, 
   return (loc >> 15) - IKEY_DL;
 }
 
+// Ghost sources (mixed form).  An image entry whose fractional offset f (the
+// offset's distance from the integer vector v) is tiny can use the
+// free-space operator of (dl, v) instead of an image key of its own: its
+// source multipole is moved by the exact M2M shift f * r onto a "ghost"
+// centre at the integer offset, X_t - v r.  M2M keeps every retained order
+// exact, and with |f| <= GHOST_MAX_FRAC the shifted multipole's extent grows
+// by less than one percent of the cell radius, so the M2L's truncation error
+// barely changes.  Bodies that fill a periodic box give |f| ~ 1e-3 or less
+// (the root radius is the bounds' half-extent times 1.00001); other entries
+// keep their image keys.  A ghost is one (source cell, image, finer level)
+// triple: gslot = (s * 26 + image') * 4 + (lf - ls).
+constexpr double GHOST_MAX_FRAC = 0.005;
+constexpr int GHOST_SLOTS = 26 * 4;  // ghost slots per source cell
+
+// Returns the free-space key of the entry's ghost (or -1: no ghost), its
+// slot, and the shift f r from the image source's centre to the ghost's.
+__device__ __forceinline__ int m2l_ghost_key(const double4 &X, const double4 &Y, int dl, int img, int s, double R0,
+                                             double cycle, int depth, long *gslot, double3 *shift) {
+  if (img == 13 || dl < -KEY_DL || dl >= KEY_DL) return -1;
+  const double m = fmin(X.w, Y.w);
+  const int lf = ilogb(R0) - ilogb(m), dlf = ilogb(Y.w) - ilogb(m);
+  if (lf < 1 || lf > depth || dlf < 0 || dlf > 3) return -1;
+  const int ix = img % 3 - 1, iy = (img / 3) % 3 - 1, iz = img / 9 - 1;
+  const double sx = image_shift_units(ix, lf, R0, cycle), sy = image_shift_units(iy, lf, R0, cycle),
+               sz = image_shift_units(iz, lf, R0, cycle);
+  const double fx = rint(sx) - sx, fy = rint(sy) - sy, fz = rint(sz) - sz;
+  if (fabs(fx) > GHOST_MAX_FRAC || fabs(fy) > GHOST_MAX_FRAC || fabs(fz) > GHOST_MAX_FRAC) return -1;
+  const double inv = 1.0 / m;
+  const double vx = rint((X.x - Y.x) * inv) - rint(sx), vy = rint((X.y - Y.y) * inv) - rint(sy),
+               vz = rint((X.z - Y.z) * inv) - rint(sz);
+  if (vx < -KEY_V || vx >= KEY_V || vy < -KEY_V || vy >= KEY_V || vz < -KEY_V || vz >= KEY_V) return -1;
+  *gslot = ((long)s * 26 + (img < 13 ? img : img - 1)) * 4 + dlf;
+  *shift = make_double3(fx * m, fy * m, fz * m);
+  return ((dl + KEY_DL) << 18) | (((int)vx + KEY_V) << 12) | (((int)vy + KEY_V) << 6) | ((int)vz + KEY_V);
+}
+
 // Marks a key and a target as present.  A few hundred keys (and every
 // target) take millions of entries: store only what this SM has not seen
 // set, so the L1-cached reads keep the stores off a few hot L2 lines.

@@ -34,6 +34,7 @@
 #include "group_key.cuh"
 #include "m2l_group.h"
 #include "tc.cuh"
+#include "translations.cuh"
 
 namespace fmm {
 
@@ -75,20 +76,51 @@ constexpr int OP_KEYS_HOST = 8192;
 // Group key of every M2L entry of the ordered CSR lists (expanded to pairs);
 // marks the keys that occur and the targets that have grouped entries.  (The
 // walk does the same for its raw entries.)
-__global__ void k_gkeys(long n, const int2 *pairs, const double4 *xr, const int *level, int *ekey, int *occ,
-                        int *gflag, int *nres, double cycle, int depth) {
+// With `gscan` (mixed form, periodic): an image entry that has a ghost takes
+// the ghost's free-space key, and its source becomes the ghost's multipole
+// row, ncells + ghost index.
+__global__ void k_gkeys(long n, int2 *pairs, const double4 *xr, const int *level, int *ekey, int *occ,
+                        int *gflag, int *nres, double cycle, int depth, const int *gscan, int ncells) {
   const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
   int key = -1;
   if (e < n) {
     const int2 pr = pairs[e];
     const int t = pr.x & (int)IDX_MASK, img = (int)((u32)pr.x >> IMG_SHIFT), s = pr.y;
-    if (img == 13) key = m2l_group_key(xr[t], xr[s], level[t] - level[s]);
-    else key = m2l_image_key(xr[t], xr[s], level[t] - level[s], img, xr[0].w, cycle, depth);
+    if (img == 13) {
+      key = m2l_group_key(xr[t], xr[s], level[t] - level[s]);
+    } else {
+      long gslot = -1;
+      double3 shift;
+      if (gscan) key = m2l_ghost_key(xr[t], xr[s], level[t] - level[s], img, s, xr[0].w, cycle, depth, &gslot, &shift);
+      if (key >= 0) pairs[e] = make_int2(pr.x, ncells + gscan[gslot]);
+      else key = m2l_image_key(xr[t], xr[s], level[t] - level[s], img, xr[0].w, cycle, depth);
+    }
     if (key >= 0) m2l_mark_key(key, t, occ, gflag);
     ekey[e] = key;
   }
   const int nr = __syncthreads_count(e < n && key < 0);  // one atomic per block
   if (threadIdx.x == 0 && nr) atomicAdd(nres, nr);
+}
+
+// Ghost slots used by the image entries (see m2l_ghost_key).
+__global__ void k_ghost_mark(long n, const int2 *pairs, const double4 *xr, const int *level, double cycle, int depth,
+                             int *gmark) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const int2 pr = pairs[e];
+  const int t = pr.x & (int)IDX_MASK, img = (int)((u32)pr.x >> IMG_SHIFT), s = pr.y;
+  if (img == 13) return;
+  long gslot = -1;
+  double3 shift;
+  if (m2l_ghost_key(xr[t], xr[s], level[t] - level[s], img, s, xr[0].w, cycle, depth, &gslot, &shift) >= 0 &&
+      gmark[gslot] == 0)
+    gmark[gslot] = 1;
+}
+
+// The slot of every ghost, in slot order.
+__global__ void k_ghost_list(long nslots, const int *gmark, const int *gscan, int *gslots) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nslots && gmark[i]) gslots[gscan[i]] = (int)i;
 }
 
 // CSR lists expanded to (target | img << 26, source) pairs in list order.
@@ -331,6 +363,48 @@ __global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const d
   row[ci] = __halves2half2(hx, hy);
   row[half_kp + ci] = __halves2half2(__double2half(v.x - (double)__half2float(hx)),
                                      __double2half(v.y - (double)__half2float(hy)));
+}
+
+// One CTA per ghost: the source's multipole moved by the M2M shift f r onto
+// the ghost centre (3d/kernel.h:204-231 for one child, offset ghost - source
+// = f r), scaled like k_mscale16 (1 / R^n, times 2^E) and split into the
+// ghost's FP16 hi / lo row, M16[ncells + g].
+__global__ void __launch_bounds__(128) k_ghost16(int nghost, const int *gslots, const double4 *xr, const double2 *M,
+                                                 int P, int KP, double cycle, int depth,
+                                                 const unsigned long long *mx, int ncells, __half2 *M16) {
+  extern __shared__ double2 gsh[];  // harmonics of the shift, then the source multipole
+  const int NT = tri(P), g = blockIdx.x;
+  double2 *Ysh = gsh, *Msh = gsh + NT;
+  const int slot = gslots[g];
+  const int s = slot / GHOST_SLOTS, ic = (slot % GHOST_SLOTS) / 4, dlf = slot % 4;
+  const int img = ic < 13 ? ic : ic + 1;
+  const double4 Y = xr[s];
+  const double R0 = xr[0].w, m = scalbn(Y.w, -dlf);
+  const int lf = ilogb(R0) - ilogb(m);
+  const int ix = img % 3 - 1, iy = (img / 3) % 3 - 1, iz = img / 9 - 1;
+  const double sx = image_shift_units(ix, lf, R0, cycle), sy = image_shift_units(iy, lf, R0, cycle),
+               sz = image_shift_units(iz, lf, R0, cycle);
+  const Sph sg = sph_of((rint(sx) - sx) * m, (rint(sy) - sy) * m, (rint(sz) - sz) * m);
+  if ((int)threadIdx.x < P)
+    regular_column(threadIdx.x, P, sg.r, sg, sg.e, [&](int n, double2 y, double2) { Ysh[tri(n) + threadIdx.x] = y; });
+  for (int k = threadIdx.x; k < NT; k += blockDim.x) Msh[k] = M[(long)s * NT + k];
+  __syncthreads();
+  const double E = scalbn(1.0, m16_exponent(*mx));
+  const int half_kp = KP / 2;
+  __half2 *row = M16 + (long)(ncells + g) * KP;
+  for (int ci = threadIdx.x; ci < half_kp; ci += blockDim.x) {
+    double2 v = make_double2(0, 0);
+    if (ci < NT) {
+      const int j = order_of(ci), k = ci - tri(j);
+      const double2 mm = m2m_coeff(j, k, Msh, Ysh);
+      const double sc = mscale_factor(ci, Y.w) * E;
+      v = make_double2(mm.x * sc, mm.y * sc);
+    }
+    const __half hx = __double2half(v.x), hy = __double2half(v.y);
+    row[ci] = __halves2half2(hx, hy);
+    row[half_kp + ci] = __halves2half2(__double2half(v.x - (double)__half2float(hx)),
+                                       __double2half(v.y - (double)__half2float(hy)));
+  }
 }
 
 __global__ void k_tkeys(int ncells, const int *gflag, const int *level, const int *parent, const int *child,
@@ -951,8 +1025,30 @@ void m2l_grouped_pass(Handle &h) {
     k_mscale<<<grid_for((long)C * gp.KP, TB), TB, 0, s>>>(C, P, gp.KP, h.c_xr.as<double4>(), h.M.as<double2>(),
                                                           h.g_mt.as<double>());
   }
+  // ghost sources (mixed form, periodic): their rows after the cells' in
+  // M16, from this evaluation's multipoles
+  const double cyc = h.prm.images ? h.prm.cycle : 0.0;
+  auto ghost_rows = [&]() {
+    if (h.g_nghost <= 0) return;
+    const size_t row = (size_t)2 * KP16 * sizeof(__half);
+    if (h.g_m16.bytes < (size_t)(C + h.g_nghost) * row) {  // grown: the cell rows again
+      h.g_m16.need((size_t)(C + h.g_nghost) * row);
+      k_mscale16<<<grid_for((long)C * (KP16 / 2), TB), TB, 0, s>>>(C, P, KP16, h.c_xr.as<double4>(),
+                                                                   h.M.as<double2>(),
+                                                                   &h.counters.as<DevCounters>()->m16_max,
+                                                                   h.g_m16.as<__half2>());
+      h.launches++;
+    }
+    const long nsl = (long)C * GHOST_SLOTS;
+    k_ghost16<<<h.g_nghost, 128, 2 * NT * sizeof(double2), s>>>(
+        h.g_nghost, h.g_gmark.as<int>() + 2 * nsl, h.c_xr.as<double4>(), h.M.as<double2>(), P, KP16, cyc, h.depth,
+        &h.counters.as<DevCounters>()->m16_max, C, h.g_m16.as<__half2>());
+    h.launches++;
+    FMM_LAUNCH();
+  };
   // same lists, P and form as the last grouping: contract directly
   if (h.g_plan.valid && h.g_plan.P == P && h.g_plan.tcore == tcore && h.g_plan.ordered == h.m2l_ordered) {
+    ghost_rows();
     if (h.g_ngroups > 0) contract(h, tcore, tp, KP16, gp, pd);
     h.launches++;
     FMM_LAUNCH();
@@ -966,7 +1062,6 @@ void m2l_grouped_pass(Handle &h) {
   const int2 *pairs = h.m2l_raw.as<int2>();
   const int *ekey = h.m2l_key.as<int>();
   const long ks = key_space(h.prm.images, h.depth);
-  const double cyc = h.prm.images ? h.prm.cycle : 0.0;
   int *occ = h.g_occ.as<int>(), *gidx = occ + ks;  // sized by build_lists
   int *gflag = h.g_cnt.as<int>(), *tslot = gflag + C;
   DevCounters *ctr = h.counters.as<DevCounters>();
@@ -980,8 +1075,24 @@ void m2l_grouped_pass(Handle &h) {
     h.g_ekey.need(nent * sizeof(int));
     FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)ks * sizeof(int), s));
     FMM_CUDA(cudaMemsetAsync(gflag, 0, (size_t)C * sizeof(int), s));
-    k_gkeys<<<grid_for(nent, TB), TB, 0, s>>>(nent, pairs, h.c_xr.as<double4>(), h.c_level.as<int>(),
-                                              h.g_ekey.as<int>(), occ, gflag, &counts[0], cyc, h.depth);
+    // ghosts: image entries with a tiny fractional offset use free-space
+    // keys (mixed form only: the FP64 form keeps the reference's offsets)
+    const int *gscan = nullptr;
+    FMM_CUDA(cudaMemsetAsync(&ctr->nghost, 0, sizeof(int), s));
+    if (tcore && h.prm.images > 0) {
+      const long nsl = (long)C * GHOST_SLOTS;
+      h.g_gmark.need((size_t)nsl * 3 * sizeof(int) + 64);
+      int *gmark = h.g_gmark.as<int>(), *gsc = gmark + nsl, *gslots = gsc + nsl;
+      FMM_CUDA(cudaMemsetAsync(gmark, 0, (size_t)nsl * sizeof(int), s));
+      k_ghost_mark<<<grid_for(nent, TB), TB, 0, s>>>(nent, h.g_pairs.as<int2>(), h.c_xr.as<double4>(),
+                                                     h.c_level.as<int>(), cyc, h.depth, gmark);
+      scan_exclusive_int(h, gmark, gsc, nsl, &ctr->nghost);
+      k_ghost_list<<<grid_for(nsl, TB), TB, 0, s>>>(nsl, gmark, gsc, gslots);
+      gscan = gsc;
+      h.launches += 2;
+    }
+    k_gkeys<<<grid_for(nent, TB), TB, 0, s>>>(nent, h.g_pairs.as<int2>(), h.c_xr.as<double4>(), h.c_level.as<int>(),
+                                              h.g_ekey.as<int>(), occ, gflag, &counts[0], cyc, h.depth, gscan, C);
     ekey = h.g_ekey.as<int>();
     h.launches += 2;
   }
@@ -1004,6 +1115,7 @@ void m2l_grouped_pass(Handle &h) {
   FMM_CUDA(cudaStreamSynchronize(s));
   const int nres = h.m2l_ordered ? h.hc.gcounts[0] : h.hc.walk_resid;
   const int nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
+  h.g_nghost = h.m2l_ordered ? h.hc.nghost : 0;
   h.launches += 4;
   if (nres > 0 && !h.m2l_ordered) {  // residual entries are summed in list order: order, then start over
     order_m2l_lists(h);
@@ -1106,6 +1218,7 @@ void m2l_grouped_pass(Handle &h) {
     k_tg_off<<<grid_for(ntiles + 1, TB), TB, 0, s>>>(ntiles, ngroups, segid, &counts[3], tg_off);
     h.g_ntiles = ntiles;
     h.g_nseg = nseg;  // an upper bound unless it was read
+    ghost_rows();
     contract(h, tcore, tp, KP16, gp, pd);
     h.launches += 10;
     FMM_LAUNCH();
