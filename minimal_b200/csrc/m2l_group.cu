@@ -757,37 +757,49 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
       tc_store(sum_hi, sum_lo, t, inv, us, 0, KP, NT, L);
     }
   } else if (warp < TC_LOAD_WARP + TC_LOAD_WARPS) {
-    // ---- producers: thread r copies target row r of the tile -- the 16-byte
-    // chunks of its source cell's multipole (hi then lo halves, contiguous
-    // in global memory) with cp.async into the swizzled layout; absent
-    // targets are zero-filled.  A warp thus has 32 rows in flight per
-    // instruction.  Producer thread 0 also starts the operator's bulk copy.
-    // Each thread's copies arrive on the stage's barrier by themselves
-    // (cp.async.mbarrier.arrive), so the producers run up to two groups
-    // ahead of the MMAs.
-    const int r = tid - TC_LOAD_WARP * 32;
-    const int nchunk = KP / 4;  // 16-byte chunks per source row (hi and lo)
-    const uint32_t rsw = (uint32_t)(r & 7) << 4;
-    auto src_of = [&](int k) { return k < n ? tg_src[(long)(g0 + k) * TC_TILE + r] : -1; };
-    auto issue = [&](int k, int s) {
+    // ---- producers: warp pw copies target rows 32pw..32pw+31 of the tile
+    // with cp.async into the swizzled layout.  Lane l takes rows
+    // 32pw + (l >> 1) and 32pw + 16 + (l >> 1), and of each source row (the
+    // multipole's hi then lo halves, 4 KP contiguous bytes in global memory)
+    // the 16-byte chunks of parity l & 1: the two lanes of a pair copy the
+    // two halves of every 32-byte sector in the same instruction, so each
+    // sector is requested from L2 once (one lane per row requested every
+    // sector twice, and the L1-to-L2 request path was the kernel's limit).
+    // Absent targets are zero-filled.  Producer thread 0 also starts the
+    // operator's bulk copy.  Each thread's copies arrive on the stage's
+    // barrier by themselves (cp.async.mbarrier.arrive), so the producers run
+    // up to two groups ahead of the MMAs.
+    const int pw = warp - TC_LOAD_WARP, par = lane & 1;
+    const int ra = 32 * pw + (lane >> 1), rb = ra + 16;
+    const int half = KP / 8;  // 16-byte chunks of one half (hi or lo) of a source row; even
+    auto src_of = [&](int k) {
+      const int *row = tg_src + (long)(g0 + k) * TC_TILE;
+      return k < n ? make_int2(row[ra], row[rb]) : make_int2(-1, -1);
+    };
+    auto issue = [&](int k, int2 s2) {
       const int st = k % nstage;
-      unsigned char *S = base + (size_t)st * stage_bytes + r * 128;
-      if (r == 0) {
+      unsigned char *S = base + (size_t)st * stage_bytes;
+      if (pw == 0 && lane == 0) {
         tc::mbar_arrive_expect_tx(&bful[st], 2 * bimg);
         tc::bulk_g2s(S + 2 * abytes, ops + (size_t)tg_gid[g0 + k] * 2 * bimg, 2 * bimg, &bful[st]);
       }
-      const __half *src = M16 + (size_t)(s < 0 ? 0 : s) * 2 * KP;
-      const uint32_t nb = s >= 0 ? 16u : 0u;
-      for (int c = 0; c < nchunk; c++) {
-        const int hl = c >= nchunk / 2, cc = c - hl * (nchunk / 2);
-        const uint32_t off = hl * abytes + (cc >> 3) * (TC_TILE * 128) + (((uint32_t)(cc & 7) << 4) ^ rsw);
-        tc::cp_async16(S + off, src + c * 8, nb);
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int r = j ? rb : ra, s = j ? s2.y : s2.x;
+        const __half *src = M16 + (size_t)(s < 0 ? 0 : s) * 2 * KP;
+        const uint32_t nb = s >= 0 ? 16u : 0u, rsw = (uint32_t)(r & 7) << 4;
+        unsigned char *R = S + r * 128;
+        for (int c = par; c < 2 * half; c += 2) {
+          const int hl = c >= half, cc = c - hl * half;
+          const uint32_t off = hl * abytes + (cc >> 3) * (TC_TILE * 128) + (((uint32_t)(cc & 7) << 4) ^ rsw);
+          tc::cp_async16(R + off, src + c * 8, nb);
+        }
       }
       tc::cp_async_commit();
     };
     bool ok = true;
     int last = -1;
-    int s_next = src_of(0);
+    int2 s_next = src_of(0);
     for (int k = 0; k < n; k++) {
       if (k >= nstage) {  // the stage is free once the MMAs of group k - nstage are done
         ok = __all_sync(0xffffffffu,
@@ -806,7 +818,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     // drain this thread's copies; the operator's bulk copy completes by
     // itself (bounded wait, no abort: the copy must land before exit)
     tc::cp_async_wait_all();
-    if (r == 0 && last >= 0) tc::mbar_wait(&bful[last % nstage], parity(last), 2 * wait_ns);
+    if (pw == 0 && lane == 0 && last >= 0) tc::mbar_wait(&bful[last % nstage], parity(last), 2 * wait_ns);
   } else if (warp == TC_MMA_WARP) {
     // ---- MMA issuer (one thread): per group and output block, K steps of
     // hi*hi + hi*lo + lo*hi into the window's accumulator
