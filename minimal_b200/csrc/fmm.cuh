@@ -175,6 +175,11 @@ struct Handle {
   } g_plan;
   bool force_direct_m2l = false;  // diagnostic: per-pair direct-form M2L only
   Buf op_scratch;  // single-operator entry points (ops.cu): staged arrays
+  // far-image harmonic sums (periodic.cu), kept for the (P, images, cycle)
+  // they were made for
+  Buf per_harm;
+  int per_P = 0, per_images = 0;
+  double per_cycle = 0;
   // tile shapes chosen at run time (exafmm_b200_set_tile; the autotuner)
   int tile_m2l_flush = 0;  // tensor-core M2L groups per FP32 accumulator window (0: default)
   int tile_p2p_stage = 0;  // near-field source tile: bodies staged per chunk (0: default)

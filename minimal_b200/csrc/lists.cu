@@ -357,7 +357,7 @@ void build_lists(Handle &h) {
   // P2P lists are ordered always: their order is the near field's summation
   // order, which keeps results reproducible.
   h.m2l_ordered = false;
-  if (images > 0 || h.force_direct_m2l || h.prm.dim == 2) order_m2l_lists(h);
+  if (h.force_direct_m2l || h.prm.dim == 2) order_m2l_lists(h);
   bucket(h, h.p2p_raw.as<int2>(), &ctr->n_p2p, h.n_p2p, h.p2p_off, h.p2p_ent, true);
 }
 

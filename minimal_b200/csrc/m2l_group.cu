@@ -365,16 +365,21 @@ __global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const d
                                      __double2half(v.y - (double)__half2float(hy)));
 }
 
-// One CTA per ghost: the source's multipole moved by the M2M shift f r onto
-// the ghost centre (3d/kernel.h:204-231 for one child, offset ghost - source
-// = f r), scaled like k_mscale16 (1 / R^n, times 2^E) and split into the
-// ghost's FP16 hi / lo row, M16[ncells + g].
-__global__ void __launch_bounds__(128) k_ghost16(int nghost, const int *gslots, const double4 *xr, const double2 *M,
-                                                 int P, int KP, double cycle, int depth,
-                                                 const unsigned long long *mx, int ncells, __half2 *M16) {
-  extern __shared__ double2 gsh[];  // harmonics of the shift, then the source multipole
-  const int NT = tri(P), g = blockIdx.x;
-  double2 *Ysh = gsh, *Msh = gsh + NT;
+// A warp per ghost (GH_WARPS per block): the source's multipole moved by the
+// M2M shift f r onto the ghost centre (3d/kernel.h:204-231 for one child,
+// offset ghost - source = f r), scaled like k_mscale16 (1 / R^n, times 2^E)
+// and split into the ghost's FP16 hi / lo row, M16[ncells + g].  Lane m < P
+// generates harmonic column m (ghosts exist for P <= 15, with the
+// tensor-core M2L).
+constexpr int GH_WARPS = 8;
+__global__ void __launch_bounds__(GH_WARPS * 32) k_ghost16(int nghost, const int *gslots, const double4 *xr,
+                                                           const double2 *M, int P, int KP, double cycle, int depth,
+                                                           const unsigned long long *mx, int ncells, __half2 *M16) {
+  extern __shared__ double2 gsh[];  // per warp: harmonics of the shift, then the source multipole
+  const int NT = tri(P), wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * GH_WARPS + wp;
+  if (g >= nghost) return;  // warp-uniform; the kernel has no block barrier
+  double2 *Ysh = gsh + (size_t)wp * 2 * NT, *Msh = Ysh + NT;
   const int slot = gslots[g];
   const int s = slot / GHOST_SLOTS, ic = (slot % GHOST_SLOTS) / 4, dlf = slot % 4;
   const int img = ic < 13 ? ic : ic + 1;
@@ -385,14 +390,13 @@ __global__ void __launch_bounds__(128) k_ghost16(int nghost, const int *gslots, 
   const double sx = image_shift_units(ix, lf, R0, cycle), sy = image_shift_units(iy, lf, R0, cycle),
                sz = image_shift_units(iz, lf, R0, cycle);
   const Sph sg = sph_of((rint(sx) - sx) * m, (rint(sy) - sy) * m, (rint(sz) - sz) * m);
-  if ((int)threadIdx.x < P)
-    regular_column(threadIdx.x, P, sg.r, sg, sg.e, [&](int n, double2 y, double2) { Ysh[tri(n) + threadIdx.x] = y; });
-  for (int k = threadIdx.x; k < NT; k += blockDim.x) Msh[k] = M[(long)s * NT + k];
-  __syncthreads();
+  if (lane < P) regular_column(lane, P, sg.r, sg, sg.e, [&](int n, double2 y, double2) { Ysh[tri(n) + lane] = y; });
+  for (int k = lane; k < NT; k += 32) Msh[k] = M[(long)s * NT + k];
+  __syncwarp();
   const double E = scalbn(1.0, m16_exponent(*mx));
   const int half_kp = KP / 2;
   __half2 *row = M16 + (long)(ncells + g) * KP;
-  for (int ci = threadIdx.x; ci < half_kp; ci += blockDim.x) {
+  for (int ci = lane; ci < half_kp; ci += 32) {
     double2 v = make_double2(0, 0);
     if (ci < NT) {
       const int j = order_of(ci), k = ci - tri(j);
@@ -1052,7 +1056,7 @@ void m2l_grouped_pass(Handle &h) {
       h.launches++;
     }
     const long nsl = (long)C * GHOST_SLOTS;
-    k_ghost16<<<h.g_nghost, 128, 2 * NT * sizeof(double2), s>>>(
+    k_ghost16<<<(h.g_nghost + GH_WARPS - 1) / GH_WARPS, GH_WARPS * 32, GH_WARPS * 2 * NT * sizeof(double2), s>>>(
         h.g_nghost, h.g_gmark.as<int>() + 2 * nsl, h.c_xr.as<double4>(), h.M.as<double2>(), P, KP16, cyc, h.depth,
         &h.counters.as<DevCounters>()->m16_max, C, h.g_m16.as<__half2>());
     h.launches++;
@@ -1079,10 +1083,19 @@ void m2l_grouped_pass(Handle &h) {
   DevCounters *ctr = h.counters.as<DevCounters>();
   int *counts = ctr->gcounts;
   FMM_CUDA(cudaMemsetAsync(counts, 0, 4 * sizeof(int), s));
-  if (h.m2l_ordered) {
+  // keys computed here: for the ordered lists, and for the mixed form's
+  // periodic entries (ghost sources change their keys)
+  const bool ghosts = tcore && h.prm.images > 0;
+  const bool rekey = h.m2l_ordered || ghosts;
+  if (rekey) {
+    // the grouping's own copy of the pairs (k_gkeys points ghost entries at
+    // ghost rows; the lists themselves stay as the walk made them)
     h.g_pairs.need(nent * sizeof(int2));
-    k_csr_pairs<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
-                                                          h.g_pairs.as<int2>());
+    if (h.m2l_ordered)
+      k_csr_pairs<<<grid_for((long)C * 32, TB), TB, 0, s>>>(C, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
+                                                            h.g_pairs.as<int2>());
+    else
+      FMM_CUDA(cudaMemcpyAsync(h.g_pairs.p, h.m2l_raw.p, nent * sizeof(int2), cudaMemcpyDeviceToDevice, s));
     pairs = h.g_pairs.as<int2>();
     h.g_ekey.need(nent * sizeof(int));
     FMM_CUDA(cudaMemsetAsync(occ, 0, (size_t)ks * sizeof(int), s));
@@ -1091,7 +1104,7 @@ void m2l_grouped_pass(Handle &h) {
     // keys (mixed form only: the FP64 form keeps the reference's offsets)
     const int *gscan = nullptr;
     FMM_CUDA(cudaMemsetAsync(&ctr->nghost, 0, sizeof(int), s));
-    if (tcore && h.prm.images > 0) {
+    if (ghosts) {
       const long nsl = (long)C * GHOST_SLOTS;
       h.g_gmark.need((size_t)nsl * 3 * sizeof(int) + 64);
       int *gmark = h.g_gmark.as<int>(), *gsc = gmark + nsl, *gslots = gsc + nsl;
@@ -1125,9 +1138,9 @@ void m2l_grouped_pass(Handle &h) {
   double4 root{};
   FMM_CUDA(cudaMemcpyAsync(&root, h.c_xr.p, sizeof(double4), cudaMemcpyDeviceToHost, s));
   FMM_CUDA(cudaStreamSynchronize(s));
-  const int nres = h.m2l_ordered ? h.hc.gcounts[0] : h.hc.walk_resid;
+  const int nres = rekey ? h.hc.gcounts[0] : h.hc.walk_resid;
   const int nflag = h.hc.gcounts[1], ngroups = h.hc.gcounts[2];
-  h.g_nghost = h.m2l_ordered ? h.hc.nghost : 0;
+  h.g_nghost = rekey ? h.hc.nghost : 0;
   h.launches += 4;
   if (nres > 0 && !h.m2l_ordered) {  // residual entries are summed in list order: order, then start over
     order_m2l_lists(h);

@@ -8,9 +8,10 @@
 //   Mp     += sum over the 26 offsets (ix,iy,iz) != 0 of M2M(Mp from ...)
 //   cyc    *= 3.
 // M2L and M2M are linear in the offset harmonics, so each sum is one
-// translation with the harmonics summed over the offsets.  One CTA, FP64 in
-// every precision form; the per-thread partial sums are reduced in a fixed
-// order, so the result is deterministic.
+// translation with the harmonics summed over the offsets; the sums depend
+// only on P, the period and the number of images and are kept between
+// evaluations.  FP64 in every precision form; the per-thread partial sums are
+// reduced in a fixed order, so the result is deterministic.
 //
 // Dipole correction (3dp/fmm.cxx:63-75): d = sum q X over all bodies,
 // coef = 4 pi / (3 cycle^3); p -= coef |d|^2 / N / q, F -= coef d.
@@ -32,13 +33,17 @@ namespace {
 
 constexpr int PT = 256;  // threads of the periodic CTA
 
-__global__ void __launch_bounds__(PT) k_periodic(const double2 *M, double2 *L, int P, int images, double cycle,
-                                                 int T) {
-  extern __shared__ double2 sp[];  // partial[T][nt], Mp[nt], Mn[nt], H[nt]
+// The harmonic sums of the far images, per sublevel l (period cycle * 3^l):
+// H[2l] the irregular harmonics summed over the 702 M2L offsets, H[2l + 1]
+// the regular harmonics summed over the 26 M2M offsets (rows of nt).  They
+// depend only on P, the period and the number of images, so they are made
+// once per parameter set and kept.  One CTA; T threads sum the offsets,
+// then the partial sums are reduced in thread order (deterministic).
+__global__ void __launch_bounds__(PT) k_periodic_harm(int P, int images, double cycle, int T, double2 *H) {
+  extern __shared__ double2 sp[];  // partial[T][nt]
   const int nt = tri(P);
-  double2 *part = sp, *Mp = part + (size_t)T * nt, *Mn = Mp + nt, *H = Mn + nt;
+  double2 *part = sp;
   const int tid = threadIdx.x;
-  for (int o = tid; o < nt; o += PT) Mp[o] = M[o];  // the root is cell 0
   double cyc = cycle;
   for (int level = 0; level < images - 1; level++) {
     // irregular harmonics summed over the 702 M2L offsets
@@ -62,19 +67,12 @@ __global__ void __launch_bounds__(PT) k_periodic(const double2 *M, double2 *L, i
     }
     __syncthreads();
     for (int o = tid; o < nt; o += PT) {
-      double2 s = make_double2(0, 0);
+      double2 v = make_double2(0, 0);
       for (int t = 0; t < T; t++) {
-        s.x += part[(size_t)t * nt + o].x;
-        s.y += part[(size_t)t * nt + o].y;
+        v.x += part[(size_t)t * nt + o].x;
+        v.y += part[(size_t)t * nt + o].y;
       }
-      H[o] = s;
-    }
-    __syncthreads();
-    for (int o = tid; o < nt; o += PT) {
-      const int j = order_of(o), k = o - tri(j);
-      const double2 v = m2l_coeff(j, k, P, Mp, H);
-      L[o].x += v.x;
-      L[o].y += v.y;
+      H[(size_t)(2 * level) * nt + o] = v;
     }
     __syncthreads();
     // regular harmonics summed over the 26 M2M offsets (parent - child)
@@ -96,23 +94,43 @@ __global__ void __launch_bounds__(PT) k_periodic(const double2 *M, double2 *L, i
     }
     __syncthreads();
     for (int o = tid; o < nt; o += PT) {
-      double2 s = make_double2(0, 0);
+      double2 v = make_double2(0, 0);
       for (int t = 0; t < T; t++) {
-        s.x += part[(size_t)t * nt + o].x;
-        s.y += part[(size_t)t * nt + o].y;
+        v.x += part[(size_t)t * nt + o].x;
+        v.y += part[(size_t)t * nt + o].y;
       }
-      H[o] = s;
+      H[(size_t)(2 * level + 1) * nt + o] = v;
     }
     __syncthreads();
+    cyc *= 3;
+  }
+}
+
+// Per evaluation: the root's multipole through the sublevels with the kept
+// harmonic sums -- L_root += M2L(Mp, H[2l]), Mp += M2M(Mp, H[2l + 1]).
+__global__ void __launch_bounds__(PT) k_periodic(const double2 *M, double2 *L, int P, int images, const double2 *H) {
+  extern __shared__ double2 sp[];  // Mp[nt], Mn[nt]
+  const int nt = tri(P);
+  double2 *Mp = sp, *Mn = Mp + nt;
+  const int tid = threadIdx.x;
+  for (int o = tid; o < nt; o += PT) Mp[o] = M[o];  // the root is cell 0
+  __syncthreads();
+  for (int level = 0; level < images - 1; level++) {
+    const double2 *H1 = H + (size_t)(2 * level) * nt, *H2 = H1 + nt;
     for (int o = tid; o < nt; o += PT) {
       const int j = order_of(o), k = o - tri(j);
-      const double2 v = m2m_coeff(j, k, Mp, H);
+      const double2 v = m2l_coeff(j, k, P, Mp, H1);
+      L[o].x += v.x;
+      L[o].y += v.y;
+    }
+    for (int o = tid; o < nt; o += PT) {
+      const int j = order_of(o), k = o - tri(j);
+      const double2 v = m2m_coeff(j, k, Mp, H2);
       Mn[o] = make_double2(Mp[o].x + v.x, Mp[o].y + v.y);
     }
     __syncthreads();
     for (int o = tid; o < nt; o += PT) Mp[o] = Mn[o];
     __syncthreads();
-    cyc *= 3;
   }
 }
 
@@ -318,15 +336,26 @@ __global__ void __launch_bounds__(EB) k_ewald_targets(const double4 *src, long n
 }  // namespace
 
 void periodic_set_attributes() {
-  cudaFuncSetAttribute(k_periodic, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_periodic_harm, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 void periodic_pass(Handle &h) {
   if (h.prm.dim == 2) return periodic_pass_2d(h);
   if (h.prm.images < 2) return;
-  const int P = h.prm.P, nt = tri(P), T = periodic_threads(P);
-  k_periodic<<<1, PT, ((size_t)T + 3) * nt * sizeof(double2), h.stream>>>(h.M.as<double2>(), h.L.as<double2>(), P,
-                                                                          h.prm.images, h.prm.cycle, T);
+  const int P = h.prm.P, nt = tri(P), T = periodic_threads(P), images = h.prm.images;
+  const double cycle = h.prm.cycle;
+  if (!(h.per_P == P && h.per_images == images && h.per_cycle == cycle)) {
+    h.per_harm.need((size_t)2 * (images - 1) * nt * sizeof(double2));
+    k_periodic_harm<<<1, PT, (size_t)T * nt * sizeof(double2), h.stream>>>(P, images, cycle, T,
+                                                                           h.per_harm.as<double2>());
+    h.launches++;
+    FMM_LAUNCH();
+    h.per_P = P;
+    h.per_images = images;
+    h.per_cycle = cycle;
+  }
+  k_periodic<<<1, PT, (size_t)2 * nt * sizeof(double2), h.stream>>>(h.M.as<double2>(), h.L.as<double2>(), P, images,
+                                                                    h.per_harm.as<double2>());
   h.launches++;
   FMM_LAUNCH();
 }
