@@ -365,32 +365,44 @@ __global__ void k_mscale16(int ncells, int P, int KP, const double4 *xr, const d
                                      __double2half(v.y - (double)__half2float(hy)));
 }
 
-// A warp per ghost (GH_WARPS per block): the source's multipole moved by the
-// M2M shift f r onto the ghost centre (3d/kernel.h:204-231 for one child,
-// offset ghost - source = f r), scaled like k_mscale16 (1 / R^n, times 2^E)
-// and split into the ghost's FP16 hi / lo row, M16[ncells + g].  Lane m < P
-// generates harmonic column m (ghosts exist for P <= 15, with the
-// tensor-core M2L).
-constexpr int GH_WARPS = 8;
-__global__ void __launch_bounds__(GH_WARPS * 32) k_ghost16(int nghost, const int *gslots, const double4 *xr,
-                                                           const double2 *M, int P, int KP, double cycle, int depth,
-                                                           const unsigned long long *mx, int ncells, __half2 *M16) {
-  extern __shared__ double2 gsh[];  // per warp: harmonics of the shift, then the source multipole
-  const int NT = tri(P), wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * GH_WARPS + wp;
-  if (g >= nghost) return;  // warp-uniform; the kernel has no block barrier
-  double2 *Ysh = gsh + (size_t)wp * 2 * NT, *Msh = Ysh + NT;
-  const int slot = gslots[g];
-  const int s = slot / GHOST_SLOTS, ic = (slot % GHOST_SLOTS) / 4, dlf = slot % 4;
+// Harmonics of the ghost shifts: the shift of image img at finer level lf is
+// f m, f = rint(s) - s with s the image's offset in cell units and m the
+// level's cell radius R0 / 2^lf, the same for every ghost of (img, lf).  A
+// warp per (img, lf), lane m < P generating column m: Y[(ic * nlev + lf) * NT].
+__global__ void __launch_bounds__(32) k_ghost_harm(int nlev, const double4 *xr, int P, double cycle, double2 *Y) {
+  const int key = blockIdx.x, ic = key / nlev, lf = key % nlev, lane = threadIdx.x;
+  const int NT = tri(P);
   const int img = ic < 13 ? ic : ic + 1;
-  const double4 Y = xr[s];
-  const double R0 = xr[0].w, m = scalbn(Y.w, -dlf);
-  const int lf = ilogb(R0) - ilogb(m);
+  const double R0 = xr[0].w, m = scalbn(R0, -lf);
   const int ix = img % 3 - 1, iy = (img / 3) % 3 - 1, iz = img / 9 - 1;
   const double sx = image_shift_units(ix, lf, R0, cycle), sy = image_shift_units(iy, lf, R0, cycle),
                sz = image_shift_units(iz, lf, R0, cycle);
   const Sph sg = sph_of((rint(sx) - sx) * m, (rint(sy) - sy) * m, (rint(sz) - sz) * m);
-  if (lane < P) regular_column(lane, P, sg.r, sg, sg.e, [&](int n, double2 y, double2) { Ysh[tri(n) + lane] = y; });
+  double2 *row = Y + (size_t)key * NT;
+  if (lane < P) regular_column(lane, P, sg.r, sg, sg.e, [&](int n, double2 y, double2) { row[tri(n) + lane] = y; });
+}
+
+// A warp per ghost (GH_WARPS per block): the source's multipole moved by the
+// M2M shift f r onto the ghost centre (3d/kernel.h:204-231 for one child,
+// offset ghost - source = f r, with the shift's harmonics from
+// k_ghost_harm), scaled like k_mscale16 (1 / R^n, times 2^E) and split into
+// the ghost's FP16 hi / lo row, M16[ncells + g].
+constexpr int GH_WARPS = 8;
+__global__ void __launch_bounds__(GH_WARPS * 32) k_ghost16(int nghost, const int *gslots, const double4 *xr,
+                                                           const double2 *M, const double2 *Yh, int nlev, int P,
+                                                           int KP, const unsigned long long *mx, int ncells,
+                                                           __half2 *M16) {
+  extern __shared__ double2 gsh[];  // per warp: the source multipole
+  const int NT = tri(P), wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * GH_WARPS + wp;
+  if (g >= nghost) return;  // warp-uniform; the kernel has no block barrier
+  double2 *Msh = gsh + (size_t)wp * NT;
+  const int slot = gslots[g];
+  const int s = slot / GHOST_SLOTS, ic = (slot % GHOST_SLOTS) / 4, dlf = slot % 4;
+  const double4 Y = xr[s];
+  const double R0 = xr[0].w, m = scalbn(Y.w, -dlf);
+  const int lf = ilogb(R0) - ilogb(m);
+  const double2 *Ysh = Yh + (size_t)(ic * nlev + lf) * NT;
   for (int k = lane; k < NT; k += 32) Msh[k] = M[(long)s * NT + k];
   __syncwarp();
   const double E = scalbn(1.0, m16_exponent(*mx));
@@ -1056,10 +1068,15 @@ void m2l_grouped_pass(Handle &h) {
       h.launches++;
     }
     const long nsl = (long)C * GHOST_SLOTS;
-    k_ghost16<<<(h.g_nghost + GH_WARPS - 1) / GH_WARPS, GH_WARPS * 32, GH_WARPS * 2 * NT * sizeof(double2), s>>>(
-        h.g_nghost, h.g_gmark.as<int>() + 2 * nsl, h.c_xr.as<double4>(), h.M.as<double2>(), P, KP16, cyc, h.depth,
-        &h.counters.as<DevCounters>()->m16_max, C, h.g_m16.as<__half2>());
-    h.launches++;
+    // the shifts' harmonics, per (image, finer level): levels up to the
+    // deepest cell's, whose ghosts sit at most 3 levels below a source
+    const int nlev = h.depth + 4;
+    h.g_gharm.need((size_t)26 * nlev * NT * sizeof(double2));
+    k_ghost_harm<<<26 * nlev, 32, 0, s>>>(nlev, h.c_xr.as<double4>(), P, cyc, h.g_gharm.as<double2>());
+    k_ghost16<<<(h.g_nghost + GH_WARPS - 1) / GH_WARPS, GH_WARPS * 32, GH_WARPS * NT * sizeof(double2), s>>>(
+        h.g_nghost, h.g_gmark.as<int>() + 2 * nsl, h.c_xr.as<double4>(), h.M.as<double2>(), h.g_gharm.as<double2>(),
+        nlev, P, KP16, &h.counters.as<DevCounters>()->m16_max, C, h.g_m16.as<__half2>());
+    h.launches += 2;
     FMM_LAUNCH();
   };
   // same lists, P and form as the last grouping: contract directly
