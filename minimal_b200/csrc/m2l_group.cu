@@ -503,10 +503,8 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
 
 __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, const int *tg_off, const int *tg_gid,
                                                           const int *tg_src, const double *ops, const double *Mt,
-                                                          const double4 *xr, double2 *L, PlanDev pd) {
-  extern __shared__ double smd[];
-  double *Wsm = smd;
-  double *Xsm = smd + pd.wsize;
+                                                          const double4 *xr, double2 *L, PlanDev pd, int nstage) {
+  extern __shared__ __align__(16) double smd[];  // nstage x (operator, gathered multipoles); then the reduction
   const int tile = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int pc[GP_MAXP], wo[GP_MAXP];
 #pragma unroll
@@ -520,17 +518,37 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
 #pragma unroll
     for (int cb = 0; cb < 4; cb++) acc[p][cb][0] = acc[p][cb][1] = 0;
   const int KP = pd.KP;
+  const size_t sstride = (size_t)pd.wsize + (size_t)KP * XS;  // doubles per stage (even: 16-byte rows)
   const int ar = lane >> 2, ak = lane & 3;
-  for (int g = tg_off[tile]; g < tg_off[tile + 1]; g++) {
+  // group g's operator and its 32 gathered multipoles into stage b, as
+  // asynchronous copies (absent targets: zeros)
+  auto issue = [&](int g, int b) {
+    double *Wd = smd + (size_t)b * sstride, *Xd = Wd + pd.wsize;
     const double *Wg = ops + (size_t)tg_gid[g] * pd.wsize;
-    __syncthreads();
-    for (int i = tid; i < pd.wsize / 2; i += blockDim.x) ((double2 *)Wsm)[i] = ((const double2 *)Wg)[i];
+    for (int i = tid; i < pd.wsize / 2; i += blockDim.x) tc::cp_async16(Wd + 2 * i, Wg + 2 * i, 16u);
     for (int i = tid; i < GP_TILE * KP; i += blockDim.x) {
       const int col = i / KP, k = i - col * KP;
       const int s = tg_src[(long)g * GP_TILE + col];
-      Xsm[k * XS + col] = s >= 0 ? Mt[(long)s * KP + k] : 0.0;
+      tc::cp_async8(Xd + k * XS + col, Mt + (long)(s >= 0 ? s : 0) * KP + k, s >= 0 ? 8u : 0u);
+    }
+    tc::cp_async_commit();
+  };
+  const int g0 = tg_off[tile], g1 = tg_off[tile + 1];
+  if (nstage == 2 && g0 < g1) issue(g0, 0);
+  for (int g = g0; g < g1; g++) {
+    // two stages: the next group's copies run while this one is contracted
+    const int b = nstage == 2 ? (g - g0) & 1 : 0;
+    if (nstage != 2) {
+      issue(g, 0);
+      tc::cp_async_wait_all();
+    } else if (g + 1 < g1) {
+      issue(g + 1, b ^ 1);
+      tc::cp_async_wait_1();
+    } else {
+      tc::cp_async_wait_all();
     }
     __syncthreads();
+    const double *Wsm = smd + (size_t)b * sstride, *Xsm = Wsm + pd.wsize;
 #pragma unroll
     for (int p = 0; p < GP_MAXP; p++) {
       if (pc[p] < 0) continue;
@@ -543,6 +561,7 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
         for (int cb = 0; cb < 4; cb++) dmma(acc[p][cb][0], acc[p][cb][1], a, xb[cb * 8]);
       }
     }
+    __syncthreads();  // stage b is free for group g + 2
   }
   // reduce the pieces into Y[row][col] (rank 0 stores, higher ranks add)
   double *Y = smd;
@@ -583,9 +602,9 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
 // 128-byte swizzled K-major layout, are staged in shared memory, and one
 // thread issues the three products hi*hi + hi*lo + lo*hi per K step of 16
 // (tcgen05.mma kind::f16), accumulating in FP32 in tensor memory.
-//   producer warp: per group, waits for its stage to be free, then one bulk
-//     copy (operator) and 4-row TMA gathers (multipoles) land on the stage's
-//     barrier; two stages;
+//   producer warps: per group, wait for its stage to be free, then one bulk
+//     copy (operator) and 16-byte cp.async copies of the gathered multipole
+//     rows land on the stage's barriers; two stages;
 //   MMA warp: waits for the stage, issues the MMAs, commits the stage back;
 //     two TMEM accumulators alternate every `flush_every` groups;
 //   epilogue warps: fold each finished accumulator into a double-FP32
@@ -942,10 +961,10 @@ PlanDev plan_dev(const PlanCache &pc) {
   return d;
 }
 
-size_t gemm64_smem(const GroupPlan &g) {
+size_t gemm64_smem(const GroupPlan &g, int nstage = 1) {
   const size_t stage = (size_t)g.wsize + (size_t)g.KP * XS;
   const size_t red = (size_t)g.nrb * 8 * GP_TILE;
-  return std::max(stage, red) * sizeof(double);
+  return std::max(nstage * stage, red) * sizeof(double);
 }
 
 constexpr size_t TC_SMEM_MAX = 227 * 1024;  // opt-in shared memory per CTA on sm_100
@@ -988,7 +1007,7 @@ bool m2l_grouped_available(int P) {
 }
 
 void m2l_grouped_set_attributes() {
-  cudaFuncSetAttribute(k_gemm64, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_gemm64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
   cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
 }
 
@@ -1015,9 +1034,11 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
     FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
     h.g_used_tc = true;
   } else {
-    k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                            h.g_ops.as<double>(), h.g_mt.as<double>(),
-                                                            h.c_xr.as<double4>(), h.L.as<double2>(), pd);
+    // two pipeline stages where they fit in shared memory (P <= 11), else one
+    const int nst = gemm64_smem(gp, 2) <= TC_SMEM_MAX ? 2 : 1;
+    k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp, nst), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                                 h.g_ops.as<double>(), h.g_mt.as<double>(),
+                                                                 h.c_xr.as<double4>(), h.L.as<double2>(), pd, nst);
   }
   h.launches++;
 }

@@ -140,6 +140,12 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t 
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
                : "memory");
 }
+// 8-byte asynchronous copy global -> shared (through L1); src_bytes = 0
+// writes zeros.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 // Arrival on the barrier once all of this thread's earlier cp.async copies
