@@ -1034,7 +1034,7 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
     FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
     h.g_used_tc = true;
   } else {
-    // two pipeline stages where they fit in shared memory (P <= 11), else one
+    // two pipeline stages where they fit in shared memory (P <= 12), else one
     const int nst = gemm64_smem(gp, 2) <= TC_SMEM_MAX ? 2 : 1;
     k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp, nst), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
                                                                  h.g_ops.as<double>(), h.g_mt.as<double>(),
