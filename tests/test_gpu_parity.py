@@ -211,3 +211,20 @@ def test_argument_and_state_errors():
     assert e.value.code == -4
     fmm.evaluate()
     assert np.isfinite(fmm.bodies()).all()
+
+
+@pytest.mark.parametrize("P", [12, 13])
+def test_fp64_contraction_stage_counts_vs_oracle(port, P):
+    """The FP64 grouped M2L stages each group's operator and gathered
+    multipoles with asynchronous copies, in two pipeline stages where they fit
+    in shared memory (P <= 12) and one above: both paths match the reference
+    restatement within the FP64 form's 1e-12."""
+    from minimal_b200 import FMM
+    from minimal_b200.bodies import uniform_bodies
+
+    xq = uniform_bodies(6000, 9)
+    ref = port.fmm(xq, P, 32, 0.4)
+    fmm = FMM(P=P, ncrit=32, theta=0.4)
+    fmm.set_bodies(xq)
+    fmm.evaluate()
+    check_results(fmm.bodies(), ref)

@@ -172,3 +172,46 @@ def test_periodic_larger_system_vs_ewald():
     assert f64 < 1e-3
     assert fmx <= 1.1 * f64 + 1e-7
     assert np.array_equal(res["fp64"][:, :4], res["mixed"][:, :4])
+
+
+def test_mixed_periodic_lists_untouched_by_ghosts():
+    """The mixed form points image entries with a tiny fractional offset at
+    ghost sources; it does so on its own copy of the walk's pairs, so the
+    lists exported after a mixed evaluation are the FP64 form's (the
+    reference's)."""
+    from minimal_b200 import FMM, drand48_bodies
+
+    cyc = 2 * np.pi
+    xq = drand48_bodies(20000, 3, "3dp", cyc)
+    lists = {}
+    for prec in ("fp64", "mixed"):
+        fmm = FMM(P=8, ncrit=32, theta=0.4, images=3, cycle=cyc, precision=prec)
+        fmm.set_bodies(xq)
+        fmm.evaluate()
+        lists[prec] = fmm.lists()
+        fmm.evaluate()  # the grouping again, on the same lists
+        again = fmm.lists()
+        for k in again:
+            assert np.array_equal(again[k], lists[prec][k]), k
+    for k in lists["fp64"]:
+        assert np.array_equal(lists["mixed"][k], lists["fp64"][k]), k
+
+
+def test_far_image_sums_follow_the_parameters():
+    """The far images' harmonic sums are kept between evaluations for the
+    (P, images, cycle) they were made for: after a change of the period or
+    the image count an evaluation gives the same bits as a fresh handle."""
+    from minimal_b200 import FMM, drand48_bodies
+
+    xq = drand48_bodies(5000, 4, "3dp", 2 * np.pi)
+    f = FMM(P=8, ncrit=32, theta=0.4, images=3, cycle=2 * np.pi)
+    f.set_bodies(xq)
+    f.evaluate()
+    for images, cyc in ((3, 2 * np.pi * 1.25), (4, 2 * np.pi * 1.25), (2, 2 * np.pi)):
+        f.set_params(images=images, cycle=cyc)
+        f.set_bodies(xq)
+        f.evaluate()
+        g = FMM(P=8, ncrit=32, theta=0.4, images=images, cycle=cyc)
+        g.set_bodies(xq)
+        g.evaluate()
+        assert np.array_equal(f.bodies(), g.bodies())
