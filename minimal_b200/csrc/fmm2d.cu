@@ -21,6 +21,8 @@
 //              target body, q log(1/R) and q dX / R^2 (2d/kernel.h:12-31);
 //   periodic   one warp: the 72 root M2Ls and the 8-copy M2M per image level
 //              (2dp/traverse_eager.h:46-93).
+#include <type_traits>
+
 #include "fmm.cuh"
 #include "harmonics.cuh"
 
@@ -184,6 +186,62 @@ __global__ void __launch_bounds__(W2 * 32) k2_m2l(int ncells, const int *off, co
   if (lane < P) L[(long)t * P + lane] = acc;
 }
 
+// The same M2L with a lane per list entry (orders P <= 16): with
+// q_m = (m-1)!/z^m, the terms of m2l_term are L[n] += (-1)^n M_k q_(n+k) for
+// n + k >= 1 and L[0] -= M_0 log z, so one lane evaluates a whole entry --
+// one reciprocal, one logarithm, the q_m by the recurrence
+// q_(m+1) = q_m m / z and P^2 complex products, summed along n + k = m --
+// with every coefficient in registers (P is a compile-time constant), while
+// the warp's lanes take the target's entries 32 at a time.  The lanes' sums
+// are then added in a fixed butterfly order (deterministic).  The operations
+// are those of m2l_term in another order: the expansions agree with it, and
+// with the reference, to rounding.
+template <int P>
+__global__ void __launch_bounds__(W2 * 32) k2_m2l_lane(int ncells, const int *off, const u32 *ent, const double4 *xr,
+                                                       const double2 *M, double2 *L, double cycle) {
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * W2 + wid;
+  if (t >= ncells) return;  // warp-uniform
+  const double4 X = xr[t];
+  double2 acc[P];
+#pragma unroll
+  for (int n = 0; n < P; n++) acc[n] = make_double2(0, 0);
+  for (int e = off[t] + lane; e < off[t + 1]; e += 32) {
+    const u32 en = ent[e];
+    const int s = (int)(en & IDX_MASK);
+    double sx, sy;
+    img_shift(en >> IMG_SHIFT, cycle, sx, sy);
+    const double4 Y = xr[s];
+    const double2 Z = make_double2(X.x - Y.x - sx, X.y - Y.y - sy);
+    double2 Mk[P];
+#pragma unroll
+    for (int k = 0; k < P; k++) Mk[k] = M[(long)s * P + k];
+    const double2 iz = crecip(Z);
+    acc[0] = csub(acc[0], cmul(Mk[0], clog2(Z)));
+    double2 q = iz;  // q_1
+#pragma unroll
+    for (int m = 1; m <= 2 * P - 2; m++) {
+#pragma unroll
+      for (int n = 0; n < P; n++) {
+        const int k = m - n;
+        if (k < 0 || k >= P) continue;
+        const double2 term = cmul(Mk[k], q);
+        acc[n] = (n & 1) ? csub(acc[n], term) : cadd(acc[n], term);
+      }
+      if (m < 2 * P - 2) q = cmulr(cmul(q, iz), (double)m);
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < P; n++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      acc[n].x += __shfl_xor_sync(0xffffffffu, acc[n].x, o);
+      acc[n].y += __shfl_xor_sync(0xffffffffu, acc[n].y, o);
+    }
+    if (lane == (n & 31)) L[(long)t * P + n] = acc[n];
+  }
+}
+
 // Far periodic images of a 2dp system (2dp/traverse_eager.h:46-93): per
 // image level, the 72 M2Ls from the super-cell (the root's multipole, at the
 // root's centre) shifted by (3 ix + cx, 3 iy + cy) cycles into the root's L,
@@ -289,43 +347,68 @@ __global__ void __launch_bounds__(W2 * 32) k2_l2p(const int *leaves, int nleaves
   }
 }
 
-// P2P (2d/kernel.h:12-31; 2dp image shift) over the ordered P2P lists: warp
-// per target leaf, lane per target body; each source leaf's sums are added
-// to the body as one term, as the reference's per-pair calls do.  Writes
-// out (the first writer).
+// P2P (2d/kernel.h:12-31; 2dp: the image shift of each list entry):
+// p += q log(1/r), F -= q (dx, dy) / r^2 over the target leaf's ordered near
+// list, each source leaf's sums added to the body as one term, as the
+// reference's per-pair calls do; writes out (the first writer).  A warp per
+// target leaf.  For leaves of up to 16
+// bodies the lanes are (target i, entry group g), G = floor(32 / nb) groups
+// taking the list entries round-robin, and the groups' sums are added in
+// group order at the end (deterministic); larger leaves take a lane per
+// target.  log(1/r) is formed as -log(r^2) / 2 and the force with one
+// reciprocal of r^2 (the reference's quantities, to rounding).
 __global__ void __launch_bounds__(W2 * 32) k2_p2p(const int *leaves, int nleaves, const int *begin, const int *count,
                                                   const int *off, const u32 *ent, const double4 *src, double4 *out,
                                                   double cycle) {
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * W2 + wid;
-  if (w >= nleaves) return;
+  if (w >= nleaves) return;  // warp-uniform
   const int c = leaves[w], b0 = begin[c], nb = count[c];
-  for (int t = lane; t - lane < nb; t += 32) {
-    const bool ok = t < nb;
+  const int e0 = off[c], e1 = off[c + 1];
+  const int G = nb <= 16 ? 32 / nb : 1;  // entry groups
+  const int span = nb <= 16 ? nb : 32;   // targets per pass
+  const int i = lane % span, g = lane / span;
+  const bool lane_ok = g < G;
+  for (int tb = 0; tb < nb; tb += span) {
+    const int t = tb + i;
+    const bool ok = lane_ok && t < nb;
     const double4 T = ok ? src[b0 + t] : make_double4(0, 0, 0, 0);
     double p = 0, fx = 0, fy = 0;
-    for (int e = off[c]; e < off[c + 1]; e++) {
-      const u32 en = ent[e];
-      const int s = (int)(en & IDX_MASK);
-      double sx, sy;
-      img_shift(en >> IMG_SHIFT, cycle, sx, sy);
-      double pp = 0, px = 0, py = 0;
-      for (int j = begin[s]; j < begin[s] + count[s]; j++) {
-        const double4 S = src[j];
-        const double dx = T.x - S.x - sx, dy = T.y - S.y - sy;
-        const double R2 = dx * dx + dy * dy;
-        if (R2 != 0) {
-          const double invR = 1 / sqrt(R2);
-          pp += S.w * log(invR);
-          px += dx * S.w / R2;
-          py += dy * S.w / R2;
+    if (lane_ok) {
+      for (int e = e0 + g; e < e1; e += G) {
+        const u32 en = ent[e];
+        const int s = (int)(en & IDX_MASK);
+        double sx, sy;
+        img_shift(en >> IMG_SHIFT, cycle, sx, sy);
+        double pp = 0, px = 0, py = 0;
+        for (int j = begin[s]; j < begin[s] + count[s]; j++) {
+          const double4 S = src[j];
+          const double dx = T.x - S.x - sx, dy = T.y - S.y - sy;
+          const double R2 = dx * dx + dy * dy;
+          if (R2 != 0) {
+            const double invR2 = 1 / R2;
+            pp -= 0.5 * S.w * log(R2);
+            px += dx * S.w * invR2;
+            py += dy * S.w * invR2;
+          }
         }
+        p += pp;
+        fx -= px;
+        fy -= py;
       }
-      p += pp;
-      fx -= px;
-      fy -= py;
     }
-    if (ok) out[b0 + t] = make_double4(p, fx, fy, 0.0);
+    // group 0 adds the other groups' sums in group order
+    for (int gg = 1; gg < G; gg++) {
+      const int from = (gg * span + i) & 31;
+      const double vp = __shfl_sync(0xffffffffu, p, from), vx = __shfl_sync(0xffffffffu, fx, from),
+                   vy = __shfl_sync(0xffffffffu, fy, from);
+      if (g == 0) {
+        p += vp;
+        fx += vx;
+        fy += vy;
+      }
+    }
+    if (ok && g == 0) out[b0 + t] = make_double4(p, fx, fy, 0.0);
   }
 }
 
@@ -404,9 +487,33 @@ void m2l_pass_2d(Handle &h) {
   const int P = h.prm.P;
   h.L.need((size_t)h.ncells * P * sizeof(double2));
   order_m2l_lists(h);
-  k2_m2l<<<grid_for(h.ncells, W2), W2 * 32, 0, h.stream>>>(h.ncells, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
-                                                           h.c_xr.as<double4>(), h.M.as<double2>(), h.L.as<double2>(),
-                                                           P, h.prm.images ? h.prm.cycle : 0.0);
+  const double cyc = h.prm.images ? h.prm.cycle : 0.0;
+  const int g = grid_for(h.ncells, W2);
+  auto lane_form = [&](auto pc) {
+    constexpr int PP = decltype(pc)::value;
+    k2_m2l_lane<PP><<<g, W2 * 32, 0, h.stream>>>(h.ncells, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(),
+                                                h.c_xr.as<double4>(), h.M.as<double2>(), h.L.as<double2>(), cyc);
+  };
+  switch (P) {
+    case 2: lane_form(std::integral_constant<int, 2>{}); break;
+    case 3: lane_form(std::integral_constant<int, 3>{}); break;
+    case 4: lane_form(std::integral_constant<int, 4>{}); break;
+    case 5: lane_form(std::integral_constant<int, 5>{}); break;
+    case 6: lane_form(std::integral_constant<int, 6>{}); break;
+    case 7: lane_form(std::integral_constant<int, 7>{}); break;
+    case 8: lane_form(std::integral_constant<int, 8>{}); break;
+    case 9: lane_form(std::integral_constant<int, 9>{}); break;
+    case 10: lane_form(std::integral_constant<int, 10>{}); break;
+    case 11: lane_form(std::integral_constant<int, 11>{}); break;
+    case 12: lane_form(std::integral_constant<int, 12>{}); break;
+    case 13: lane_form(std::integral_constant<int, 13>{}); break;
+    case 14: lane_form(std::integral_constant<int, 14>{}); break;
+    case 15: lane_form(std::integral_constant<int, 15>{}); break;
+    case 16: lane_form(std::integral_constant<int, 16>{}); break;
+    default:  // larger orders: a warp per entry, a lane per coefficient
+      k2_m2l<<<g, W2 * 32, 0, h.stream>>>(h.ncells, h.m2l_off.as<int>(), h.m2l_ent.as<u32>(), h.c_xr.as<double4>(),
+                                          h.M.as<double2>(), h.L.as<double2>(), P, cyc);
+  }
   h.launches++;
   FMM_LAUNCH();
 }
