@@ -364,6 +364,9 @@ void build_lists(Handle &h) {
 // Lists in the reference's cell numbering (host arrays, CSR over ref index).
 void export_lists(Handle &h, int *m2l_off, int *m2l_src, int *m2l_img, int *p2p_off, int *p2p_src, int *p2p_img) {
   order_m2l_lists(h);
+  // the ordering runs on the handle's (non-blocking) stream: the plain
+  // copies below must wait for it
+  FMM_CUDA(cudaStreamSynchronize(h.stream));
   const int C = h.ncells;
   std::vector<int> ref(C), moff(C + 1), poff(C + 1);
   std::vector<u32> ment(h.n_m2l > 0 ? h.n_m2l : 1), pent(h.n_p2p > 0 ? h.n_p2p : 1);
