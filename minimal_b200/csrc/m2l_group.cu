@@ -11,19 +11,27 @@
 // with conj(M) folded in), it is a 2NT x 2NT real matrix, zero for j+n >= P.
 //
 // Pipeline per evaluation:
-//   k_gkeys    key of every M2L entry (periodic images, far-out offsets or
-//              level gaps beyond the key range stay "residual" and are done
-//              by the direct-form kernel), occupancy of the key space;
+//   keys       the walk's key of every M2L entry, or k_gkeys (ordered
+//              lists; mixed-form periodic entries, where image entries with
+//              a tiny fractional offset become ghost-source entries with
+//              free-space keys); periodic image entries carry the image and
+//              level in their key; far-out offsets or level gaps beyond the
+//              key range stay "residual" and are done by the direct-form
+//              kernel; occupancy of the key space;
 //   scan       group ids of the occupied keys;
-//   k_gops     the realified operator of every group (FP64);
+//   k_gops     the realified operator of every group not yet cached (FP64;
+//              k_gops16: FP16 hi/lo images for the tensor core);
 //   tiles      targets with grouped entries sorted by (level, child rank) and
 //              cut into tiles (32 targets for DMMA, 128 for tcgen05); the
 //              (tile, group) pairs that hold entries are marked, scanned into
 //              segment ids and filled with the source cell of every tile slot;
-//   k_gemm64   one CTA (8 warps) per tile: for each group of the tile, stage
-//              the operator and the 32 gathered scaled multipoles in shared
-//              memory and accumulate with FP64 DMMA (mma.m8n8k4) in registers;
-//              then reduce the warps' pieces, unscale and store L.
+//   k_gemm64   one CTA (8 warps) per tile: for each group of the tile, the
+//              operator and the 32 gathered scaled multipoles are copied into
+//              shared memory with cp.async (two stages: the next group's
+//              copies run under this group's contraction), accumulated with
+//              FP64 DMMA (mma.m8n8k4) in registers; then the warps' pieces
+//              are reduced, unscaled and stored in L;
+//   k_m2l_tc   the mixed form's contraction on tcgen05 (below).
 #include <map>
 #include <mutex>
 #include <unordered_map>
