@@ -1,6 +1,7 @@
 // GPU interaction-list builder: the reference's dual-tree traversal
 // (3d/traverse_eager.h:147-165, recorded as lists by 3d/traverse_lazy.h:27-44;
-// periodic shifts 3dp/traverse_lazy.h:39-58 and the 27-image loop :276-293)
+// periodic shifts 3dp/traverse_lazy.h:39-58 and the 27-image loop
+// 3dp/traverse_lazy.h:128-134)
 // run breadth first over a frontier of (target, source, image) cell pairs.
 //
 // Each step applies the reference's branch rules to every pair of the

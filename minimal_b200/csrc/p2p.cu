@@ -1,12 +1,16 @@
 // Near field in FP64 (3d/kernel.h:122-150; periodic shift 3dp/kernel.h:133)
 // and the direct-summation check (3d/traverse_eager.h:193-202).
 //
-// P2P: one warp per target leaf; each lane keeps up to two target bodies in
-// registers while the warp streams every source leaf of the target's P2P
-// list through a 32-body shared-memory tile (coalesced 32-byte loads, all
-// lanes then read the same body: a broadcast).  Pairs at distance zero are
-// skipped as in the reference.  P2P is the first writer of the outputs, so it
-// stores p and F; L2P adds to them later.
+// P2P: k_p2p_cta (target leaves of up to 256 bodies, both forms) -- one CTA
+// per target leaf: the leaf's P2P list is taken in chunks of whole source
+// leaves staged into shared memory, shifted into the target leaf's frame
+// (the FP32 form scaled and interleaved into source pairs for packed FP32x2
+// sweeps), and the threads, two targets each, sweep contiguous parts of the
+// chunk; their partial sums are reduced in a fixed order.  Larger leaves take
+// k_p2p / k_p2p_f32: one warp per target leaf streaming every source leaf
+// through a 32-body shared-memory tile (coalesced loads, then a broadcast).
+// Pairs at distance zero are skipped as in the reference.  P2P is the first
+// writer of the outputs, so it stores p and F; L2P adds to them later.
 #include <type_traits>
 
 #include "fmm.cuh"
