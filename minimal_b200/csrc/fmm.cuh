@@ -178,6 +178,7 @@ struct Handle {
   // far-image harmonic sums (periodic.cu), kept for the (P, images, cycle)
   // they were made for
   Buf per_harm;
+  Buf per_part;  // partial charge sums (the mixed form's root monopole)
   Buf g_gharm;  // harmonics of the ghost shifts, per (image, finer level)
   int per_P = 0, per_images = 0;
   double per_cycle = 0;

@@ -145,6 +145,35 @@ int periodic_threads(int P) {
 // ---- dipole correction
 constexpr int DB = 256;
 
+// The root's monopole for the far images of the mixed form: the total
+// charge, summed in FP64 in a fixed order (block partial sums, then one block
+// over the partials in block order).  The mixed upward pass forms it from
+// FP32 products, and the far images' lattice sums multiply a spurious net
+// charge by their growing image shells: at 60,000 neutral bodies, P = 10,
+// the potentials then drifted from the FP64 form's by 5.9e-7, 7.9e-6 and
+// 7.0e-4 with 1, 2 and 4 image layers (forces unaffected: the shift is
+// nearly constant).
+__global__ void k_charge_partial(const double4 *src, long n, double *part) {
+  __shared__ double red[DB];
+  double q = 0;
+  for (long i = (long)blockIdx.x * DB + threadIdx.x; i < n; i += (long)gridDim.x * DB) q += src[i].w;
+  red[threadIdx.x] = q;
+  __syncthreads();
+  for (int s = DB / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void k_root_monopole(const double *part, int nblk, double2 *M) {
+  if (threadIdx.x == 0) {
+    double q = 0;
+    for (int b = 0; b < nblk; b++) q += part[b];
+    M[0] = make_double2(q, 0.0);  // M_0^0 of the root (cell 0): the total charge
+  }
+}
+
 __global__ void k_dipole_partial(const double4 *src, long n, double *part) {
   __shared__ double red[3][DB];
   double d[3] = {0, 0, 0};
@@ -353,6 +382,13 @@ void periodic_pass(Handle &h) {
     h.per_P = P;
     h.per_images = images;
     h.per_cycle = cycle;
+  }
+  if (h.prm.precision == EXAFMM_MIXED) {  // the root's monopole in FP64 (see k_charge_partial)
+    const int nblk = 148;
+    h.per_part.need(nblk * sizeof(double));
+    k_charge_partial<<<nblk, DB, 0, h.stream>>>(h.src.as<double4>(), h.n, h.per_part.as<double>());
+    k_root_monopole<<<1, 32, 0, h.stream>>>(h.per_part.as<double>(), nblk, h.M.as<double2>());
+    h.launches += 2;
   }
   k_periodic<<<1, PT, (size_t)2 * nt * sizeof(double2), h.stream>>>(h.M.as<double2>(), h.L.as<double2>(), P, images,
                                                                     h.per_harm.as<double2>());

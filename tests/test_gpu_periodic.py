@@ -215,3 +215,26 @@ def test_far_image_sums_follow_the_parameters():
         g.set_bodies(xq)
         g.evaluate()
         assert np.array_equal(f.bodies(), g.bodies())
+
+
+def test_mixed_potentials_do_not_drift_with_image_layers():
+    """The far images multiply the root's net charge by image shells that grow
+    with every layer; the mixed form takes the root's monopole as the FP64
+    total charge, so its potentials stay as close to the FP64 form's with 4
+    image layers as with 1 (an FP32 root monopole drifted by 7e-4 at 4
+    layers)."""
+    from minimal_b200 import FMM, drand48_bodies
+
+    cyc = 2 * np.pi
+    xq = drand48_bodies(30000, 6, "3dp", cyc)
+    diff = {}
+    for images in (1, 4):
+        out = {}
+        for prec in ("fp64", "mixed"):
+            f = FMM(P=8, ncrit=64, theta=0.4, images=images, cycle=cyc, precision=prec)
+            f.set_bodies(xq)
+            f.evaluate()
+            f.dipole_correction()
+            out[prec] = f.bodies()
+        diff[images] = rel_l2(out["mixed"][:, 4], out["fp64"][:, 4])
+    assert diff[4] < 3 * diff[1] + 1e-7, diff
