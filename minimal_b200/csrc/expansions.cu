@@ -162,11 +162,16 @@ __device__ __forceinline__ void regular_all_f(int Prt, const SphF &g, float2 e1,
   }
 }
 
+// Binary exponent of a leaf radius (clamped): the FP32 expansion kernels work
+// in units of 2^e, where the radius lies in [1, 2).
+__device__ __forceinline__ int leaf_exponent(double R) { return R > 0 ? max(-100, min(100, ilogb(R))) : 0; }
+
 // P2M in FP32: lane per body, each coefficient reduced over the warp by a
 // float butterfly, chunks of 32 bodies summed in FP64.
 template <int PT>
 __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int nleaves, const int *begin,
-                                                        const int *count, const float4 *srcf, double2 *M, int Prt) {
+                                                        const int *count, const double4 *xr, const float4 *srcf,
+                                                        double2 *M, int Prt) {
   extern __shared__ double2 sh[];
   const int P = PT > 0 ? PT : Prt;
   const int nt = tri(P);
@@ -177,11 +182,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int n
   for (int k = lane; k < nt; k += 32) acc[k] = make_double2(0, 0);
   __syncwarp();
   const int c = leaves[w];
+  const int ex = leaf_exponent(xr[c].w);
+  const float sc = exp2f((float)-ex);  // coordinates in units where the leaf radius is in [1, 2)
   const int b0 = begin[c], nb = count[c];
   for (int t = 0; t < nb; t += 32) {
     const bool ok = t + lane < nb;
     const float4 B = ok ? srcf[b0 + t + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const SphF g = sph_of_f(B.x, B.y, B.z);
+    const SphF g = sph_of_f(B.x * sc, B.y * sc, B.z * sc);
     regular_all_f<PT, false>(P, g, make_float2(g.e.x, -g.e.y), [&](int n, int m, float2 Y, float2) {
       float x = B.w * Y.x, y = B.w * Y.y;
 #pragma unroll
@@ -196,7 +203,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32(const int *leaves, int n
     });
   }
   __syncwarp();
-  for (int k = lane; k < nt; k += 32) M[(long)c * nt + k] = acc[k];
+  for (int k = lane; k < nt; k += 32) {  // back to the input units: M_n = M~_n R_s^n (exact)
+    const int n = order_of(k);
+    M[(long)c * nt + k] = make_double2(scalbn(acc[k].x, ex * n), scalbn(acc[k].y, ex * n));
+  }
 }
 
 // P2M in FP32 for a compile-time order: each lane writes its body's q Y
@@ -209,7 +219,8 @@ constexpr size_t p2m_t_smem(int nt) { return WARPS * (nt * sizeof(double2) + 32 
 
 template <int PT>
 __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32t(const int *leaves, int nleaves, const int *begin,
-                                                         const int *count, const float4 *srcf, double2 *M) {
+                                                         const int *count, const double4 *xr, const float4 *srcf,
+                                                         double2 *M) {
   constexpr int NT = PT * (PT + 1) / 2, ROW = P2M_ROW;
   extern __shared__ double2 sh[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -220,11 +231,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32t(const int *leaves, int 
   int *rowidx = (int *)((float2 *)(sh + WARPS * NT) + WARPS * 32 * ROW) + wid * 32;
   for (int k = lane; k < NT; k += 32) acc[k] = make_double2(0, 0);
   const int c = leaves[w];
+  const int ex = leaf_exponent(xr[c].w);
+  const float sc = exp2f((float)-ex);  // coordinates in units where the leaf radius is in [1, 2)
   const int b0 = begin[c], nb = count[c];
   for (int t = 0; t < nb; t += 32) {
     const bool ok = t + lane < nb;
     const float4 B = ok ? srcf[b0 + t + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const SphF g = sph_of_f(B.x, B.y, B.z);
+    const SphF g = sph_of_f(B.x * sc, B.y * sc, B.z * sc);
     int gen = 0;  // terms generated so far (a constant at every unrolled step)
     __syncwarp();
     regular_all_f<PT, false>(PT, g, make_float2(g.e.x, -g.e.y), [&](int n, int m, float2 Y, float2) {
@@ -251,15 +264,18 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32t(const int *leaves, int 
     });
   }
   __syncwarp();
-  for (int k = lane; k < NT; k += 32) M[(long)c * NT + k] = acc[k];
+  for (int k = lane; k < NT; k += 32) {  // back to the input units: M_n = M~_n R_s^n (exact)
+    const int n = order_of(k);
+    M[(long)c * NT + k] = make_double2(scalbn(acc[k].x, ex * n), scalbn(acc[k].y, ex * n));
+  }
 }
 
 // L2P in FP32: lane per body, the leaf's local expansion broadcast from
 // shared memory as float; p and F added to the FP64 results.
 template <int PT>
 __global__ void __launch_bounds__(WARPS * 32, L2P_F32_MIN_BLOCKS) k_l2p_f32(const int *leaves, int nleaves, const int *begin,
-                                                        const int *count, const float4 *srcf, const double2 *L,
-                                                        double4 *out, int Prt) {
+                                                        const int *count, const double4 *xr, const float4 *srcf,
+                                                        const double2 *L, double4 *out, int Prt) {
   extern __shared__ float2 shf[];
   const int P = PT > 0 ? PT : Prt;
   const int nt = tri(P);
@@ -267,10 +283,16 @@ __global__ void __launch_bounds__(WARPS * 32, L2P_F32_MIN_BLOCKS) k_l2p_f32(cons
   const int w = blockIdx.x * WARPS + wid;
   if (w >= nleaves) return;
   const int c = leaves[w];
+  // coordinates in units where the leaf radius is in [1, 2), and the local
+  // expansion with them, L~_n = L_n R_s^n (exact powers of two): the FP32
+  // terms stay in range at any domain size
+  const int ex = leaf_exponent(xr[c].w);
+  const float sc = exp2f((float)-ex);
   float2 *Lc = shf + wid * nt;
   for (int k = lane; k < nt; k += 32) {
     const double2 l = L[(long)c * nt + k];
-    Lc[k] = make_float2((float)l.x, (float)l.y);
+    const int n = order_of(k);
+    Lc[k] = make_float2((float)scalbn(l.x, ex * n), (float)scalbn(l.y, ex * n));
   }
   __syncwarp();
   const int b0 = begin[c], nb = count[c];
@@ -278,7 +300,7 @@ __global__ void __launch_bounds__(WARPS * 32, L2P_F32_MIN_BLOCKS) k_l2p_f32(cons
     const int b = b0 + t + lane;
     const bool ok = t + lane < nb;
     const float4 B = ok ? srcf[b] : make_float4(1.f, 0.f, 0.f, 0.f);
-    const SphF g = sph_of_f(B.x, B.y, B.z);
+    const SphF g = sph_of_f(B.x * sc, B.y * sc, B.z * sc);
     float pot = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
     regular_all_f<PT, true>(P, g, g.e, [&](int n, int m, float2 Y, float2 dY) {
       const float2 l = Lc[tri(n) + m];
@@ -304,11 +326,11 @@ __global__ void __launch_bounds__(WARPS * 32, L2P_F32_MIN_BLOCKS) k_l2p_f32(cons
           fy += cp / r / st * s2;
         }
       }
-      double4 &d = out[b];
+      double4 &d = out[b];  // the gradient back to the input units
       d.x += pot;
-      d.y += fx;
-      d.z += fy;
-      d.w += fz;
+      d.y += fx * sc;
+      d.z += fy * sc;
+      d.w += fz * sc;
     }
   }
 }
@@ -806,12 +828,12 @@ void upward_pass(Handle &h, cudaStream_t s) {
     const size_t sm = WARPS * nt * sizeof(double2);
     auto args = [&](auto kernel) {
       kernel<<<grid, block, sm, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
-                                     h.srcf.as<float4>(), h.M.as<double2>(), P);
+                                     h.c_xr.as<double4>(), h.srcf.as<float4>(), h.M.as<double2>(), P);
     };
     const size_t smt = p2m_t_smem(nt);
     auto argst = [&](auto kernel) {
       kernel<<<grid, block, smt, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
-                                      h.srcf.as<float4>(), h.M.as<double2>());
+                                      h.c_xr.as<double4>(), h.srcf.as<float4>(), h.M.as<double2>());
     };
     switch (P) {
 #define EXAFMM_P2M_CASE(p) \
@@ -878,7 +900,8 @@ void downward_pass(Handle &h, cudaStream_t s, cudaEvent_t before_l2p) {
     const size_t sm = WARPS * nt * sizeof(float2);
     auto args = [&](auto kernel) {
       kernel<<<grid, block, sm, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
-                                     h.srcf.as<float4>(), h.L.as<double2>(), h.out.as<double4>(), P);
+                                     h.c_xr.as<double4>(), h.srcf.as<float4>(), h.L.as<double2>(),
+                                     h.out.as<double4>(), P);
     };
     switch (P) {
 #define EXAFMM_L2P_CASE(p) \

@@ -120,3 +120,35 @@ def test_mixed_high_orders_stay_correct(P):
     g.evaluate()
     p6, f6, _ = errors(g, 8000, 200)
     assert fm <= 2 * f6 + 1e-6 and pm <= 2 * p6 + 1e-6
+
+
+@pytest.mark.parametrize("P", [10, 16, 18])
+@pytest.mark.parametrize("scale", [1e-6, 1e6])
+def test_mixed_is_scale_free(P, scale):
+    """A domain scaled by s gives potentials scaled by 1/s and forces by
+    1/s^2: the FP32 P2M and L2P work in units of each leaf's radius (a power
+    of two), so their terms r^n and L_n stay in FP32 range whatever the
+    domain's size.  P=10 covers the tensor-core path's FP32 kernels, P=16 the
+    unrolled ones and P=18 the runtime-order ones."""
+    from minimal_b200 import FMM, drand48_bodies
+
+    n = 20000
+    xq = drand48_bodies(n, 8)
+    outs = {}
+    for prec, s in (("fp64", 1.0), ("mixed", 1.0), ("mixed", scale)):
+        x = xq.copy()
+        x[:, :3] *= s
+        f = FMM(P=P, ncrit=64, theta=0.4, precision=prec)
+        f.set_bodies(x)
+        f.evaluate()
+        outs[prec, s] = f.bodies()
+        f.close()
+    ref, base, o = outs["fp64", 1.0], outs["mixed", 1.0], outs["mixed", scale]
+    assert np.array_equal(o[:, :3], base[:, :3] * scale)  # the same tree
+    assert np.isfinite(o[:, 4:]).all()
+    # against the unscaled FP64 result, the scaled domain keeps the mixed
+    # form's own error (two FP32 roundings of the same sums differ by about
+    # sqrt(2) times that error, so they are not compared with each other)
+    for k, back in ((4, scale), (slice(5, 8), scale * scale)):
+        err0 = rel(base[:, k], ref[:, k])
+        assert rel(o[:, k] * back, ref[:, k]) <= 2 * err0 + 1e-7
