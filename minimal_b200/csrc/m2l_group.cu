@@ -60,6 +60,7 @@ constexpr int TC_LOAD_WARP = 4; // first of the producer warps
 constexpr int TC_LOAD_WARPS = 4;
 constexpr int TC_MMA_WARP = TC_LOAD_WARP + TC_LOAD_WARPS;  // MMA issuer, TMEM owner
 constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
+constexpr int TC_MAX_STAGES = 4;  // pipeline stages (groups in flight), as many as shared memory holds
 // Groups accumulated in FP32 in tensor memory before the partial sum is
 // folded into the compensated running sum.  The tensor core's FP32
 // accumulation truncates toward zero, so with same-signed contributions (all
@@ -235,15 +236,17 @@ struct TcPlan {
   int abytes;                        // bytes of one (hi or lo) multipole tile
 };
 
-TcPlan make_tc_plan(int P, int KP) {
+constexpr int tc_tri(int n) { return n * (n + 1) / 2; }
+
+constexpr TcPlan make_tc_plan(int P, int KP) {
   TcPlan t{};
   t.nb = (KP + 63) / 64;
   int off = 0;
   for (int b = 0; b < t.nb; b++) {
     t.rows[b] = KP - 64 * b < 64 ? KP - 64 * b : 64;
     int j = 0;
-    while (tri(j + 1) <= 32 * b) j++;  // order of the block's first output
-    const int kreal = 2 * tri(P - j);
+    while (tc_tri(j + 1) <= 32 * b) j++;  // order of the block's first output
+    const int kreal = 2 * tc_tri(P - j);
     const int k16 = (kreal + 15) / 16 * 16;
     t.ksteps[b] = (k16 < KP ? k16 : KP) / 16;
     t.boff[b] = off;
@@ -254,6 +257,32 @@ TcPlan make_tc_plan(int P, int KP) {
   t.abytes = TC_TILE * 128 * t.atomsA;
   return t;
 }
+
+constexpr size_t TC_SMEM_MAX = 227 * 1024;  // opt-in shared memory per CTA on sm_100
+
+constexpr int tc_kp(int P) { return (P * (P + 1) + 15) / 16 * 16; }
+constexpr size_t tc_stage_bytes(const TcPlan &t) { return 2 * (size_t)t.abytes + 2 * (size_t)t.bimg; }
+// + 1024 to align the stages to the swizzle atom, + 256 for the barriers and the TMEM slot
+constexpr size_t TC_SMEM_EXTRA = 1024 + 256;
+// as many stages as fit, at most TC_MAX_STAGES
+constexpr int tc_stages(const TcPlan &t) {
+  int n = 1;
+  while (n < TC_MAX_STAGES && (n + 1) * tc_stage_bytes(t) + TC_SMEM_EXTRA <= TC_SMEM_MAX) n++;
+  return n;
+}
+constexpr size_t tc_smem(const TcPlan &t) { return tc_stages(t) * tc_stage_bytes(t) + TC_SMEM_EXTRA; }
+
+// The orders compiled with their plan as constants (6, 8, 10 and 12, the
+// switch in contract()): the MMA issue loop and the producers' copy loop
+// unroll with immediate offsets, so the issuing thread and the producers
+// spend fewer instructions per segment.  Other orders take the plan at run
+// time.
+template <int PT>
+struct TcFixed {
+  static constexpr int KP = tc_kp(PT);
+  static constexpr TcPlan plan = make_tc_plan(PT, KP);
+  static constexpr int nstage = tc_stages(plan);
+};
 
 // One CTA per group: the operator split into FP16 hi + lo parts, written as
 // the byte image the MMA reads from shared memory (hi image, then lo image).
@@ -727,25 +756,31 @@ struct TcAcc {
   uint32_t stride, hi, lo, ncols;
 };
 
+// PT > 0: the order PT with its plan and stage count as compile-time
+// constants (the run-time arguments are then ignored); PT = 0: any order.
+template <int PT>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, const int *tg_off, const int *tg_gid,
                                                           const int *tg_src, const unsigned char *ops,
-                                                          const __half *M16, const double4 *xr, double2 *L, int P,
-                                                          int KP, TcPlan pl,
-                                                          int nstage, TcAcc ta, int flush_every,
+                                                          const __half *M16, const double4 *xr, double2 *L, int P_,
+                                                          int KP_, TcPlan pl_,
+                                                          int nstage_, TcAcc ta, int flush_every,
                                                           const unsigned long long *m16_max, int *err, long wait_ns,
                                                           long stall_ns) {
+  constexpr bool FIX = PT > 0;
+  const int P = FIX ? PT : P_, KP = FIX ? TcFixed<PT>::KP : KP_, nstage = FIX ? TcFixed<PT>::nstage : nstage_;
+  const TcPlan pl = FIX ? TcFixed<PT>::plan : pl_;
   extern __shared__ __align__(1024) unsigned char smraw[];
   unsigned char *base = smraw + ((1024u - (tc::smem_u32(smraw) & 1023u)) & 1023u);  // swizzle atoms: 1024-aligned
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, tile = blockIdx.x;
   const uint32_t abytes = (uint32_t)pl.abytes, bimg = (uint32_t)pl.bimg;
   const uint32_t stage_bytes = 2 * abytes + 2 * bimg;  // A hi, A lo, B hi, B lo
-  uint64_t *full = (uint64_t *)(base + (size_t)nstage * stage_bytes);  // [2] multipoles landed (producer warps)
-  uint64_t *bful = full + 2;                                           // [2] operator landed (bulk copy bytes)
-  uint64_t *empty = full + 4;                                          // [2] MMAs reading the stage finished
-  uint64_t *accf = full + 6;                                           // [2] accumulator window complete
-  uint64_t *acce = full + 8;                                           // [2] accumulator folded, reusable
-  uint64_t *stall = full + 10;  // nothing arrives here (the stall test hook waits on it)
-  uint32_t *tslot = (uint32_t *)(full + 11);
+  uint64_t *full = (uint64_t *)(base + (size_t)nstage * stage_bytes);  // [stage] multipoles landed (producer warps)
+  uint64_t *bful = full + TC_MAX_STAGES;                               // [stage] operator landed (bulk copy bytes)
+  uint64_t *empty = bful + TC_MAX_STAGES;                              // [stage] MMAs reading the stage finished
+  uint64_t *accf = empty + TC_MAX_STAGES;                              // [2] accumulator window complete
+  uint64_t *acce = accf + 2;                                           // [2] accumulator folded, reusable
+  uint64_t *stall = acce + 2;  // nothing arrives here (the stall test hook waits on it)
+  uint32_t *tslot = (uint32_t *)(stall + 1);
   volatile int *abort = (volatile int *)(tslot + 1);  // a role gave up: the others stop waiting
   const uint32_t ncols = ta.ncols;
   const int fold = ta.fold;
@@ -754,9 +789,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
   auto phase_of = [&](int w) { return (uint32_t)(ta.nacc == 2 ? (w >> 1) : w) & 1u; };
   if (warp == TC_MMA_WARP) tc::alloc(tslot, ncols);
   if (tid == 0) {
-    for (int b = 0; b < 2; b++) tc::mbar_init(&full[b], TC_LOAD_WARPS * 32);
-    for (int b = 2; b < 8; b++) tc::mbar_init(&full[b], 1);
-    for (int b = 8; b < 10; b++) tc::mbar_init(&full[b], TC_EPI_WARPS);
+    for (int b = 0; b < TC_MAX_STAGES; b++) {
+      tc::mbar_init(&full[b], TC_LOAD_WARPS * 32);
+      tc::mbar_init(&bful[b], 1);
+      tc::mbar_init(&empty[b], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      tc::mbar_init(&accf[b], 1);
+      tc::mbar_init(&acce[b], TC_EPI_WARPS);
+    }
     tc::mbar_init(stall, 1);
     *abort = 0;
   }
@@ -811,7 +852,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     // Absent targets are zero-filled.  Producer thread 0 also starts the
     // operator's bulk copy.  Each thread's copies arrive on the stage's
     // barrier by themselves (cp.async.mbarrier.arrive), so the producers run
-    // up to two groups ahead of the MMAs.
+    // up to `nstage` groups ahead of the MMAs.  The next group's source rows
+    // and operator slot are loaded one group ahead.
     const int pw = warp - TC_LOAD_WARP, par = lane & 1;
     const int ra = 32 * pw + (lane >> 1), rb = ra + 16;
     const int half = KP / 8;  // 16-byte chunks of one half (hi or lo) of a source row; even
@@ -819,40 +861,52 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
       const int *row = tg_src + (long)(g0 + k) * TC_TILE;
       return k < n ? make_int2(row[ra], row[rb]) : make_int2(-1, -1);
     };
-    auto issue = [&](int k, int2 s2) {
-      const int st = k % nstage;
+    const bool bulk = pw == 0 && lane == 0;  // the thread that starts the operator's bulk copy
+    auto gid_of = [&](int k) { return bulk && k < n ? tg_gid[g0 + k] : 0; };
+    auto issue = [&](int st, int2 s2, int gid) {
       unsigned char *S = base + (size_t)st * stage_bytes;
-      if (pw == 0 && lane == 0) {
+      if (bulk) {
         tc::mbar_arrive_expect_tx(&bful[st], 2 * bimg);
-        tc::bulk_g2s(S + 2 * abytes, ops + (size_t)tg_gid[g0 + k] * 2 * bimg, 2 * bimg, &bful[st]);
+        tc::bulk_g2s(S + 2 * abytes, ops + (size_t)gid * 2 * bimg, 2 * bimg, &bful[st]);
       }
+      // chunk c = c0 + par with c0 even: half is even, so c0 alone decides
+      // the half (hl) and the atom, and the lane's parity only sets bit 4 of
+      // the in-row offset (folded into the row's swizzle q)
 #pragma unroll
       for (int j = 0; j < 2; j++) {
         const int r = j ? rb : ra, s = j ? s2.y : s2.x;
-        const __half *src = M16 + (size_t)(s < 0 ? 0 : s) * 2 * KP;
-        const uint32_t nb = s >= 0 ? 16u : 0u, rsw = (uint32_t)(r & 7) << 4;
+        const __half *src = M16 + (size_t)(s < 0 ? 0 : s) * 2 * KP + par * 8;
+        const uint32_t nb = s >= 0 ? 16u : 0u, q = ((uint32_t)par << 4) ^ ((uint32_t)(r & 7) << 4);
         unsigned char *R = S + r * 128;
-        for (int c = par; c < 2 * half; c += 2) {
-          const int hl = c >= half, cc = c - hl * half;
-          const uint32_t off = hl * abytes + (cc >> 3) * (TC_TILE * 128) + (((uint32_t)(cc & 7) << 4) ^ rsw);
-          tc::cp_async16(R + off, src + c * 8, nb);
+#pragma unroll
+        for (int c0 = 0; c0 < 2 * half; c0 += 2) {
+          const int hl = c0 >= half, cc0 = c0 - hl * half;
+          const uint32_t off = hl * abytes + (cc0 >> 3) * (TC_TILE * 128) + ((((uint32_t)cc0 & 7) << 4) ^ q);
+          tc::cp_async16(R + off, src + c0 * 8, nb);
         }
       }
       tc::cp_async_commit();
     };
     bool ok = true;
-    int last = -1;
+    int last = -1, lst = 0;
     int2 s_next = src_of(0);
-    for (int k = 0; k < n; k++) {
-      if (k >= nstage) {  // the stage is free once the MMAs of group k - nstage are done
-        ok = __all_sync(0xffffffffu,
-                        tc::mbar_wait(&empty[k % nstage], (uint32_t)(k / nstage - 1) & 1u, wait_ns, abort));
+    int gid_next = gid_of(0);
+    // stage st of round rnd = k / nstage (counters, no divisions)
+    for (int k = 0, st = 0, rnd = 0; k < n; k++) {
+      if (rnd > 0) {  // the stage is free once the MMAs of group k - nstage are done
+        ok = __all_sync(0xffffffffu, tc::mbar_wait(&empty[st], (uint32_t)(rnd - 1) & 1u, wait_ns, abort));
         if (!ok) break;
       }
-      issue(k, s_next);
-      tc::cp_async_arrive(&full[k % nstage]);  // arrives when this thread's copies have landed
+      issue(st, s_next, gid_next);
+      tc::cp_async_arrive(&full[st]);  // arrives when this thread's copies have landed
       last = k;
+      lst = st;
       s_next = src_of(k + 1);
+      gid_next = gid_of(k + 1);
+      if (++st == nstage) {
+        st = 0;
+        rnd++;
+      }
     }
     if (!ok) {
       *abort = 1;
@@ -861,7 +915,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     // drain this thread's copies; the operator's bulk copy completes by
     // itself (bounded wait, no abort: the copy must land before exit)
     tc::cp_async_wait_all();
-    if (pw == 0 && lane == 0 && last >= 0) tc::mbar_wait(&bful[last % nstage], parity(last), 2 * wait_ns);
+    if (pw == 0 && lane == 0 && last >= 0) tc::mbar_wait(&bful[lst], parity(last), 2 * wait_ns);
   } else if (warp == TC_MMA_WARP) {
     // ---- MMA issuer (one thread): per group and output block, K steps of
     // hi*hi + hi*lo + lo*hi into the window's accumulator
@@ -878,20 +932,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
       // test hook: a wait on a barrier that nothing arrives at, as if the
       // tensor core's inputs never came; it runs out after stall_ns
       bool ok = stall_ns <= 0 || tc::mbar_wait(stall, 0u, stall_ns, abort);
-      int last = -1;
-      for (int k = 0; ok && k < n; k++) {
-        const int st = k % nstage, w = k / flush_every, a = acc_of(w);
-        ok = tc::mbar_wait(&full[st], parity(k), wait_ns, abort) && tc::mbar_wait(&bful[st], parity(k), wait_ns, abort);
+      int last = -1, lst = 0;
+      // stage st of round rnd = k / nstage, window w = k / flush_every with
+      // kf = k % flush_every groups in it (counters, no divisions)
+      for (int k = 0, st = 0, rnd = 0, w = 0, kf = 0; ok && k < n; k++) {
+        const int a = acc_of(w);
+        const uint32_t ph = (uint32_t)rnd & 1u;
+        ok = tc::mbar_wait(&full[st], ph, wait_ns, abort) && tc::mbar_wait(&bful[st], ph, wait_ns, abort);
         // a new window reuses accumulator a once the epilogue has folded
         // window w - nacc, its previous user
-        if (ok && k % flush_every == 0 && w >= ta.nacc)
-          ok = tc::mbar_wait(&acce[a], phase_of(w - ta.nacc), wait_ns, abort);
+        if (ok && kf == 0 && w >= ta.nacc) ok = tc::mbar_wait(&acce[a], phase_of(w - ta.nacc), wait_ns, abort);
         if (!ok) break;
         tc::fence_after();
         const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
         const uint64_t dA = tc::smem_desc_sw128(sA), dB = tc::smem_desc_sw128(sB);
         const uint64_t lo_a = abytes >> 4, lo_b = bimg >> 4;  // descriptor start fields count 16 bytes
-        const bool fresh = k % flush_every == 0;
+        const bool fresh = kf == 0;
         const uint32_t acc = tmem + (uint32_t)a * ta.stride;
         // per K step: hi*hi, then hi*lo with the same A, then lo*hi (issuing
         // the small products first lowered the truncation bias by a third
@@ -899,6 +955,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
 #pragma unroll
         for (int b = 0; b < 4; b++) {
           if (b >= pl.nb) break;
+#pragma unroll
           for (int ks = 0; ks < ksteps[b]; ks++) {
             const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
             const uint64_t bo = ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * rows[b] * 128 + (uint64_t)(ks & 3) * 32) >> 4;
@@ -909,15 +966,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
           }
         }
         tc::commit(&empty[st]);
-        if (k % flush_every == flush_every - 1 || k == n - 1) tc::commit(&accf[a]);
+        if (kf == flush_every - 1 || k == n - 1) tc::commit(&accf[a]);
         last = k;
+        lst = st;
+        if (++st == nstage) {
+          st = 0;
+          rnd++;
+        }
+        if (++kf == flush_every) {
+          kf = 0;
+          w++;
+        }
       }
       if (!ok) {
         *abort = 1;
         atomicExch(err, 1);
       }
       // drain: the MMAs already issued complete by themselves (no abort)
-      if (last >= 0) tc::mbar_wait(&empty[last % nstage], parity(last), 2 * wait_ns);
+      if (last >= 0) tc::mbar_wait(&empty[lst], parity(last), 2 * wait_ns);
     }
     __syncwarp();
   }
@@ -975,13 +1041,6 @@ size_t gemm64_smem(const GroupPlan &g, int nstage = 1) {
   return std::max(nstage * stage, red) * sizeof(double);
 }
 
-constexpr size_t TC_SMEM_MAX = 227 * 1024;  // opt-in shared memory per CTA on sm_100
-
-int tc_kp(int P) { return (P * (P + 1) + 15) / 16 * 16; }
-size_t tc_stage_bytes(const TcPlan &t) { return 2 * (size_t)t.abytes + 2 * (size_t)t.bimg; }
-// + 1024 to align the stages to the swizzle atom, + 128 for 10 barriers and the TMEM slot
-int tc_stages(const TcPlan &t) { return 2 * tc_stage_bytes(t) + 1024 + 128 <= TC_SMEM_MAX ? 2 : 1; }
-size_t tc_smem(const TcPlan &t) { return tc_stages(t) * tc_stage_bytes(t) + 1024 + 128; }
 // columns of one TMEM accumulator: a power of two >= KP (and >= 32)
 uint32_t tc_half_cols(int KP) {
   uint32_t c = 32;
@@ -1016,7 +1075,11 @@ bool m2l_grouped_available(int P) {
 
 void m2l_grouped_set_attributes() {
   cudaFuncSetAttribute(k_gemm64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
-  cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
+  cudaFuncSetAttribute(k_m2l_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
+  cudaFuncSetAttribute(k_m2l_tc<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
+  cudaFuncSetAttribute(k_m2l_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
+  cudaFuncSetAttribute(k_m2l_tc<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
+  cudaFuncSetAttribute(k_m2l_tc<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
 }
 
 // Grouped M2L of the whole tree: L stored for every cell (zero where no
@@ -1033,11 +1096,20 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
   DevCounters *ctr = h.counters.as<DevCounters>();
   if (tcore) {
     FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
-    k_m2l_tc<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                    h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
-                                                    h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
-                                                    tc_stages(tp), tc_acc_layout(KP16), m2l_flush_interval(h),
-                                                    &ctr->m16_max, &ctr->tc_error, TC_WAIT_NS, h.tc_stall_ns);
+    auto launch = [&](auto kern) {
+      kern<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
+                                                   h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
+                                                   h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
+                                                   tc_stages(tp), tc_acc_layout(KP16), m2l_flush_interval(h),
+                                                   &ctr->m16_max, &ctr->tc_error, TC_WAIT_NS, h.tc_stall_ns);
+    };
+    switch (P) {  // the orders compiled with their plan as constants
+      case 6: launch(k_m2l_tc<6>); break;
+      case 8: launch(k_m2l_tc<8>); break;
+      case 10: launch(k_m2l_tc<10>); break;
+      case 12: launch(k_m2l_tc<12>); break;
+      default: launch(k_m2l_tc<0>);
+    }
     h.tc_stall_ns = 0;  // the test hook stalls one launch
     FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
     h.g_used_tc = true;
