@@ -180,6 +180,8 @@ struct Handle {
   Buf per_harm;
   Buf per_part;  // partial charge sums (the mixed form's root monopole)
   Buf g_gharm;  // harmonics of the ghost shifts, per (image, finer level)
+  Buf g_part;   // tensor-core M2L: partial local expansions of tiles split between CTAs
+  int nsm = 0;  // streaming multiprocessors of the device (0: not read yet)
   int per_P = 0, per_images = 0;
   double per_cycle = 0;
   // tile shapes chosen at run time (exafmm_b200_set_tile; the autotuner)

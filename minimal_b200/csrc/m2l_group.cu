@@ -272,6 +272,51 @@ constexpr int tc_stages(const TcPlan &t) {
 }
 constexpr size_t tc_smem(const TcPlan &t) { return tc_stages(t) * tc_stage_bytes(t) + TC_SMEM_EXTRA; }
 
+// Tensor-memory layout of the accumulators (columns; 128 lanes = targets):
+// nacc accumulators of KP columns `stride` apart, used in turn, one per
+// window (the tensor core fills one while the epilogue folds another; with
+// one, the tensor core waits for each fold).  fold = 1: the double-FP32
+// running sum at columns [hi, hi + KP) and [lo, lo + KP); fold = 2: an FP32
+// running sum at [hi, hi + KP) (round-to-nearest adds); fold = 0: windows are
+// added to L in global memory.  ncols is the allocation (a power of two).
+struct TcAcc {
+  int nacc, fold;
+  uint32_t stride, hi, lo, ncols;
+};
+constexpr int TC_MAX_ACC = 3;
+
+// columns of one TMEM accumulator: a power of two >= KP (and >= 32)
+constexpr uint32_t tc_half_cols(int KP) {
+  uint32_t c = 32;
+  while (c < (uint32_t)KP) c <<= 1;
+  return c;
+}
+
+// Two accumulators and the running sum where they fit (KP up to 128: P <=
+// 10), else one accumulator and the running sum (3 x KP rounded to 32
+// columns within 512: P = 11, 12), else windows added to L in global memory.
+constexpr TcAcc tc_acc_layout(int KP) {
+  const uint32_t hc = tc_half_cols(KP), k32 = ((uint32_t)KP + 31u) / 32u * 32u;
+  if (4 * hc <= 512) return TcAcc{2, 1, hc, 2 * hc, 3 * hc, 4 * hc};
+  if (3 * k32 <= 512) return TcAcc{1, 1, 0, k32, 2 * k32, 512};
+  return TcAcc{2, 0, hc, 0, 0, 2 * hc};
+}
+
+// Orders compiled with their plan: three accumulators, so that a fold has
+// two windows' time before the tensor core needs its accumulator again --
+// with the double-FP32 running sum where five fit (KP <= 64), else (KP <=
+// 128) with an FP32 running sum.  The window sums carry the tensor core's
+// truncating FP32 accumulation, which the short window bounds; the running
+// sum's round-to-nearest adds are unbiased, ~sqrt(windows) * 2^-24 relative
+// (about 6e-7 over the ~95 windows of a tile at P = 10, far below the
+// expansion's error).  Otherwise the layout above.
+constexpr TcAcc tc_acc_fixed(int KP) {
+  const uint32_t hc = tc_half_cols(KP);
+  if (5 * hc <= 512) return TcAcc{3, 1, hc, 3 * hc, 4 * hc, 5 * hc <= 256 ? 256u : 512u};
+  if (4 * hc <= 512) return TcAcc{3, 2, hc, 3 * hc, 0, 512};
+  return tc_acc_layout(KP);
+}
+
 // The orders compiled with their plan as constants (6, 8, 10 and 12, the
 // switch in contract()): the MMA issue loop and the producers' copy loop
 // unroll with immediate offsets, so the issuing thread and the producers
@@ -282,6 +327,7 @@ struct TcFixed {
   static constexpr int KP = tc_kp(PT);
   static constexpr TcPlan plan = make_tc_plan(PT, KP);
   static constexpr int nstage = tc_stages(plan);
+  static constexpr TcAcc acc = tc_acc_fixed(KP);
 };
 
 // One CTA per group: the operator split into FP16 hi + lo parts, written as
@@ -676,6 +722,20 @@ __device__ __forceinline__ void tc_fold(uint32_t acc, uint32_t hi, uint32_t lo, 
   tc::wait_st();
 }
 
+// tc_fold with an FP32 running sum (round-to-nearest adds, no error term).
+__device__ __forceinline__ void tc_fold32(uint32_t acc, uint32_t hi, int cb, int ce) {
+  for (int c0 = cb; c0 < ce; c0 += 16) {
+    uint32_t a[16], h[16];
+    tc::ld_32x32b_x16_async(acc + (uint32_t)c0, a);
+    tc::ld_32x32b_x16_async(hi + (uint32_t)c0, h);
+    tc::wait_ld();
+#pragma unroll
+    for (int k = 0; k < 16; k++) h[k] = __float_as_uint(__uint_as_float(h[k]) + __uint_as_float(a[k]));
+    tc::st_32x32b_x16(hi + (uint32_t)c0, h);
+  }
+  tc::wait_st();
+}
+
 __device__ __forceinline__ void tc_zero(uint32_t cols, int cb, int ce) {
   const uint32_t z[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int c0 = cb; c0 < ce; c0 += 16) tc::st_32x32b_x16(cols + (uint32_t)c0, z);
@@ -685,16 +745,19 @@ __device__ __forceinline__ void tc_zero(uint32_t cols, int cb, int ce) {
 // Stores the running sum as the FP64 local expansion, unscaled
 // (L = L~ / R_t^(j+1), and the split's 2^E removed: us = 2^-E).  The tile is
 // the only grouped writer of its targets.
-__device__ __forceinline__ void tc_store(uint32_t hi, uint32_t lo, int t, double inv, double us, int cb, int ce,
-                                         int NT, double2 *L) {
+__device__ __forceinline__ void tc_store(uint32_t hi, uint32_t lo, bool has_lo, int t, double inv, double us, int cb,
+                                         int ce, int NT, double2 *L) {
   int j = 0;
   double sj = inv * us;  // us * inv^(j+1)
   for (int c0 = cb; c0 < ce; c0 += 16) {
     uint32_t h[16], l[16];
     tc::ld_32x32b_x16_async(hi + (uint32_t)c0, h);
-    tc::ld_32x32b_x16_async(lo + (uint32_t)c0, l);
+    if (has_lo) tc::ld_32x32b_x16_async(lo + (uint32_t)c0, l);
     tc::wait_ld();
     if (t < 0) continue;
+    if (!has_lo)
+#pragma unroll
+      for (int k = 0; k < 16; k++) l[k] = 0u;
     for (int k = 0; k < 16; k += 2) {
       const int o = (c0 + k) >> 1;
       if (o >= NT) break;
@@ -745,48 +808,62 @@ __device__ __forceinline__ void tc_flush_global(uint32_t acc, int t, double inv,
   }
 }
 
-// Tensor-memory layout of the accumulators (columns; 128 lanes = targets):
-// nacc accumulators of KP columns `stride` apart, alternating per window
-// (two: the tensor core fills one while the epilogue folds the other; one:
-// the tensor core waits for each fold); with `fold`, the double-FP32 running
-// sum at columns [hi, hi + KP) and [lo, lo + KP), else windows are added to L
-// in global memory.  ncols is the allocation (a power of two).
-struct TcAcc {
-  int nacc, fold;
-  uint32_t stride, hi, lo, ncols;
-};
-
 // PT > 0: the order PT with its plan and stage count as compile-time
 // constants (the run-time arguments are then ignored); PT = 0: any order.
+// Largest tile t < ntiles with tg_off[t] <= s (the tile holding segment s,
+// for s below the segment count).
+__device__ __forceinline__ int tile_at(const int *tg_off, int ntiles, int s) {
+  int lo = 0, hi = ntiles - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tg_off[mid] <= s) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// First segment of CTA c of G when nseg segments are cut into equal ranges.
+__device__ __forceinline__ int range_start(int nseg, int c, int G) { return (int)((long long)nseg * c / G); }
+
+// Work split of the orders compiled with their plan and a running sum in
+// TMEM ("balanced"): one CTA per SM, each taking an equal contiguous range of
+// the (tile, group) segments -- the tiles hold 182 to 325 segments at 1M
+// uniform bodies, and with two tiles per SM the SM that drew the longest
+// ones set the kernel's time (720 us against 557 us of average SM work).  A
+// CTA stores the tiles that lie wholly in its range; of a tile cut by a
+// range boundary it writes its partial sums to `part` (slot 0: its first
+// tile, 1: its last), which k_m2l_join adds in CTA order (deterministic).
+// Otherwise one CTA per tile.
 template <int PT>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, const int *tg_off, const int *tg_gid,
                                                           const int *tg_src, const unsigned char *ops,
                                                           const __half *M16, const double4 *xr, double2 *L, int P_,
                                                           int KP_, TcPlan pl_,
-                                                          int nstage_, TcAcc ta, int flush_every,
+                                                          int nstage_, TcAcc ta_, int flush_every,
                                                           const unsigned long long *m16_max, int *err, long wait_ns,
-                                                          long stall_ns) {
+                                                          long stall_ns, int ntiles, double2 *part) {
   constexpr bool FIX = PT > 0;
+  constexpr bool BAL = FIX && TcFixed<PT>::acc.fold != 0;
   const int P = FIX ? PT : P_, KP = FIX ? TcFixed<PT>::KP : KP_, nstage = FIX ? TcFixed<PT>::nstage : nstage_;
   const TcPlan pl = FIX ? TcFixed<PT>::plan : pl_;
+  const TcAcc ta = FIX ? TcFixed<PT>::acc : ta_;
   extern __shared__ __align__(1024) unsigned char smraw[];
   unsigned char *base = smraw + ((1024u - (tc::smem_u32(smraw) & 1023u)) & 1023u);  // swizzle atoms: 1024-aligned
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, tile = blockIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t abytes = (uint32_t)pl.abytes, bimg = (uint32_t)pl.bimg;
   const uint32_t stage_bytes = 2 * abytes + 2 * bimg;  // A hi, A lo, B hi, B lo
   uint64_t *full = (uint64_t *)(base + (size_t)nstage * stage_bytes);  // [stage] multipoles landed (producer warps)
   uint64_t *bful = full + TC_MAX_STAGES;                               // [stage] operator landed (bulk copy bytes)
   uint64_t *empty = bful + TC_MAX_STAGES;                              // [stage] MMAs reading the stage finished
-  uint64_t *accf = empty + TC_MAX_STAGES;                              // [2] accumulator window complete
-  uint64_t *acce = accf + 2;                                           // [2] accumulator folded, reusable
-  uint64_t *stall = acce + 2;  // nothing arrives here (the stall test hook waits on it)
+  uint64_t *accf = empty + TC_MAX_STAGES;                              // [acc] accumulator window complete
+  uint64_t *acce = accf + TC_MAX_ACC;                                  // [acc] accumulator folded, reusable
+  uint64_t *stall = acce + TC_MAX_ACC;  // nothing arrives here (the stall test hook waits on it)
   uint32_t *tslot = (uint32_t *)(stall + 1);
   volatile int *abort = (volatile int *)(tslot + 1);  // a role gave up: the others stop waiting
   const uint32_t ncols = ta.ncols;
   const int fold = ta.fold;
-  // window w's accumulator, and the phase of its barriers
-  auto acc_of = [&](int w) { return ta.nacc == 2 ? (w & 1) : 0; };
-  auto phase_of = [&](int w) { return (uint32_t)(ta.nacc == 2 ? (w >> 1) : w) & 1u; };
+  // window w uses accumulator a = w % nacc for the u-th time, u = w / nacc
+  // (both kept as counters): its barriers complete once per use
   if (warp == TC_MMA_WARP) tc::alloc(tslot, ncols);
   if (tid == 0) {
     for (int b = 0; b < TC_MAX_STAGES; b++) {
@@ -794,7 +871,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
       tc::mbar_init(&bful[b], 1);
       tc::mbar_init(&empty[b], 1);
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < TC_MAX_ACC; b++) {
       tc::mbar_init(&accf[b], 1);
       tc::mbar_init(&acce[b], TC_EPI_WARPS);
     }
@@ -805,40 +882,67 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = *tslot;
-  const int g0 = tg_off[tile], n = tg_off[tile + 1] - g0;
-  const int nwin = (n + flush_every - 1) / flush_every;
+  // this CTA's segments [g0, g1) and the first tile they touch
+  int g0, g1, tfirst;
+  if (BAL) {
+    const int nseg = tg_off[ntiles];
+    g0 = range_start(nseg, blockIdx.x, gridDim.x);
+    g1 = range_start(nseg, blockIdx.x + 1, gridDim.x);
+    tfirst = g1 > g0 ? tile_at(tg_off, ntiles, g0) : 0;
+  } else {
+    tfirst = blockIdx.x;
+    g0 = tg_off[tfirst];
+    g1 = tg_off[tfirst + 1];
+  }
+  const int n = g1 - g0;
   auto parity = [&](int k) { return (uint32_t)(k / nstage) & 1u; };
 
   if (warp < TC_EPI_WARPS) {
-    // ---- epilogue: warp w owns TMEM lanes 32w.. = targets 32w..
-    const int t = tile_tgt[tile * TC_TILE + tid];
-    const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
+    // ---- epilogue: warp w owns TMEM lanes 32w.. = targets 32w..; per tile
+    // of the range, its windows (as the MMA issuer closes them: every
+    // flush_every groups and at the tile's last group in the range)
     const double us = scalbn(1.0, -m16_exponent(*m16_max));
     const int NT = tri(P);
     const uint32_t lanes = tmem + ((uint32_t)(warp * 32) << 16);
     const uint32_t sum_hi = lanes + ta.hi, sum_lo = lanes + ta.lo;
-    if (fold) {
-      tc_zero(sum_hi, 0, KP);
-      tc_zero(sum_lo, 0, KP);
-    }
     bool ok = true;
-    for (int w = 0; w < nwin; w++) {
-      const int a = acc_of(w);
-      ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[a], phase_of(w), wait_ns, abort));
-      if (!ok) break;
-      tc::fence_after();
-      const uint32_t acc = lanes + (uint32_t)a * ta.stride;
-      if (fold) tc_fold(acc, sum_hi, sum_lo, 0, KP);
-      else tc_flush_global(acc, t, inv, us, 0, KP, NT, L);
-      tc::fence_before();
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&acce[a]);
+    int a = 0, u = 0;  // accumulator of the next window, and its use count
+    for (int tt = tfirst; ok && n > 0 && tt < ntiles; tt++) {
+      const int ts = max(g0, tg_off[tt]), te = min(g1, tg_off[tt + 1]);
+      if (ts >= g1) break;
+      if (te <= ts) continue;  // a tile without segments
+      const int t = tile_tgt[tt * TC_TILE + tid];
+      const double inv = t >= 0 ? 1.0 / xr[t].w : 0.0;
+      if (fold) tc_zero(sum_hi, 0, KP);
+      if (fold == 1) tc_zero(sum_lo, 0, KP);
+      const int nwin = (te - ts + flush_every - 1) / flush_every;
+      for (int w = 0; w < nwin; w++) {
+        ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[a], (uint32_t)u & 1u, wait_ns, abort));
+        if (!ok) break;
+        tc::fence_after();
+        const uint32_t acc = lanes + (uint32_t)a * ta.stride;
+        if (fold == 1) tc_fold(acc, sum_hi, sum_lo, 0, KP);
+        else if (fold == 2) tc_fold32(acc, sum_hi, 0, KP);
+        else tc_flush_global(acc, t, inv, us, 0, KP, NT, L);
+        tc::fence_before();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&acce[a]);
+        if (++a == ta.nacc) {
+          a = 0;
+          u++;
+        }
+      }
+      if (!ok || !fold) continue;
+      if (tg_off[tt] >= g0 && tg_off[tt + 1] <= g1) {
+        tc_store(sum_hi, sum_lo, fold == 1, t, inv, us, 0, KP, NT, L);
+      } else {  // a part of a tile cut by a range boundary
+        double2 *slot = part + (size_t)(2 * blockIdx.x + (tt == tfirst ? 0 : 1)) * TC_TILE * NT;
+        tc_store(sum_hi, sum_lo, fold == 1, t >= 0 ? tid : -1, inv, us, 0, KP, NT, slot);
+      }
     }
     if (!ok) {
       *abort = 1;
       if (lane == 0) atomicExch(err, 1);
-    } else if (fold && n > 0) {
-      tc_store(sum_hi, sum_lo, t, inv, us, 0, KP, NT, L);
     }
   } else if (warp < TC_LOAD_WARP + TC_LOAD_WARPS) {
     // ---- producers: warp pw copies target rows 32pw..32pw+31 of the tile
@@ -933,15 +1037,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
       // tensor core's inputs never came; it runs out after stall_ns
       bool ok = stall_ns <= 0 || tc::mbar_wait(stall, 0u, stall_ns, abort);
       int last = -1, lst = 0;
-      // stage st of round rnd = k / nstage, window w = k / flush_every with
-      // kf = k % flush_every groups in it (counters, no divisions)
-      for (int k = 0, st = 0, rnd = 0, w = 0, kf = 0; ok && k < n; k++) {
-        const int a = acc_of(w);
+      // end of the current tile's segments in the range (a window closes
+      // there too)
+      int tcur = tfirst, tend = BAL ? min(g1, tg_off[tfirst + 1]) : g1;
+      // stage st of round rnd = k / nstage; the window has kf groups so far
+      // and uses accumulator a for the u-th time (counters, no divisions)
+      for (int k = 0, st = 0, rnd = 0, kf = 0, a = 0, u = 0; ok && k < n; k++) {
+        if (BAL && g0 + k >= tend) {  // next tile (skipping tiles without segments)
+          do tcur++;
+          while (tg_off[tcur + 1] <= g0 + k);
+          tend = min(g1, tg_off[tcur + 1]);
+        }
+        const bool close = kf == flush_every - 1 || g0 + k + 1 == tend;
         const uint32_t ph = (uint32_t)rnd & 1u;
         ok = tc::mbar_wait(&full[st], ph, wait_ns, abort) && tc::mbar_wait(&bful[st], ph, wait_ns, abort);
         // a new window reuses accumulator a once the epilogue has folded
-        // window w - nacc, its previous user
-        if (ok && kf == 0 && w >= ta.nacc) ok = tc::mbar_wait(&acce[a], phase_of(w - ta.nacc), wait_ns, abort);
+        // its previous use
+        if (ok && kf == 0 && u > 0) ok = tc::mbar_wait(&acce[a], (uint32_t)(u - 1) & 1u, wait_ns, abort);
         if (!ok) break;
         tc::fence_after();
         const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
@@ -966,16 +1078,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
           }
         }
         tc::commit(&empty[st]);
-        if (kf == flush_every - 1 || k == n - 1) tc::commit(&accf[a]);
+        if (close) tc::commit(&accf[a]);
         last = k;
         lst = st;
         if (++st == nstage) {
           st = 0;
           rnd++;
         }
-        if (++kf == flush_every) {
+        if (close) {
           kf = 0;
-          w++;
+          if (++a == ta.nacc) {
+            a = 0;
+            u++;
+          }
+        } else {
+          kf++;
         }
       }
       if (!ok) {
@@ -991,6 +1108,41 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
   __syncthreads();
   tc::fence_after();
   if (warp == TC_MMA_WARP) tc::dealloc(tmem, ncols);
+}
+
+// Tiles cut by the balanced ranges of k_m2l_tc: L of the tile's targets is
+// the sum of the CTAs' parts, added in CTA order.  One CTA per tile, a
+// thread per target row.
+__global__ void k_m2l_join(const int *tile_tgt, const int *tg_off, int ntiles, int G, const double2 *part, int NT,
+                           double2 *L) {
+  const int t = blockIdx.x, nseg = tg_off[ntiles];
+  const int a = tg_off[t], b = tg_off[t + 1];
+  if (b <= a) return;
+  // the CTA whose range holds segment s
+  auto cta_of = [&](int s) {
+    int c = (int)((long long)s * G / nseg);
+    while (c + 1 < G && range_start(nseg, c + 1, G) <= s) c++;
+    while (c > 0 && range_start(nseg, c, G) > s) c--;
+    return c;
+  };
+  const int c0 = cta_of(a), c1 = cta_of(b - 1);
+  if (c0 == c1) return;  // the tile lies in one range: stored by its CTA
+  const int row = threadIdx.x, tgt = tile_tgt[t * TC_TILE + row];
+  if (tgt < 0) return;
+  // the tile is the first tile (slot 0) of every CTA after c0, whose ranges
+  // start inside it; for c0 it is the last (slot 1) unless c0's range
+  // starts at the tile
+  const int slot0 = range_start(nseg, c0, G) < a ? 1 : 0;
+  for (int o = 0; o < NT; o++) {
+    double2 sum = make_double2(0, 0);
+    for (int c = c0; c <= c1; c++) {
+      const int slot = c == c0 ? slot0 : 0;
+      const double2 v = part[((size_t)(2 * c + slot) * TC_TILE + row) * NT + o];
+      sum.x += v.x;
+      sum.y += v.y;
+    }
+    L[(long)tgt * NT + o] = sum;
+  }
 }
 
 struct PlanCache {
@@ -1041,24 +1193,6 @@ size_t gemm64_smem(const GroupPlan &g, int nstage = 1) {
   return std::max(nstage * stage, red) * sizeof(double);
 }
 
-// columns of one TMEM accumulator: a power of two >= KP (and >= 32)
-uint32_t tc_half_cols(int KP) {
-  uint32_t c = 32;
-  while (c < (uint32_t)KP) c <<= 1;
-  return c;
-}
-
-// Two double-buffered accumulators and the running sum where they fit (KP up
-// to 128: P <= 10), else one accumulator and the running sum (3 x KP
-// rounded to 32 columns within 512: P = 11, 12), else windows added to L in
-// global memory.
-TcAcc tc_acc_layout(int KP) {
-  const uint32_t hc = tc_half_cols(KP), k32 = ((uint32_t)KP + 31u) / 32u * 32u;
-  if (4 * hc <= 512) return TcAcc{2, 1, hc, 2 * hc, 3 * hc, 4 * hc};
-  if (3 * k32 <= 512) return TcAcc{1, 1, 0, k32, 2 * k32, 512};
-  return TcAcc{2, 0, hc, 0, 0, 2 * hc};
-}
-
 bool tc_available(int P) {
   const int KP = tc_kp(P);
   return KP <= 256 && tc_smem(make_tc_plan(P, KP)) <= TC_SMEM_MAX;
@@ -1096,19 +1230,30 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
   DevCounters *ctr = h.counters.as<DevCounters>();
   if (tcore) {
     FMM_CUDA(cudaMemsetAsync(&ctr->tc_error, 0, sizeof(int), s));
+    // the orders compiled with their plan as constants; those with a running
+    // sum in TMEM take balanced segment ranges, one CTA per SM
+    const bool fixed = P == 6 || P == 8 || P == 10 || P == 12;
+    const bool bal = fixed && tc_acc_fixed(KP16).fold != 0;
+    if (bal && h.nsm == 0) FMM_CUDA(cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.prm.device));
+    const int G = bal ? std::min(ntiles, h.nsm) : ntiles, NT = tri(P);
+    if (bal) h.g_part.need((size_t)G * 2 * TC_TILE * NT * sizeof(double2));
+    double2 *part = bal ? h.g_part.as<double2>() : nullptr;
     auto launch = [&](auto kern) {
-      kern<<<ntiles, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                   h.g_ops.as<unsigned char>(), h.g_m16.as<__half>(),
-                                                   h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16, tp,
-                                                   tc_stages(tp), tc_acc_layout(KP16), m2l_flush_interval(h),
-                                                   &ctr->m16_max, &ctr->tc_error, TC_WAIT_NS, h.tc_stall_ns);
+      kern<<<G, TC_THREADS, tc_smem(tp), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src, h.g_ops.as<unsigned char>(),
+                                              h.g_m16.as<__half>(), h.c_xr.as<double4>(), h.L.as<double2>(), P, KP16,
+                                              tp, tc_stages(tp), tc_acc_layout(KP16), m2l_flush_interval(h),
+                                              &ctr->m16_max, &ctr->tc_error, TC_WAIT_NS, h.tc_stall_ns, ntiles, part);
     };
-    switch (P) {  // the orders compiled with their plan as constants
+    switch (P) {
       case 6: launch(k_m2l_tc<6>); break;
       case 8: launch(k_m2l_tc<8>); break;
       case 10: launch(k_m2l_tc<10>); break;
       case 12: launch(k_m2l_tc<12>); break;
       default: launch(k_m2l_tc<0>);
+    }
+    if (bal) {
+      k_m2l_join<<<ntiles, TC_TILE, 0, s>>>(h.g_tile.as<int>(), tg_off, ntiles, G, part, NT, h.L.as<double2>());
+      h.launches++;
     }
     h.tc_stall_ns = 0;  // the test hook stalls one launch
     FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
