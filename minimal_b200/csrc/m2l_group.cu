@@ -1111,10 +1111,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
 }
 
 // Tiles cut by the balanced ranges of k_m2l_tc: L of the tile's targets is
-// the sum of the CTAs' parts, added in CTA order.  One CTA per tile, a
-// thread per target row.
-__global__ void k_m2l_join(const int *tile_tgt, const int *tg_off, int ntiles, int G, const double2 *part, int NT,
-                           double2 *L) {
+// the sum of the CTAs' parts, added in CTA order.  One CTA per tile; threads
+// run over (target row, coefficient) with the coefficient fastest, so the
+// parts and L are read and written contiguously.
+constexpr int JOIN_T = 256;
+__global__ void __launch_bounds__(JOIN_T) k_m2l_join(const int *tile_tgt, const int *tg_off, int ntiles, int G,
+                                                     const double2 *part, int NT, double2 *L) {
   const int t = blockIdx.x, nseg = tg_off[ntiles];
   const int a = tg_off[t], b = tg_off[t + 1];
   if (b <= a) return;
@@ -1127,17 +1129,17 @@ __global__ void k_m2l_join(const int *tile_tgt, const int *tg_off, int ntiles, i
   };
   const int c0 = cta_of(a), c1 = cta_of(b - 1);
   if (c0 == c1) return;  // the tile lies in one range: stored by its CTA
-  const int row = threadIdx.x, tgt = tile_tgt[t * TC_TILE + row];
-  if (tgt < 0) return;
   // the tile is the first tile (slot 0) of every CTA after c0, whose ranges
   // start inside it; for c0 it is the last (slot 1) unless c0's range
   // starts at the tile
   const int slot0 = range_start(nseg, c0, G) < a ? 1 : 0;
-  for (int o = 0; o < NT; o++) {
+  for (int e = threadIdx.x; e < TC_TILE * NT; e += JOIN_T) {
+    const int row = e / NT, o = e - row * NT, tgt = tile_tgt[t * TC_TILE + row];
+    if (tgt < 0) continue;
     double2 sum = make_double2(0, 0);
     for (int c = c0; c <= c1; c++) {
       const int slot = c == c0 ? slot0 : 0;
-      const double2 v = part[((size_t)(2 * c + slot) * TC_TILE + row) * NT + o];
+      const double2 v = part[(size_t)(2 * c + slot) * TC_TILE * NT + e];
       sum.x += v.x;
       sum.y += v.y;
     }
@@ -1252,7 +1254,7 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
       default: launch(k_m2l_tc<0>);
     }
     if (bal) {
-      k_m2l_join<<<ntiles, TC_TILE, 0, s>>>(h.g_tile.as<int>(), tg_off, ntiles, G, part, NT, h.L.as<double2>());
+      k_m2l_join<<<ntiles, JOIN_T, 0, s>>>(h.g_tile.as<int>(), tg_off, ntiles, G, part, NT, h.L.as<double2>());
       h.launches++;
     }
     h.tc_stall_ns = 0;  // the test hook stalls one launch
