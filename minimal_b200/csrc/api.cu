@@ -362,7 +362,7 @@ int exafmm_b200_destroy(exafmm_b200 *H) {
                  &h.m2l_units, &h.stage, &h.g_mt, &h.g_ekey, &h.g_occ, &h.g_cnt, &h.g_keyof, &h.g_ops,
                  &h.g_tk, &h.g_tile, &h.g_seg, &h.g_tg, &h.g_m16, &h.g_slot, &h.g_pairs, &h.shift_ops, &h.shift_terms,
                  &h.op_scratch, &h.g_gmark, &h.per_harm, &h.g_gharm, &h.per_part,
-                 &h.g_part};
+                 &h.g_part, &h.body_leaf, &h.l2p_f};
   for (Buf *b : bufs) b->release();
   if (h.ev_ok)
     for (int p = 0; p < PH_COUNT + 1; p++)

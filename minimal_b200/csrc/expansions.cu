@@ -97,7 +97,7 @@ __constant__ float c_recip_f[2 * EXAFMM_MAX_P + 4];
 #define P2M_TRANSPOSE 1
 #endif
 #ifndef L2P_F32_MIN_BLOCKS
-#define L2P_F32_MIN_BLOCKS 4  // the unrolled L2P would otherwise hold all of L in registers
+#define L2P_F32_MIN_BLOCKS 6  // 128-thread blocks per SM: up to 80 registers a thread
 #endif
 // orders with unrolled FP32 P2M / L2P kernels (others take the runtime-order ones)
 #define EXAFMM_UNROLLED_ORDERS(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
@@ -270,69 +270,67 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2m_f32t(const int *leaves, int 
   }
 }
 
-// L2P in FP32: lane per body, the leaf's local expansion broadcast from
-// shared memory as float; p and F added to the FP64 results.
+// L2P in FP32, in two parts.  k_l2p_prep (before the wait for the near
+// field): per leaf, the local expansion in the leaf's units, L~_n = L_n R^n
+// with R the leaf radius rounded down to a power of two (exact), as FP32,
+// and the scale 1/R for the coordinates -- so the FP32 terms stay in range
+// at any domain size.  k_l2p_f32: a thread per body over all bodies (tree
+// order, every lane busy whatever the leaf sizes), its leaf's expansion
+// read through L1 (the lanes of a warp share one or two leaves); p and F
+// added to the FP64 results.
+__global__ void k_l2p_prep(const int *leaves, int nleaves, const double4 *xr, const double2 *L, int nt, float2 *Lf,
+                           float *lsc) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)nleaves * nt) return;
+  const int w = (int)(i / nt), k = (int)(i - (long)w * nt), c = leaves[w];
+  const int ex = leaf_exponent(xr[c].w), n = order_of(k);
+  const double2 l = L[(long)c * nt + k];
+  Lf[i] = make_float2((float)scalbn(l.x, ex * n), (float)scalbn(l.y, ex * n));
+  if (k == 0) lsc[w] = exp2f((float)-ex);
+}
+
 template <int PT>
-__global__ void __launch_bounds__(WARPS * 32, L2P_F32_MIN_BLOCKS) k_l2p_f32(const int *leaves, int nleaves, const int *begin,
-                                                        const int *count, const double4 *xr, const float4 *srcf,
-                                                        const double2 *L, double4 *out, int Prt) {
-  extern __shared__ float2 shf[];
+__global__ void __launch_bounds__(128, L2P_F32_MIN_BLOCKS) k_l2p_f32(long nbodies, const int *body_leaf,
+                                                                   const float4 *srcf, const float2 *Lf,
+                                                                   const float *lsc, double4 *out, int Prt) {
   const int P = PT > 0 ? PT : Prt;
   const int nt = tri(P);
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int w = blockIdx.x * WARPS + wid;
-  if (w >= nleaves) return;
-  const int c = leaves[w];
-  // coordinates in units where the leaf radius is in [1, 2), and the local
-  // expansion with them, L~_n = L_n R_s^n (exact powers of two): the FP32
-  // terms stay in range at any domain size
-  const int ex = leaf_exponent(xr[c].w);
-  const float sc = exp2f((float)-ex);
-  float2 *Lc = shf + wid * nt;
-  for (int k = lane; k < nt; k += 32) {
-    const double2 l = L[(long)c * nt + k];
-    const int n = order_of(k);
-    Lc[k] = make_float2((float)scalbn(l.x, ex * n), (float)scalbn(l.y, ex * n));
-  }
-  __syncwarp();
-  const int b0 = begin[c], nb = count[c];
-  for (int t = 0; t < nb; t += 32) {
-    const int b = b0 + t + lane;
-    const bool ok = t + lane < nb;
-    const float4 B = ok ? srcf[b] : make_float4(1.f, 0.f, 0.f, 0.f);
-    const SphF g = sph_of_f(B.x * sc, B.y * sc, B.z * sc);
-    float pot = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
-    regular_all_f<PT, true>(P, g, g.e, [&](int n, int m, float2 Y, float2 dY) {
-      const float2 l = Lc[tri(n) + m];
-      const float w2 = m == 0 ? 1.f : 2.f;
-      const float re = l.x * Y.x - l.y * Y.y;
-      const float red = l.x * dY.x - l.y * dY.y;
-      const float rei = -(l.x * Y.y + l.y * Y.x);
-      pot += w2 * re;
-      s0 += w2 * re * (float)n;
-      s1 += w2 * red;
-      s2 += w2 * rei * (float)m;
-    });
-    s0 = g.r != 0.f ? s0 / g.r : 0.f;
-    if (ok) {
-      const float st = g.s, ct = g.c, cp = g.e.x, sp = g.e.y, r = g.r;
-      float fx = st * cp * s0, fy = st * sp * s0, fz = ct * s0;
-      if (r != 0.f) {
-        fx += ct * cp / r * s1;
-        fy += ct * sp / r * s1;
-        fz -= st / r * s1;
-        if (st != 0.f) {
-          fx -= sp / r / st * s2;
-          fy += cp / r / st * s2;
-        }
-      }
-      double4 &d = out[b];  // the gradient back to the input units
-      d.x += pot;
-      d.y += fx * sc;
-      d.z += fy * sc;
-      d.w += fz * sc;
+  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbodies) return;
+  const int w = body_leaf[b];
+  const float sc = lsc[w];
+  const float2 *Lw = Lf + (size_t)w * nt;
+  const float4 B = srcf[b];
+  const SphF g = sph_of_f(B.x * sc, B.y * sc, B.z * sc);
+  float pot = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
+  regular_all_f<PT, true>(P, g, g.e, [&](int n, int m, float2 Y, float2 dY) {
+    const float2 l = __ldg(Lw + tri(n) + m);
+    const float w2 = m == 0 ? 1.f : 2.f;
+    const float re = l.x * Y.x - l.y * Y.y;
+    const float red = l.x * dY.x - l.y * dY.y;
+    const float rei = -(l.x * Y.y + l.y * Y.x);
+    pot += w2 * re;
+    s0 += w2 * re * (float)n;
+    s1 += w2 * red;
+    s2 += w2 * rei * (float)m;
+  });
+  s0 = g.r != 0.f ? s0 / g.r : 0.f;
+  const float st = g.s, ct = g.c, cp = g.e.x, sp = g.e.y, r = g.r;
+  float fx = st * cp * s0, fy = st * sp * s0, fz = ct * s0;
+  if (r != 0.f) {
+    fx += ct * cp / r * s1;
+    fy += ct * sp / r * s1;
+    fz -= st / r * s1;
+    if (st != 0.f) {
+      fx -= sp / r / st * s2;
+      fy += cp / r / st * s2;
     }
   }
+  double4 &d = out[b];  // the gradient back to the input units
+  d.x += pot;
+  d.y += fx * sc;
+  d.z += fy * sc;
+  d.w += fz * sc;
 }
 
 // M2M and L2L.  A child sits at its parent's centre +-R_child on every
@@ -733,10 +731,8 @@ void expansions_set_attributes() {
   cudaFuncSetAttribute(k_l2p, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 #define EXAFMM_F32_ATTR(p)                                                                     \
   cudaFuncSetAttribute(k_p2m_f32<p>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
-  cudaFuncSetAttribute(k_p2m_f32t<p>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
-  cudaFuncSetAttribute(k_l2p_f32<p>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_p2m_f32t<p>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_p2m_f32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_l2p_f32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   EXAFMM_UNROLLED_ORDERS(EXAFMM_F32_ATTR)
 #undef EXAFMM_F32_ATTR
   cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -892,16 +888,25 @@ void downward_pass(Handle &h, cudaStream_t s, cudaEvent_t before_l2p) {
     h.launches++;
     FMM_LAUNCH();
   }
-  // L2P adds into the near-field sums
-  if (before_l2p) FMM_CUDA(cudaStreamWaitEvent(s, before_l2p, 0));
+  // L2P adds into the near-field sums; the mixed form's leaf expansions are
+  // prepared before the wait for the near field
+  float2 *Lf = nullptr;
+  float *lsc = nullptr;
   if (h.prm.precision == EXAFMM_MIXED) {
     make_srcf(h);
-    const dim3 grid(grid_for(h.nleaves, WARPS)), block(WARPS * 32);
-    const size_t sm = WARPS * nt * sizeof(float2);
+    const size_t nlf = (size_t)h.nleaves * nt;
+    h.l2p_f.need(nlf * sizeof(float2) + (size_t)h.nleaves * sizeof(float) + 16);
+    Lf = h.l2p_f.as<float2>();
+    lsc = (float *)(Lf + nlf);
+    k_l2p_prep<<<grid_for((long)nlf, 256), 256, 0, s>>>(h.leaves.as<int>(), h.nleaves, h.c_xr.as<double4>(),
+                                                         h.L.as<double2>(), nt, Lf, lsc);
+    h.launches++;
+  }
+  if (before_l2p) FMM_CUDA(cudaStreamWaitEvent(s, before_l2p, 0));
+  if (h.prm.precision == EXAFMM_MIXED) {
     auto args = [&](auto kernel) {
-      kernel<<<grid, block, sm, s>>>(h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(),
-                                     h.c_xr.as<double4>(), h.srcf.as<float4>(), h.L.as<double2>(),
-                                     h.out.as<double4>(), P);
+      kernel<<<grid_for(h.n, 128), 128, 0, s>>>((long)h.n, h.body_leaf.as<int>(), h.srcf.as<float4>(), Lf, lsc,
+                                                h.out.as<double4>(), P);
     };
     switch (P) {
 #define EXAFMM_L2P_CASE(p) \

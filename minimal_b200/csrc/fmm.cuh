@@ -115,6 +115,8 @@ struct Handle {
   Buf out;     // double4 (p,Fx,Fy,Fz), tree order
   Buf perm;    // int, tree position -> input index
   Buf srcf;    // float4 (x,y,z rel. to leaf centre, q), tree order (mixed form)
+  Buf body_leaf;  // int, tree order: the leaf slot (index into `leaves`) of each body (mixed form)
+  Buf l2p_f;      // mixed-form L2P: FP32 local expansions of the leaves in leaf units, then their scales
   bool srcf_ready = false;  // srcf matches the current tree
   Buf stage;   // staging for Body records crossing the boundary
 

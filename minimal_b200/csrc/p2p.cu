@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(DT) k_direct(const double4 *tgt, long nt, cons
 // rounding), so the pair offset dx = (xi - ci) + (ci - cj) - (xj - cj) keeps
 // the bits that an FP32 copy of the absolute coordinates would lose.
 __global__ void k_make_srcf(const int *leaves, int nleaves, const int *begin, const int *count, const double4 *xr,
-                            const double4 *src, float4 *srcf) {
+                            const double4 *src, float4 *srcf, int *body_leaf) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= nleaves) return;
   const int c = leaves[w];
@@ -124,6 +124,7 @@ __global__ void k_make_srcf(const int *leaves, int nleaves, const int *begin, co
   for (int b = begin[c] + lane; b < begin[c] + count[c]; b += 32) {
     const double4 B = src[b];
     srcf[b] = make_float4((float)(B.x - C.x), (float)(B.y - C.y), (float)(B.z - C.z), (float)B.w);
+    body_leaf[b] = w;
   }
 }
 
@@ -636,13 +637,15 @@ __global__ void __launch_bounds__(CT, F32 ? 7 : 5) k_p2p_cta(const int *leaves, 
 
 }  // namespace
 
-// The FP32 leaf-relative copy of the bodies (mixed form), once per tree.
+// The FP32 leaf-relative copy of the bodies (mixed form) and each body's
+// leaf slot, once per tree (and charge set).
 void make_srcf(Handle &h) {
   if (h.srcf_ready) return;
   h.srcf.need((size_t)h.n * sizeof(float4));
+  h.body_leaf.need((size_t)h.n * sizeof(int));
   k_make_srcf<<<grid_for((long)h.nleaves * 32, 256), 256, 0, h.stream>>>(
       h.leaves.as<int>(), h.nleaves, h.c_begin.as<int>(), h.c_count.as<int>(), h.c_xr.as<double4>(),
-      h.src.as<double4>(), h.srcf.as<float4>());
+      h.src.as<double4>(), h.srcf.as<float4>(), h.body_leaf.as<int>());
   h.launches++;
   FMM_LAUNCH();
   h.srcf_ready = true;
