@@ -253,6 +253,52 @@ __global__ void __launch_bounds__(SEG_WARPS * 32) k_order_segments(const int *of
   }
 }
 
+// The same order as a 32-bit key, (loop << 27) | pre, for trees of fewer
+// than 2^27 cells (the common case): rank sort with the keys read four at a
+// time and two entries ranked per pass, half the shared memory of the
+// 64-bit version (so more warps per SM).
+__device__ __forceinline__ u32 order_key32(u32 e, const int *pre) {
+  const u32 img = e >> IMG_SHIFT;
+  const u32 x = img % 3, y = (img / 3) % 3, z = img / 9;
+  return ((x * 9 + y * 3 + z) << 27) | (u32)pre[e & IDX_MASK];
+}
+
+constexpr int SEG32_SMEM = 512;  // keys per warp held in shared memory
+
+__global__ void __launch_bounds__(SEG_WARPS * 32) k_order_segments32(const int *off, int ncells, const u32 *in,
+                                                                    u32 *out, const int *pre) {
+  __shared__ __align__(16) u32 keys[SEG_WARPS][SEG32_SMEM];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * SEG_WARPS + wid;
+  if (w >= ncells) return;
+  const int b = off[w], m = off[w + 1] - b;
+  if (m > SEG32_SMEM) {  // long segments: rank from global memory
+    for (int a = lane; a < m; a += 32) {
+      const u32 e = in[b + a], key = order_key32(e, pre);
+      int r = 0;
+      for (int k = 0; k < m; k++) r += order_key32(in[b + k], pre) < key;
+      out[b + r] = e;
+    }
+    return;
+  }
+  const int m4 = (m + 3) & ~3;  // padded with keys that rank below none
+  for (int a = lane; a < m4; a += 32) keys[wid][a] = a < m ? order_key32(in[b + a], pre) : 0xFFFFFFFFu;
+  __syncwarp();
+  const uint4 *k4 = (const uint4 *)keys[wid];
+  for (int a = lane; a < m; a += 64) {
+    const bool two = a + 32 < m;
+    const u32 key0 = keys[wid][a], key1 = two ? keys[wid][a + 32] : 0u;
+    int r0 = 0, r1 = 0;
+    for (int k = 0; k < m4 / 4; k++) {
+      const uint4 q = k4[k];
+      r0 += (q.x < key0) + (q.y < key0) + (q.z < key0) + (q.w < key0);
+      r1 += (q.x < key1) + (q.y < key1) + (q.z < key1) + (q.w < key1);
+    }
+    out[b + r0] = in[b + a];
+    if (two) out[b + r1] = in[b + a + 32];
+  }
+}
+
 }  // namespace
 
 // CSR by target from the raw (target, source) pairs.  With `order` the
@@ -276,8 +322,12 @@ static void bucket(Handle &h, const int2 *raw, unsigned long long *n_dev, int64_
   k_bucket<<<g, TB, 0, s>>>(raw, n_dev, (u64)n, off_b.as<int>(), cnt, order ? tmp : ent_b.as<u32>());
   h.launches += 2;
   if (order) {
-    k_order_segments<<<grid_for(C, SEG_WARPS), SEG_WARPS * 32, 0, s>>>(off_b.as<int>(), C, tmp, ent_b.as<u32>(),
-                                                                      h.c_pre.as<int>());
+    if (C < (1 << 27))
+      k_order_segments32<<<grid_for(C, SEG_WARPS), SEG_WARPS * 32, 0, s>>>(off_b.as<int>(), C, tmp,
+                                                                          ent_b.as<u32>(), h.c_pre.as<int>());
+    else
+      k_order_segments<<<grid_for(C, SEG_WARPS), SEG_WARPS * 32, 0, s>>>(off_b.as<int>(), C, tmp, ent_b.as<u32>(),
+                                                                        h.c_pre.as<int>());
     h.launches++;
   }
   FMM_LAUNCH();
