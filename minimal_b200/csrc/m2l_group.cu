@@ -53,7 +53,11 @@ namespace {
 constexpr int TB = 256;
 constexpr int IMG_SHIFT = 26;
 constexpr u32 IDX_MASK = (1u << IMG_SHIFT) - 1;
-constexpr int XS = 36;      // padded row stride of the staged multipoles (doubles)
+// Row stride (doubles) of the FP64 contraction's staged multipoles: target
+// rows of KP values, padded to 4 mod 16 so that the DMMA B-fragment reads
+// (8 rows x 4 consecutive k per instruction) take the minimum two wavefronts.
+__host__ __device__ constexpr int gp_kpad(int KP) { return KP + 4; }  // KP is a multiple of 16
+static_assert(GP_WARPS * 32 == GP_TILE * 8, "k_gemm64 copies each staged row with 8 threads");
 constexpr int TC_TILE = 128;    // targets per tile on the tensor core (MMA M)
 constexpr int TC_EPI_WARPS = 4; // warps 0-3: epilogue (warp w owns TMEM lanes 32w..32w+31)
 constexpr int TC_LOAD_WARP = 4; // first of the producer warps
@@ -584,11 +588,27 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// Largest tile t < ntiles with tg_off[t] <= s (the tile holding segment s,
+// for s below the segment count).
+__device__ __forceinline__ int tile_at(const int *tg_off, int ntiles, int s) {
+  int lo = 0, hi = ntiles - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tg_off[mid] <= s) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// First segment of CTA c of G when nseg segments are cut into equal ranges.
+__device__ __forceinline__ int range_start(int nseg, int c, int G) { return (int)((long long)nseg * c / G); }
+
 __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, const int *tg_off, const int *tg_gid,
                                                           const int *tg_src, const double *ops, const double *Mt,
-                                                          const double4 *xr, double2 *L, PlanDev pd, int nstage) {
+                                                          const double4 *xr, double2 *L, PlanDev pd, int nstage,
+                                                          int ntiles, double2 *part) {
   extern __shared__ __align__(16) double smd[];  // nstage x (operator, gathered multipoles); then the reduction
-  const int tile = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int pc[GP_MAXP], wo[GP_MAXP];
 #pragma unroll
   for (int p = 0; p < GP_MAXP; p++) {
@@ -596,28 +616,49 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
     wo[p] = pc[p] >= 0 ? pd.woff[pc[p] & 255] : 0;
   }
   double acc[GP_MAXP][4][2];
-#pragma unroll
-  for (int p = 0; p < GP_MAXP; p++)
-#pragma unroll
-    for (int cb = 0; cb < 4; cb++) acc[p][cb][0] = acc[p][cb][1] = 0;
   const int KP = pd.KP;
-  const size_t sstride = (size_t)pd.wsize + (size_t)KP * XS;  // doubles per stage (even: 16-byte rows)
+  const int KPAD = gp_kpad(KP);
+  const size_t sstride = (size_t)pd.wsize + (size_t)GP_TILE * KPAD;  // doubles per stage (even: 16-byte rows)
   const int ar = lane >> 2, ak = lane & 3;
   // group g's operator and its 32 gathered multipoles into stage b, as
-  // asynchronous copies (absent targets: zeros)
+  // asynchronous copies (absent targets: zeros).  The multipoles stay in
+  // rows (target-major, X[col][k]): each source row, KP contiguous doubles,
+  // is copied in 16-byte chunks by 8 threads (thread t: row t / 8, chunks
+  // t % 8, t % 8 + 8, ...), one index load per row.
+  const int xcol = tid >> 3, xpart = tid & 7;
   auto issue = [&](int g, int b) {
     double *Wd = smd + (size_t)b * sstride, *Xd = Wd + pd.wsize;
     const double *Wg = ops + (size_t)tg_gid[g] * pd.wsize;
     for (int i = tid; i < pd.wsize / 2; i += blockDim.x) tc::cp_async16(Wd + 2 * i, Wg + 2 * i, 16u);
-    for (int i = tid; i < GP_TILE * KP; i += blockDim.x) {
-      const int col = i / KP, k = i - col * KP;
-      const int s = tg_src[(long)g * GP_TILE + col];
-      tc::cp_async8(Xd + k * XS + col, Mt + (long)(s >= 0 ? s : 0) * KP + k, s >= 0 ? 8u : 0u);
-    }
+    const int s = tg_src[(long)g * GP_TILE + xcol];
+    const double *src = Mt + (long)(s >= 0 ? s : 0) * KP;
+    double *dst = Xd + xcol * KPAD;
+    for (int c = xpart; c < KP / 2; c += 8) tc::cp_async16(dst + 2 * c, src + 2 * c, s >= 0 ? 16u : 0u);
     tc::cp_async_commit();
   };
-  const int g0 = tg_off[tile], g1 = tg_off[tile + 1];
-  if (nstage == 2 && g0 < g1) issue(g0, 0);
+  // this CTA's segments [r0, r1): with `part`, an equal range of all the
+  // segments (tiles cut by a range boundary are written to `part` and added
+  // by k_m2l_join, as in k_m2l_tc); else tile blockIdx.x
+  int r0, r1, tfirst;
+  if (part) {
+    const int nseg = tg_off[ntiles];
+    r0 = range_start(nseg, blockIdx.x, gridDim.x);
+    r1 = range_start(nseg, blockIdx.x + 1, gridDim.x);
+    tfirst = r1 > r0 ? tile_at(tg_off, ntiles, r0) : ntiles;
+  } else {
+    tfirst = blockIdx.x;
+    r0 = tg_off[tfirst];
+    r1 = tg_off[tfirst + 1];
+  }
+  for (int tile = tfirst; tile < ntiles; tile++) {
+  const int g0 = max(r0, tg_off[tile]), g1 = min(r1, tg_off[tile + 1]);
+  if (g0 >= r1) break;
+  if (g1 <= g0) continue;  // no segments: L stays zero
+#pragma unroll
+  for (int p = 0; p < GP_MAXP; p++)
+#pragma unroll
+    for (int cb = 0; cb < 4; cb++) acc[p][cb][0] = acc[p][cb][1] = 0;
+  if (nstage == 2) issue(g0, 0);
   for (int g = g0; g < g1; g++) {
     // two stages: the next group's copies run while this one is contracted
     const int b = nstage == 2 ? (g - g0) & 1 : 0;
@@ -639,9 +680,9 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
       const double *Wb = Wsm + wo[p];
       for (int k = k0; k < k1; k += 4) {
         const double a = Wb[(k + ak) * 8 + ar];
-        const double *xb = Xsm + (k + ak) * XS + ar;
+        const double *xb = Xsm + ar * KPAD + k + ak;
 #pragma unroll
-        for (int cb = 0; cb < 4; cb++) dmma(acc[p][cb][0], acc[p][cb][1], a, xb[cb * 8]);
+        for (int cb = 0; cb < 4; cb++) dmma(acc[p][cb][0], acc[p][cb][1], a, xb[cb * 8 * KPAD]);
       }
     }
     __syncthreads();  // stage b is free for group g + 2
@@ -664,7 +705,9 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
     }
     __syncthreads();
   }
-  // unscale (L = L~ / R_t^(j+1)) and store
+  // unscale (L = L~ / R_t^(j+1)) and store, or write the part
+  const bool whole = tg_off[tile] >= r0 && tg_off[tile + 1] <= r1;
+  double2 *slot = whole ? nullptr : part + (size_t)(2 * blockIdx.x + (tile == tfirst ? 0 : 1)) * GP_TILE * pd.NT;
   for (int i = tid; i < GP_TILE * pd.NT; i += blockDim.x) {
     const int col = i / pd.NT, o = i - col * pd.NT;
     const int t = tile_tgt[tile * GP_TILE + col];
@@ -674,7 +717,11 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
     const double inv = 1.0 / xr[t].w;
     double s = inv;
     for (int q = 0; q < j; q++) s *= inv;
-    L[(long)t * pd.NT + o] = make_double2(Y[(2 * o) * GP_TILE + col] * s, Y[(2 * o + 1) * GP_TILE + col] * s);
+    const double2 v = make_double2(Y[(2 * o) * GP_TILE + col] * s, Y[(2 * o + 1) * GP_TILE + col] * s);
+    if (whole) L[(long)t * pd.NT + o] = v;
+    else slot[i] = v;
+  }
+  __syncthreads();  // the next tile's copies reuse the reduction's shared memory
   }
 }
 
@@ -810,21 +857,6 @@ __device__ __forceinline__ void tc_flush_global(uint32_t acc, int t, double inv,
 
 // PT > 0: the order PT with its plan and stage count as compile-time
 // constants (the run-time arguments are then ignored); PT = 0: any order.
-// Largest tile t < ntiles with tg_off[t] <= s (the tile holding segment s,
-// for s below the segment count).
-__device__ __forceinline__ int tile_at(const int *tg_off, int ntiles, int s) {
-  int lo = 0, hi = ntiles - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (tg_off[mid] <= s) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-// First segment of CTA c of G when nseg segments are cut into equal ranges.
-__device__ __forceinline__ int range_start(int nseg, int c, int G) { return (int)((long long)nseg * c / G); }
-
 // Work split of the orders compiled with their plan and a running sum in
 // TMEM ("balanced"): one CTA per SM, each taking an equal contiguous range of
 // the (tile, group) segments -- the tiles hold 182 to 325 segments at 1M
@@ -1110,13 +1142,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
   if (warp == TC_MMA_WARP) tc::dealloc(tmem, ncols);
 }
 
-// Tiles cut by the balanced ranges of k_m2l_tc: L of the tile's targets is
-// the sum of the CTAs' parts, added in CTA order.  One CTA per tile; threads
-// run over (target row, coefficient) with the coefficient fastest, so the
-// parts and L are read and written contiguously.
+// Tiles cut by the balanced ranges of k_m2l_tc / k_gemm64 (tiles of tile_n
+// targets): L of the tile's targets is the sum of the CTAs' parts, added in
+// CTA order.  One CTA per tile; threads run over (target row, coefficient)
+// with the coefficient fastest, so the parts and L are read and written
+// contiguously.
 constexpr int JOIN_T = 256;
 __global__ void __launch_bounds__(JOIN_T) k_m2l_join(const int *tile_tgt, const int *tg_off, int ntiles, int G,
-                                                     const double2 *part, int NT, double2 *L) {
+                                                     const double2 *part, int NT, int tile_n, double2 *L) {
   const int t = blockIdx.x, nseg = tg_off[ntiles];
   const int a = tg_off[t], b = tg_off[t + 1];
   if (b <= a) return;
@@ -1133,13 +1166,13 @@ __global__ void __launch_bounds__(JOIN_T) k_m2l_join(const int *tile_tgt, const 
   // start inside it; for c0 it is the last (slot 1) unless c0's range
   // starts at the tile
   const int slot0 = range_start(nseg, c0, G) < a ? 1 : 0;
-  for (int e = threadIdx.x; e < TC_TILE * NT; e += JOIN_T) {
-    const int row = e / NT, o = e - row * NT, tgt = tile_tgt[t * TC_TILE + row];
+  for (int e = threadIdx.x; e < tile_n * NT; e += JOIN_T) {
+    const int row = e / NT, o = e - row * NT, tgt = tile_tgt[t * tile_n + row];
     if (tgt < 0) continue;
     double2 sum = make_double2(0, 0);
     for (int c = c0; c <= c1; c++) {
       const int slot = c == c0 ? slot0 : 0;
-      const double2 v = part[(size_t)(2 * c + slot) * TC_TILE * NT + e];
+      const double2 v = part[(size_t)(2 * c + slot) * tile_n * NT + e];
       sum.x += v.x;
       sum.y += v.y;
     }
@@ -1190,7 +1223,7 @@ PlanDev plan_dev(const PlanCache &pc) {
 }
 
 size_t gemm64_smem(const GroupPlan &g, int nstage = 1) {
-  const size_t stage = (size_t)g.wsize + (size_t)g.KP * XS;
+  const size_t stage = (size_t)g.wsize + (size_t)GP_TILE * gp_kpad(g.KP);
   const size_t red = (size_t)g.nrb * 8 * GP_TILE;
   return std::max(nstage * stage, red) * sizeof(double);
 }
@@ -1254,18 +1287,41 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
       default: launch(k_m2l_tc<0>);
     }
     if (bal) {
-      k_m2l_join<<<ntiles, JOIN_T, 0, s>>>(h.g_tile.as<int>(), tg_off, ntiles, G, part, NT, h.L.as<double2>());
+      k_m2l_join<<<ntiles, JOIN_T, 0, s>>>(h.g_tile.as<int>(), tg_off, ntiles, G, part, NT, TC_TILE,
+                                          h.L.as<double2>());
       h.launches++;
     }
     h.tc_stall_ns = 0;  // the test hook stalls one launch
     FMM_CUDA(cudaMemcpyAsync(h.flags_host, &ctr->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s));
     h.g_used_tc = true;
   } else {
-    // two pipeline stages where they fit in shared memory (P <= 12), else one
+    // two pipeline stages where they fit in shared memory (P <= 12), else
+    // one.  P <= 10: equal segment ranges over as many CTAs as fit on the GPU
+    // at once (at 1M uniform bodies 7.82 -> 7.29 ms per evaluation at P = 8,
+    // 9.03 -> 8.47 at P = 10); above, one CTA per tile (P = 12: 10.87
+    // against 11.13 ms with the ranges)
     const int nst = gemm64_smem(gp, 2) <= TC_SMEM_MAX ? 2 : 1;
-    k_gemm64<<<ntiles, GP_WARPS * 32, gemm64_smem(gp, nst), s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src,
-                                                                 h.g_ops.as<double>(), h.g_mt.as<double>(),
-                                                                 h.c_xr.as<double4>(), h.L.as<double2>(), pd, nst);
+    const size_t smem = gemm64_smem(gp, nst);
+    const bool bal = P <= 10;
+    int G = ntiles;
+    const int NT = tri(P);
+    double2 *part = nullptr;
+    if (bal) {
+      int occ = 1;
+      FMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_gemm64, GP_WARPS * 32, smem));
+      if (h.nsm == 0) FMM_CUDA(cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.prm.device));
+      G = std::max(1, std::min(ntiles, h.nsm * std::max(occ, 1)));
+      h.g_part.need((size_t)G * 2 * GP_TILE * NT * sizeof(double2));
+      part = h.g_part.as<double2>();
+    }
+    k_gemm64<<<G, GP_WARPS * 32, smem, s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src, h.g_ops.as<double>(),
+                                            h.g_mt.as<double>(), h.c_xr.as<double4>(), h.L.as<double2>(), pd, nst,
+                                            ntiles, part);
+    if (bal) {
+      k_m2l_join<<<ntiles, JOIN_T, 0, s>>>(h.g_tile.as<int>(), tg_off, ntiles, G, part, NT, GP_TILE,
+                                          h.L.as<double2>());
+      h.launches++;
+    }
   }
   h.launches++;
 }
