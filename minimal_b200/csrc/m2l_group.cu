@@ -232,20 +232,36 @@ __global__ void k_gops(const int *keys, const int *slots, PlanDev pd, double *op
 // 16 * ksteps input columns.  Each block is stored K-major with the 128-byte
 // swizzle: atoms of 64 input columns, each atom `rows` x 128 bytes.  The
 // multipole tile (A) is 128 rows x atomsA atoms, hi and lo parts.
+//
+// The operator image (hi and lo parts, 2 * bimg bytes, one bulk copy) holds
+// the blocks one after the other.  A block's region holds its hi atoms and
+// its lo atoms: all hi atoms then all lo atoms, or -- a "paired" block --
+// each hi atom followed by its lo atom, so that the hi and lo rows form one
+// B operand of 2 * rows rows: one MMA then makes hi*hi and hi*lo together
+// (A read once), into 2 * rows accumulator columns (the products of the hi
+// rows, then those of the lo rows, added by the epilogue), and the lo*hi
+// MMA adds into the second half.  Block b's accumulator columns start at
+// dcol[b].
 struct TcPlan {
   int nb;                            // output row blocks
-  int rows[4], ksteps[4], boff[4];   // rows, K steps of 16, byte offset in one image
-  int bimg;                          // bytes of one (hi or lo) operator image
+  int rows[4], ksteps[4];            // rows, K steps of 16
+  int boff[4];                       // byte offset of the block's region in the image
+  int astride[4], lodelta[4];        // bytes from one hi atom to the next; from a hi atom to its lo atom
+  int pair[4];                       // paired block
+  int dcol[4];                       // first accumulator column
+  int accw;                          // accumulator columns
+  int bimg;                          // half the bytes of the operator image
   int atomsA;                        // 64-column atoms of the multipole tile
   int abytes;                        // bytes of one (hi or lo) multipole tile
 };
 
 constexpr int tc_tri(int n) { return n * (n + 1) / 2; }
 
-constexpr TcPlan make_tc_plan(int P, int KP) {
+// pair_first: block 0 is paired (the orders whose accumulators leave room)
+constexpr TcPlan make_tc_plan(int P, int KP, bool pair_first) {
   TcPlan t{};
   t.nb = (KP + 63) / 64;
-  int off = 0;
+  int off = 0, col = 0;
   for (int b = 0; b < t.nb; b++) {
     t.rows[b] = KP - 64 * b < 64 ? KP - 64 * b : 64;
     int j = 0;
@@ -253,14 +269,25 @@ constexpr TcPlan make_tc_plan(int P, int KP) {
     const int kreal = 2 * tc_tri(P - j);
     const int k16 = (kreal + 15) / 16 * 16;
     t.ksteps[b] = (k16 < KP ? k16 : KP) / 16;
+    const int natoms = (t.ksteps[b] + 3) / 4, ab = t.rows[b] * 128;
+    t.pair[b] = pair_first && b == 0;
     t.boff[b] = off;
-    off += (t.ksteps[b] + 3) / 4 * t.rows[b] * 128;
+    t.astride[b] = t.pair[b] ? 2 * ab : ab;
+    t.lodelta[b] = t.pair[b] ? ab : natoms * ab;
+    off += 2 * natoms * ab;
+    t.dcol[b] = col;
+    col += (t.pair[b] ? 2 : 1) * t.rows[b];
   }
-  t.bimg = off;
+  t.accw = col;
+  t.bimg = off / 2;
   t.atomsA = (KP + 63) / 64;
   t.abytes = TC_TILE * 128 * t.atomsA;
   return t;
 }
+
+// Orders whose block 0 is paired: P = 8 and 10, where two accumulators of
+// the wider block 0 and an FP32 running sum fit in TMEM.
+constexpr bool tc_pair_first(int P) { return P == 8 || P == 10; }
 
 constexpr size_t TC_SMEM_MAX = 227 * 1024;  // opt-in shared memory per CTA on sm_100
 
@@ -314,7 +341,11 @@ constexpr TcAcc tc_acc_layout(int KP) {
 // sum's round-to-nearest adds are unbiased, ~sqrt(windows) * 2^-24 relative
 // (about 6e-7 over the ~95 windows of a tile at P = 10, far below the
 // expansion's error).  Otherwise the layout above.
-constexpr TcAcc tc_acc_fixed(int KP) {
+constexpr TcAcc tc_acc_fixed(int KP, const TcPlan &t) {
+  if (t.pair[0]) {  // two accumulators of the paired width (64-column steps) and an FP32 running sum
+    const uint32_t st = ((uint32_t)t.accw + 63u) / 64u * 64u;
+    if (2 * st + (uint32_t)KP <= 512) return TcAcc{2, 3, st, 2 * st, 0, 512};
+  }
   const uint32_t hc = tc_half_cols(KP);
   if (5 * hc <= 512) return TcAcc{3, 1, hc, 3 * hc, 4 * hc, 5 * hc <= 256 ? 256u : 512u};
   if (4 * hc <= 512) return TcAcc{3, 2, hc, 3 * hc, 0, 512};
@@ -329,9 +360,9 @@ constexpr TcAcc tc_acc_fixed(int KP) {
 template <int PT>
 struct TcFixed {
   static constexpr int KP = tc_kp(PT);
-  static constexpr TcPlan plan = make_tc_plan(PT, KP);
+  static constexpr TcPlan plan = make_tc_plan(PT, KP, tc_pair_first(PT));
   static constexpr int nstage = tc_stages(plan);
-  static constexpr TcAcc acc = tc_acc_fixed(KP);
+  static constexpr TcAcc acc = tc_acc_fixed(KP, plan);
 };
 
 // One CTA per group: the operator split into FP16 hi + lo parts, written as
@@ -341,19 +372,25 @@ __global__ void k_gops16(const int *keys, const int *slots, int P, TcPlan pl, __
   const int NT = tri(P);
   const int dl = group_harmonics(keys[blockIdx.x], P, Zsh, kg);
   const int nh = pl.bimg / 2;  // halves per image
-  __half *Wh = ops16 + (size_t)slots[blockIdx.x] * 2 * nh, *Wl = Wh + nh;
+  __half *Wh = ops16 + (size_t)slots[blockIdx.x] * 2 * nh;  // the whole image (hi and lo parts)
   for (int e = threadIdx.x; e < nh; e += blockDim.x) {
     const int byte = 2 * e;
-    int b = 0;
-    while (b + 1 < pl.nb && pl.boff[b + 1] <= byte) b++;
-    const int ab = pl.rows[b] * 128, rem = byte - pl.boff[b];
+    // `byte` enumerates the hi values block by block, atom by atom; its hi
+    // and lo values go to their places in the block's region
+    int b = 0, lb = 0;  // block, and its first byte in this enumeration
+    while (b + 1 < pl.nb && lb + (pl.ksteps[b] + 3) / 4 * pl.rows[b] * 128 <= byte) {
+      lb += (pl.ksteps[b] + 3) / 4 * pl.rows[b] * 128;
+      b++;
+    }
+    const int ab = pl.rows[b] * 128, rem = byte - lb;
     const int a = rem / ab, r2 = rem - a * ab;
     const int rb = r2 >> 7, chunk = (r2 >> 4) & 7, q = (r2 >> 1) & 7;
     const int k = a * 64 + ((chunk ^ (rb & 7)) << 3) + q;  // undo the swizzle
     const double w = k < 16 * pl.ksteps[b] ? op_value(64 * b + rb, k, P, NT, dl, Zsh) : 0.0;
     const __half hi = __double2half(w);
-    Wh[e] = hi;
-    Wl[e] = __double2half(w - (double)__half2float(hi));
+    const int ph = pl.boff[b] + a * pl.astride[b] + r2;  // the hi value's byte in the image
+    Wh[ph / 2] = hi;
+    Wh[(ph + pl.lodelta[b]) / 2] = __double2half(w - (double)__half2float(hi));
   }
 }
 
@@ -783,6 +820,29 @@ __device__ __forceinline__ void tc_fold32(uint32_t acc, uint32_t hi, int cb, int
   tc::wait_st();
 }
 
+// tc_fold32 for a plan with paired blocks: output column c of block b is
+// the sum of accumulator columns dcol[b] + w and, paired, dcol[b] + rows[b]
+// + w (w = c - 64 b).
+__device__ __forceinline__ void tc_fold_paired(uint32_t acc, uint32_t sum, const TcPlan &pl, int KP) {
+  for (int c0 = 0; c0 < KP; c0 += 16) {
+    const int b = c0 >> 6, w = c0 - 64 * b;
+    const uint32_t big = acc + (uint32_t)(pl.dcol[b] + w);
+    uint32_t a[16], m[16], h[16];
+    tc::ld_32x32b_x16_async(big, a);
+    if (pl.pair[b]) tc::ld_32x32b_x16_async(big + (uint32_t)pl.rows[b], m);
+    tc::ld_32x32b_x16_async(sum + (uint32_t)c0, h);
+    tc::wait_ld();
+    if (!pl.pair[b])
+#pragma unroll
+      for (int k = 0; k < 16; k++) m[k] = 0u;
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      h[k] = __float_as_uint(__uint_as_float(h[k]) + (__uint_as_float(a[k]) + __uint_as_float(m[k])));
+    tc::st_32x32b_x16(sum + (uint32_t)c0, h);
+  }
+  tc::wait_st();
+}
+
 __device__ __forceinline__ void tc_zero(uint32_t cols, int cb, int ce) {
   const uint32_t z[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int c0 = cb; c0 < ce; c0 += 16) tc::st_32x32b_x16(cols + (uint32_t)c0, z);
@@ -955,6 +1015,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         const uint32_t acc = lanes + (uint32_t)a * ta.stride;
         if (fold == 1) tc_fold(acc, sum_hi, sum_lo, 0, KP);
         else if (fold == 2) tc_fold32(acc, sum_hi, 0, KP);
+        else if (fold == 3) tc_fold_paired(acc, sum_hi, pl, KP);
         else tc_flush_global(acc, t, inv, us, 0, KP, NT, L);
         tc::fence_before();
         __syncwarp();
@@ -1057,13 +1118,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
     // hi*hi + hi*lo + lo*hi into the window's accumulator
     if (lane == 0) {
       int rows[4], ksteps[4];
-      uint32_t boff[4], idesc[4];
+      uint32_t boff[4], idesc[4], idesc2[4];
 #pragma unroll
       for (int b = 0; b < 4; b++) {
         rows[b] = b < pl.nb ? pl.rows[b] : 0;
         ksteps[b] = b < pl.nb ? pl.ksteps[b] : 0;
         boff[b] = b < pl.nb ? (uint32_t)pl.boff[b] : 0u;
         idesc[b] = tc::idesc_f16_f32(TC_TILE, rows[b] > 0 ? rows[b] : 16);
+        idesc2[b] = tc::idesc_f16_f32(TC_TILE, rows[b] > 0 ? 2 * rows[b] : 16);  // paired: hi and lo rows
       }
       // test hook: a wait on a barrier that nothing arrives at, as if the
       // tensor core's inputs never came; it runs out after stall_ns
@@ -1090,7 +1152,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         tc::fence_after();
         const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
         const uint64_t dA = tc::smem_desc_sw128(sA), dB = tc::smem_desc_sw128(sB);
-        const uint64_t lo_a = abytes >> 4, lo_b = bimg >> 4;  // descriptor start fields count 16 bytes
+        const uint64_t lo_a = abytes >> 4;  // descriptor start fields count 16 bytes
         const bool fresh = kf == 0;
         const uint32_t acc = tmem + (uint32_t)a * ta.stride;
         // per K step: hi*hi, then hi*lo with the same A, then lo*hi (issuing
@@ -1102,11 +1164,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
 #pragma unroll
           for (int ks = 0; ks < ksteps[b]; ks++) {
             const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
-            const uint64_t bo = ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * rows[b] * 128 + (uint64_t)(ks & 3) * 32) >> 4;
-            const uint32_t d = acc + 64u * (uint32_t)b;
-            tc::mma_f16(d, dA + ao, dB + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
-            tc::mma_f16(d, dA + ao, dB + lo_b + bo, idesc[b], 1u);
-            tc::mma_f16(d, dA + lo_a + ao, dB + bo, idesc[b], 1u);
+            const uint64_t bo =
+                ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * pl.astride[b] + (uint64_t)(ks & 3) * 32) >> 4;
+            const uint64_t lo_b = (uint64_t)pl.lodelta[b] >> 4;
+            const uint32_t d = acc + (uint32_t)pl.dcol[b];
+            if (pl.pair[b]) {  // hi*hi and hi*lo in one MMA (columns [0, rows) and [rows, 2 rows)), then lo*hi
+              tc::mma_f16(d, dA + ao, dB + bo, idesc2[b], (!fresh || ks > 0) ? 1u : 0u);
+              tc::mma_f16(d + (uint32_t)rows[b], dA + lo_a + ao, dB + bo, idesc[b], 1u);
+            } else {
+              tc::mma_f16(d, dA + ao, dB + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
+              tc::mma_f16(d, dA + ao, dB + lo_b + bo, idesc[b], 1u);
+              tc::mma_f16(d, dA + lo_a + ao, dB + bo, idesc[b], 1u);
+            }
           }
         }
         tc::commit(&empty[st]);
@@ -1230,7 +1299,7 @@ size_t gemm64_smem(const GroupPlan &g, int nstage = 1) {
 
 bool tc_available(int P) {
   const int KP = tc_kp(P);
-  return KP <= 256 && tc_smem(make_tc_plan(P, KP)) <= TC_SMEM_MAX;
+  return KP <= 256 && tc_smem(make_tc_plan(P, KP, tc_pair_first(P))) <= TC_SMEM_MAX;
 }
 
 }  // namespace
@@ -1268,7 +1337,7 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
     // the orders compiled with their plan as constants; those with a running
     // sum in TMEM take balanced segment ranges, one CTA per SM
     const bool fixed = P == 6 || P == 8 || P == 10 || P == 12;
-    const bool bal = fixed && tc_acc_fixed(KP16).fold != 0;
+    const bool bal = fixed && tc_acc_fixed(KP16, tp).fold != 0;
     if (bal && h.nsm == 0) FMM_CUDA(cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.prm.device));
     const int G = bal ? std::min(ntiles, h.nsm) : ntiles, NT = tri(P);
     if (bal) h.g_part.need((size_t)G * 2 * TC_TILE * NT * sizeof(double2));
@@ -1334,7 +1403,7 @@ void m2l_grouped_pass(Handle &h) {
   const PlanDev pd = plan_dev(pc);
   const bool tcore = h.prm.precision == EXAFMM_MIXED && tc_available(P);
   const int KP16 = tc_kp(P);
-  const TcPlan tp = make_tc_plan(P, KP16);
+  const TcPlan tp = make_tc_plan(P, KP16, tc_pair_first(P));
   const int tile_n = tcore ? TC_TILE : GP_TILE;
   const long nent = h.n_m2l;
   h.L.need((size_t)C * NT * sizeof(double2));
