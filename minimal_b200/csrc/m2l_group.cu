@@ -241,13 +241,18 @@ __global__ void k_gops(const int *keys, const int *slots, PlanDev pd, double *op
 // (A read once), into 2 * rows accumulator columns (the products of the hi
 // rows, then those of the lo rows, added by the epilogue), and the lo*hi
 // MMA adds into the second half.  Block b's accumulator columns start at
-// dcol[b].
+// dcol[b].  A "narrow" block (after the first, fewer than four K steps, so
+// less than one 64-column atom: the high output orders need only the low
+// input orders) is stored in the 32-byte swizzle instead: per K step the
+// block's rows x 32 bytes, the two 16-byte chunks of a row swapped where the
+// row's bit 2 is set -- no padding to 128-byte rows to copy.
 struct TcPlan {
   int nb;                            // output row blocks
   int rows[4], ksteps[4];            // rows, K steps of 16
   int boff[4];                       // byte offset of the block's region in the image
   int astride[4], lodelta[4];        // bytes from one hi atom to the next; from a hi atom to its lo atom
   int pair[4];                       // paired block
+  int narrow[4];                     // block in the 32-byte swizzle (one rows x 32-byte slab per K step)
   int dcol[4];                       // first accumulator column
   int accw;                          // accumulator columns
   int bimg;                          // half the bytes of the operator image
@@ -271,10 +276,17 @@ constexpr TcPlan make_tc_plan(int P, int KP, bool pair_first) {
     t.ksteps[b] = (k16 < KP ? k16 : KP) / 16;
     const int natoms = (t.ksteps[b] + 3) / 4, ab = t.rows[b] * 128;
     t.pair[b] = pair_first && b == 0;
+    t.narrow[b] = b > 0 && t.ksteps[b] < 4;
     t.boff[b] = off;
-    t.astride[b] = t.pair[b] ? 2 * ab : ab;
-    t.lodelta[b] = t.pair[b] ? ab : natoms * ab;
-    off += 2 * natoms * ab;
+    if (t.narrow[b]) {
+      t.astride[b] = t.rows[b] * 32;  // bytes per K step
+      t.lodelta[b] = t.ksteps[b] * t.rows[b] * 32;
+      off += 2 * t.ksteps[b] * t.rows[b] * 32;
+    } else {
+      t.astride[b] = t.pair[b] ? 2 * ab : ab;
+      t.lodelta[b] = t.pair[b] ? ab : natoms * ab;
+      off += 2 * natoms * ab;
+    }
     t.dcol[b] = col;
     col += (t.pair[b] ? 2 : 1) * t.rows[b];
   }
@@ -377,18 +389,30 @@ __global__ void k_gops16(const int *keys, const int *slots, int P, TcPlan pl, __
     const int byte = 2 * e;
     // `byte` enumerates the hi values block by block, atom by atom; its hi
     // and lo values go to their places in the block's region
+    auto hsize = [&](int q) {  // bytes of block q's hi part
+      return pl.narrow[q] ? pl.ksteps[q] * pl.rows[q] * 32 : (pl.ksteps[q] + 3) / 4 * pl.rows[q] * 128;
+    };
     int b = 0, lb = 0;  // block, and its first byte in this enumeration
-    while (b + 1 < pl.nb && lb + (pl.ksteps[b] + 3) / 4 * pl.rows[b] * 128 <= byte) {
-      lb += (pl.ksteps[b] + 3) / 4 * pl.rows[b] * 128;
+    while (b + 1 < pl.nb && lb + hsize(b) <= byte) {
+      lb += hsize(b);
       b++;
     }
-    const int ab = pl.rows[b] * 128, rem = byte - lb;
-    const int a = rem / ab, r2 = rem - a * ab;
-    const int rb = r2 >> 7, chunk = (r2 >> 4) & 7, q = (r2 >> 1) & 7;
-    const int k = a * 64 + ((chunk ^ (rb & 7)) << 3) + q;  // undo the swizzle
+    const int rem = byte - lb;
+    int rb, k, ph;  // output row in the block, input column, the hi value's byte in the image
+    if (pl.narrow[b]) {  // undo the 32-byte swizzle
+      const int ts = rem / (pl.rows[b] * 32), w = rem - ts * (pl.rows[b] * 32);
+      rb = w >> 5;
+      k = ts * 16 + ((((w >> 4) & 1) ^ ((rb >> 2) & 1)) << 3) + ((w >> 1) & 7);
+      ph = pl.boff[b] + rem;
+    } else {  // undo the 128-byte swizzle
+      const int ab = pl.rows[b] * 128, a = rem / ab, r2 = rem - a * ab;
+      const int chunk = (r2 >> 4) & 7, q = (r2 >> 1) & 7;
+      rb = r2 >> 7;
+      k = a * 64 + ((chunk ^ (rb & 7)) << 3) + q;
+      ph = pl.boff[b] + a * pl.astride[b] + r2;
+    }
     const double w = k < 16 * pl.ksteps[b] ? op_value(64 * b + rb, k, P, NT, dl, Zsh) : 0.0;
     const __half hi = __double2half(w);
-    const int ph = pl.boff[b] + a * pl.astride[b] + r2;  // the hi value's byte in the image
     Wh[ph / 2] = hi;
     Wh[(ph + pl.lodelta[b]) / 2] = __double2half(w - (double)__half2float(hi));
   }
@@ -1151,7 +1175,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
         if (!ok) break;
         tc::fence_after();
         const uint32_t sA = tc::smem_u32(base + (size_t)st * stage_bytes), sB = sA + 2 * abytes;
-        const uint64_t dA = tc::smem_desc_sw128(sA), dB = tc::smem_desc_sw128(sB);
+        const uint64_t dA = tc::smem_desc_sw128(sA), dB = tc::smem_desc_sw128(sB), dB32 = tc::smem_desc_sw32(sB);
         const uint64_t lo_a = abytes >> 4;  // descriptor start fields count 16 bytes
         const bool fresh = kf == 0;
         const uint32_t acc = tmem + (uint32_t)a * ta.stride;
@@ -1165,10 +1189,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(const int *tile_tgt, c
           for (int ks = 0; ks < ksteps[b]; ks++) {
             const uint64_t ao = ((uint64_t)(ks >> 2) * (TC_TILE * 128) + (uint64_t)(ks & 3) * 32) >> 4;
             const uint64_t bo =
-                ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * pl.astride[b] + (uint64_t)(ks & 3) * 32) >> 4;
+                pl.narrow[b] ? ((uint64_t)boff[b] + (uint64_t)ks * pl.astride[b]) >> 4
+                             : ((uint64_t)boff[b] + (uint64_t)(ks >> 2) * pl.astride[b] + (uint64_t)(ks & 3) * 32) >> 4;
             const uint64_t lo_b = (uint64_t)pl.lodelta[b] >> 4;
             const uint32_t d = acc + (uint32_t)pl.dcol[b];
-            if (pl.pair[b]) {  // hi*hi and hi*lo in one MMA (columns [0, rows) and [rows, 2 rows)), then lo*hi
+            if (pl.narrow[b]) {
+              tc::mma_f16(d, dA + ao, dB32 + bo, idesc[b], (!fresh || ks > 0) ? 1u : 0u);
+              tc::mma_f16(d, dA + ao, dB32 + lo_b + bo, idesc[b], 1u);
+              tc::mma_f16(d, dA + lo_a + ao, dB32 + bo, idesc[b], 1u);
+            } else if (pl.pair[b]) {  // hi*hi and hi*lo in one MMA (columns [0, rows) and [rows, 2 rows)), then lo*hi
               tc::mma_f16(d, dA + ao, dB + bo, idesc2[b], (!fresh || ks > 0) ? 1u : 0u);
               tc::mma_f16(d + (uint32_t)rows[b], dA + lo_a + ao, dB + bo, idesc[b], 1u);
             } else {

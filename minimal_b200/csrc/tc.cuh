@@ -40,6 +40,19 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
   return d;
 }
 
+// Shared-memory matrix descriptor, K-major operand with the 32-byte swizzle:
+// rows of 16 halves (32 bytes), the two 16-byte chunks swapped in rows whose
+// bit 2 is set (256-byte atoms of 8 rows); sbo = 256 (8-row groups).
+__device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;           // leading byte offset: 16 bytes (unused)
+  d |= (uint64_t)(256 >> 4) << 32;  // stride byte offset: 256 bytes
+  d |= (uint64_t)1 << 46;           // descriptor version (Blackwell)
+  d |= (uint64_t)6 << 61;           // layout type: 32-byte swizzle
+  return d;
+}
+
 // Instruction descriptor, kind::f16: A and B f16, K-major; D f32; M x N.
 __host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
   return (1u << 4)                     // D format f32
