@@ -11,19 +11,6 @@ namespace tc {
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Shared-memory matrix descriptor, K-major operand without swizzle: core
-// matrices of 8 rows x 16 bytes; lbo = byte distance between the two 16-byte
-// K chunks of one K=16 step, sbo = byte distance between 8-row groups.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version (Blackwell)
-  // base offset 0, lbo mode 0, layout type 0 = no swizzle
-  return d;
-}
-
 // Shared-memory matrix descriptor, K-major operand with the 128-byte swizzle:
 // rows of 64 halves (128 bytes) whose 16-byte chunks are permuted by
 // chunk ^ (row % 8) within 1024-byte atoms of 8 rows (the layout a TMA load
@@ -153,12 +140,6 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t 
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
                : "memory");
 }
-// 8-byte asynchronous copy global -> shared (through L1); src_bytes = 0
-// writes zeros.
-__device__ __forceinline__ void cp_async8(void *dst, const void *src, uint32_t src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
-               : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 // Arrival on the barrier once all of this thread's earlier cp.async copies
@@ -202,12 +183,6 @@ __device__ __forceinline__ void st_32x32b_x16(uint32_t taddr, const uint32_t *r)
       : "memory");
 }
 __device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
-
-// Element offset of (row, col) in a K-major no-swizzle operand with kp
-// columns: [row/8][col/8][row%8][col%8].
-__host__ __device__ __forceinline__ int canon(int row, int col, int kp) {
-  return (((row >> 3) * (kp >> 3) + (col >> 3)) << 6) + ((row & 7) << 3) + (col & 7);
-}
 
 }  // namespace tc
 }  // namespace fmm
