@@ -41,10 +41,29 @@ thread_local std::string exafmm_b200_static_err;
 namespace {
 
 
+// The handle's device for the duration of a call, whichever device the
+// calling thread has current (a new thread starts on device 0); the
+// caller's device is put back afterwards.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    if (prev != dev) FMM_CUDA(cudaSetDevice(dev));
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 template <class F>
 int guarded(exafmm_b200 *H, F f) {
   if (!H) return EXAFMM_ERR_ARG;
   try {
+    DeviceScope scope(H->h.prm.device);
     f(H->h);
     H->h.err.clear();
     return EXAFMM_OK;
