@@ -152,7 +152,7 @@ __global__ void k_key_of_gid(long nkeys, const int *occ, const int *gidx, int *k
 }
 
 struct PlanDev {
-  int P, NT, KP, nrb, wsize, maxrank;
+  int P, NT, KP, nrb, wsize, maxrank, maxp;
   const int *woff, *jmin, *pieces, *prank;
 };
 
@@ -664,19 +664,21 @@ __device__ __forceinline__ int tile_at(const int *tg_off, int ntiles, int s) {
 // First segment of CTA c of G when nseg segments are cut into equal ranges.
 __device__ __forceinline__ int range_start(int nseg, int c, int G) { return (int)((long long)nseg * c / G); }
 
-__global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, const int *tg_off, const int *tg_gid,
-                                                          const int *tg_src, const double *ops, const double *Mt,
-                                                          const double4 *xr, double2 *L, PlanDev pd, int nstage,
-                                                          int ntiles, double2 *part) {
+// MAXP: the plan's pieces per warp (pd.maxp); at GP_MAXP_SMALL the
+// accumulators leave registers for two CTAs per SM.
+template <int MAXP>
+__global__ void __launch_bounds__(GP_WARPS * 32, MAXP == GP_MAXP_SMALL ? 2 : 1)
+    k_gemm64(const int *tile_tgt, const int *tg_off, const int *tg_gid, const int *tg_src, const double *ops,
+             const double *Mt, const double4 *xr, double2 *L, PlanDev pd, int nstage, int ntiles, double2 *part) {
   extern __shared__ __align__(16) double smd[];  // nstage x (operator, gathered multipoles); then the reduction
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int pc[GP_MAXP], wo[GP_MAXP];
+  int pc[MAXP], wo[MAXP];
 #pragma unroll
-  for (int p = 0; p < GP_MAXP; p++) {
-    pc[p] = pd.pieces[warp * GP_MAXP + p];
+  for (int p = 0; p < MAXP; p++) {
+    pc[p] = pd.pieces[warp * MAXP + p];
     wo[p] = pc[p] >= 0 ? pd.woff[pc[p] & 255] : 0;
   }
-  double acc[GP_MAXP][4][2];
+  double acc[MAXP][4][2];
   const int KP = pd.KP;
   const int KPAD = gp_kpad(KP);
   const size_t sstride = (size_t)pd.wsize + (size_t)GP_TILE * KPAD;  // doubles per stage (even: 16-byte rows)
@@ -716,7 +718,7 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
   if (g0 >= r1) break;
   if (g1 <= g0) continue;  // no segments: L stays zero
 #pragma unroll
-  for (int p = 0; p < GP_MAXP; p++)
+  for (int p = 0; p < MAXP; p++)
 #pragma unroll
     for (int cb = 0; cb < 4; cb++) acc[p][cb][0] = acc[p][cb][1] = 0;
   if (nstage == 2) issue(g0, 0);
@@ -735,7 +737,7 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
     __syncthreads();
     const double *Wsm = smd + (size_t)b * sstride, *Xsm = Wsm + pd.wsize;
 #pragma unroll
-    for (int p = 0; p < GP_MAXP; p++) {
+    for (int p = 0; p < MAXP; p++) {
       if (pc[p] < 0) continue;
       const int k0 = (pc[p] >> 8) & 4095, k1 = pc[p] >> 20;
       const double *Wb = Wsm + wo[p];
@@ -753,8 +755,8 @@ __global__ void __launch_bounds__(GP_WARPS * 32) k_gemm64(const int *tile_tgt, c
   __syncthreads();
   for (int rank = 0; rank <= pd.maxrank; rank++) {
 #pragma unroll
-    for (int p = 0; p < GP_MAXP; p++) {
-      if (pc[p] < 0 || pd.prank[warp * GP_MAXP + p] != rank) continue;
+    for (int p = 0; p < MAXP; p++) {
+      if (pc[p] < 0 || pd.prank[warp * MAXP + p] != rank) continue;
       const int rb = pc[p] & 255;
 #pragma unroll
       for (int cb = 0; cb < 4; cb++)
@@ -1312,11 +1314,11 @@ PlanCache &plan_cache(int P) {
 PlanDev plan_dev(const PlanCache &pc) {
   const GroupPlan &g = pc.host;
   PlanDev d;
-  d.P = g.P; d.NT = g.NT; d.KP = g.KP; d.nrb = g.nrb; d.wsize = g.wsize; d.maxrank = g.maxrank;
+  d.P = g.P; d.NT = g.NT; d.KP = g.KP; d.nrb = g.nrb; d.wsize = g.wsize; d.maxrank = g.maxrank; d.maxp = g.maxp;
   d.woff = pc.dev;
   d.jmin = d.woff + g.nrb + 1;
   d.pieces = d.jmin + g.nrb;
-  d.prank = d.pieces + GP_WARPS * GP_MAXP;
+  d.prank = d.pieces + GP_WARPS * g.maxp;
   return d;
 }
 
@@ -1341,7 +1343,8 @@ bool m2l_grouped_available(int P) {
 }
 
 void m2l_grouped_set_attributes() {
-  cudaFuncSetAttribute(k_gemm64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
+  cudaFuncSetAttribute(k_gemm64<GP_MAXP_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
+  cudaFuncSetAttribute(k_gemm64<GP_MAXP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
   cudaFuncSetAttribute(k_m2l_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
   cudaFuncSetAttribute(k_m2l_tc<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
   cudaFuncSetAttribute(k_m2l_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX);
@@ -1401,20 +1404,21 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
     const int nst = gemm64_smem(gp, 2) <= TC_SMEM_MAX ? 2 : 1;
     const size_t smem = gemm64_smem(gp, nst);
     const bool bal = P <= 10;
+    auto kern = gp.maxp == GP_MAXP_SMALL ? k_gemm64<GP_MAXP_SMALL> : k_gemm64<GP_MAXP>;
     int G = ntiles;
     const int NT = tri(P);
     double2 *part = nullptr;
     if (bal) {
       int occ = 1;
-      FMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_gemm64, GP_WARPS * 32, smem));
+      FMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, GP_WARPS * 32, smem));
       if (h.nsm == 0) FMM_CUDA(cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.prm.device));
       G = std::max(1, std::min(ntiles, h.nsm * std::max(occ, 1)));
       h.g_part.need((size_t)G * 2 * GP_TILE * NT * sizeof(double2));
       part = h.g_part.as<double2>();
     }
-    k_gemm64<<<G, GP_WARPS * 32, smem, s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src, h.g_ops.as<double>(),
-                                            h.g_mt.as<double>(), h.c_xr.as<double4>(), h.L.as<double2>(), pd, nst,
-                                            ntiles, part);
+    kern<<<G, GP_WARPS * 32, smem, s>>>(h.g_tile.as<int>(), tg_off, tg_gid, tg_src, h.g_ops.as<double>(),
+                                        h.g_mt.as<double>(), h.c_xr.as<double4>(), h.L.as<double2>(), pd, nst, ntiles,
+                                        part);
     if (bal) {
       k_m2l_join<<<ntiles, JOIN_T, 0, s>>>(h.g_tile.as<int>(), tg_off, ntiles, G, part, NT, GP_TILE,
                                           h.L.as<double2>());

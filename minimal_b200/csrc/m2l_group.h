@@ -11,7 +11,10 @@
 //
 // The FP64 kernel runs 8 warps per tile of 32 targets; each warp owns up to
 // GP_MAXP "pieces" (row block, k range), balanced by K length, with DMMA
-// accumulators for all 4 column blocks of the tile held in registers.
+// accumulators for all 4 column blocks of the tile held in registers.  A
+// plan whose warps hold at most GP_MAXP_SMALL pieces (every order up to 10,
+// and 12) is laid out with that stride and run by the kernel instantiated for
+// it: fewer accumulator registers, so two CTAs share an SM.
 #pragma once
 #include <algorithm>
 #include <vector>
@@ -20,12 +23,14 @@ namespace fmm {
 
 constexpr int GP_WARPS = 8;
 constexpr int GP_MAXP = 6;
+constexpr int GP_MAXP_SMALL = 4;
 constexpr int GP_TILE = 32;
 
 struct GroupPlan {
   int P = 0, NT = 0, KP = 0, nrb = 0, wsize = 0;
+  int maxp = 0;  // pieces per warp in the layout: GP_MAXP_SMALL or GP_MAXP
   std::vector<int> kp4, woff, jmin;
-  // pieces[w*GP_MAXP + p] = rb | k0 << 8 | k1 << 20 (k1 exclusive), -1 none
+  // pieces[w*maxp + p] = rb | k0 << 8 | k1 << 20 (k1 exclusive), -1 none
   std::vector<int> pieces;
   // rank of the piece among the pieces of its row block (0 stores, >0 adds)
   std::vector<int> prank;
@@ -79,15 +84,16 @@ inline GroupPlan make_group_plan(int P) {
       cnt[best]++;
     }
     if (!ok) continue;
-    g.pieces.assign(GP_WARPS * GP_MAXP, -1);
-    g.prank.assign(GP_WARPS * GP_MAXP, 0);
+    g.maxp = *std::max_element(cnt.begin(), cnt.end()) <= GP_MAXP_SMALL ? GP_MAXP_SMALL : GP_MAXP;
+    g.pieces.assign(GP_WARPS * g.maxp, -1);
+    g.prank.assign(GP_WARPS * g.maxp, 0);
     std::vector<int> seen(g.nrb, 0);
     for (int w = 0; w < GP_WARPS; w++)
       for (size_t p = 0; p < wp[w].size(); p++) {
         const Pc &c = wp[w][p];
-        g.pieces[w * GP_MAXP + p] = c.rb | (c.k0 << 8) | (c.k1 << 20);
-        g.prank[w * GP_MAXP + p] = seen[c.rb]++;
-        g.maxrank = std::max(g.maxrank, g.prank[w * GP_MAXP + p]);
+        g.pieces[w * g.maxp + p] = c.rb | (c.k0 << 8) | (c.k1 << 20);
+        g.prank[w * g.maxp + p] = seen[c.rb]++;
+        g.maxrank = std::max(g.maxrank, g.prank[w * g.maxp + p]);
       }
     return g;
   }
