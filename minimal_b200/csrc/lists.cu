@@ -23,7 +23,7 @@ namespace fmm {
 namespace {
 
 constexpr int TB = 256;
-constexpr int WALK_BLOCKS_PER_SM = 6;    // one wave of the walk (register-bound: 40 per thread)
+constexpr int WALK_PAIRS = 2;  // frontier pairs per thread per walk iteration
 constexpr int IMG_SHIFT = 26;             // entry = src | img << 26
 constexpr u32 IDX_MASK = (1u << IMG_SHIFT) - 1;
 
@@ -38,13 +38,30 @@ __device__ __forceinline__ void img3(int img, int &x, int &y, int &z) {
   z = img / 9 - 1;
 }
 
+// Level difference of two cells from their radii (R0 / 2^level, exactly):
+// the difference of the FP64 exponent fields when both are normal numbers,
+// else of ilogb.
+__device__ __forceinline__ int radius_level_diff(double rb, double ra) {
+  const int eb = (__double2hiint(rb) >> 20) & 0x7ff, ea = (__double2hiint(ra) >> 20) & 0x7ff;
+  if (eb != 0 && ea != 0 && eb != 0x7ff && ea != 0x7ff) return eb - ea;
+  return ilogb(rb) - ilogb(ra);
+}
+
+// One step of the walk.  Each thread takes WP frontier pairs per iteration
+// (the block's CHUNK = TB * WP consecutive pairs, pair r of thread t at
+// r * TB + t), so one block scan and one atomic per list reserve the output
+// ranges of CHUNK pairs; a thread's entries of one list are consecutive.
+// PERIODIC false: every pair is of image 13 (no shift), so the shift terms,
+// zero, are left out: x - 0 is x in every rounding.
+template <int WP, bool PERIODIC>
 __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const unsigned long long *nin_p,
                                             int2 *fout, unsigned long long *nout, unsigned long long *nnext,
                                             u64 fcap, int2 *m2l, unsigned long long *nm2l, u64 mcap, int2 *p2p,
                                             unsigned long long *np2p, u64 pcap, double theta, double cycle,
                                             int depth, int *overflow, int *m2l_key, int *occ, int *gflag,
                                             int *nres) {
-  constexpr int NW = TB / 32;
+  constexpr int NW = TB / 32, CHUNK = TB * WP;
+  static_assert(CHUNK < 4096, "per-block M2L and P2P counts are packed in 12-bit fields");
   __shared__ int s_tot[NW], s_totk[NW];    // every warp's packed list counts and frontier count
   __shared__ unsigned long long s_base[3];  // the block's M2L, P2P and frontier ranges
   __shared__ int s_res;                     // M2L entries without a group key
@@ -55,55 +72,68 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
   const u64 nin = min((u64)*nin_p, fcap);
   // the counter the step after next appends to: nothing reads it any more
   if (blockIdx.x == 0 && threadIdx.x == 0) *nnext = 0;
-  const u64 stride = (u64)gridDim.x * blockDim.x;
+  const u64 stride = (u64)gridDim.x * CHUNK;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   // every thread of a block iterates the same number of times (block-wide appends)
-  for (u64 base = (u64)blockIdx.x * blockDim.x; base < nin; base += stride) {
-    const u64 idx = base + threadIdx.x;
-    const bool act = idx < nin;
-    int i = 0, j = 0, img = 13, kind = -1;  // 0 m2l, 1 p2p, 2 split i, 3 split j
-    int nk = 0, first = 0, key = -1;
-    if (act) {
-      const int2 pr = fin[idx];
-      i = pr.x & (int)IDX_MASK;
-      img = (int)((u32)pr.x >> IMG_SHIFT);
-      j = pr.y;
-      int ix, iy, iz;
-      img3(img, ix, iy, iz);
+  for (u64 base = (u64)blockIdx.x * CHUNK; base < nin; base += stride) {
+    int2 pr[WP];
+#pragma unroll
+    for (int r = 0; r < WP; r++) {
+      const u64 idx = base + (u64)r * TB + threadIdx.x;
+      pr[r] = idx < nin ? fin[idx] : make_int2(0, -1);  // y = -1: no pair
+    }
+    int kind[WP], nk[WP], first[WP], key[WP];  // kind: -1 none, 0 m2l, 1 p2p, 2 split i, 3 split j
+    int nm = 0, np = 0, nf = 0;
+#pragma unroll
+    for (int r = 0; r < WP; r++) {
+      kind[r] = -1;
+      nk[r] = 0;
+      first[r] = 0;
+      key[r] = -1;
+      if (pr[r].y < 0) continue;
+      const int i = pr[r].x & (int)IDX_MASK, img = PERIODIC ? (int)((u32)pr[r].x >> IMG_SHIFT) : 13, j = pr[r].y;
       const double4 a = cv.xr[i], b = cv.xr[j];
-      const double dx = __dadd_rn(__dadd_rn(a.x, -b.x), -__dmul_rn((double)ix, cycle));
-      const double dy = __dadd_rn(__dadd_rn(a.y, -b.y), -__dmul_rn((double)iy, cycle));
-      const double dz = __dadd_rn(__dadd_rn(a.z, -b.z), -__dmul_rn((double)iz, cycle));
+      double dx = __dadd_rn(a.x, -b.x), dy = __dadd_rn(a.y, -b.y), dz = __dadd_rn(a.z, -b.z);
+      if (PERIODIC) {
+        int ix, iy, iz;
+        img3(img, ix, iy, iz);
+        dx = __dadd_rn(dx, -__dmul_rn((double)ix, cycle));
+        dy = __dadd_rn(dy, -__dmul_rn((double)iy, cycle));
+        dz = __dadd_rn(dz, -__dmul_rn((double)iz, cycle));
+      }
       const double nrm = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
       const double R2 = __dmul_rn(__dmul_rn(nrm, theta), theta);
       const double rs = __dadd_rn(a.w, b.w);
       const int ci = cv.nchild[i], cj = cv.nchild[j];
       if (R2 > __dmul_rn(rs, rs)) {
-        kind = 0;
+        kind[r] = 0;
         // the group key of the grouped M2L (radii are R0 / 2^level exactly,
         // so their exponents give the level difference)
-        if (img == 13) key = m2l_group_key(a, b, ilogb(b.w) - ilogb(a.w));
-        else key = m2l_image_key(a, b, ilogb(b.w) - ilogb(a.w), img, cv.xr[0].w, cycle, depth);
-        if (key >= 0) m2l_mark_key(key, i, occ, gflag);
+        const int dl = radius_level_diff(b.w, a.w);
+        if (img == 13) key[r] = m2l_group_key(a, b, dl);
+        else key[r] = m2l_image_key(a, b, dl, img, cv.xr[0].w, cycle, depth);
+        if (key[r] >= 0) m2l_mark_key(key[r], i, occ, gflag);
         else res++;
+        nm++;
       } else if (ci == 0 && cj == 0) {
-        kind = 1;
+        kind[r] = 1;
+        np++;
       } else if (cj == 0 || (a.w >= b.w && ci != 0)) {
-        kind = 2;
-        nk = ci;
-        first = cv.child[i];
+        kind[r] = 2;
+        nk[r] = ci;
+        first[r] = cv.child[i];
       } else {
-        kind = 3;
-        nk = cj;
-        first = cv.child[j];
+        kind[r] = 3;
+        nk[r] = cj;
+        first[r] = cv.child[j];
       }
+      nf += nk[r];
     }
-    const int packed_i = i | (img << IMG_SHIFT);
-    // warp scans for the three appends: M2L count in bits 0-10 and P2P in
-    // 11-21 of one word (at most 256 each per block), frontier pairs in a
+    // warp scans for the three appends: M2L count in bits 0-11 and P2P in
+    // 12-23 of one word (at most CHUNK each per block), frontier pairs in a
     // second
-    const int mine = (kind == 0) | ((kind == 1) << 11);
-    int incl = mine, inck = nk;
+    const int mine = nm | (np << 12);
+    int incl = mine, inck = nf;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int t = __shfl_up_sync(0xffffffffu, incl, o), tk = __shfl_up_sync(0xffffffffu, inck, o);
@@ -121,7 +151,7 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
     if (threadIdx.x < 3) {  // threads 0, 1, 2 reserve the block's M2L, P2P and frontier ranges
       int tot = 0;
       for (int w = 0; w < NW; w++) tot += threadIdx.x == 2 ? s_totk[w] : s_tot[w];
-      const unsigned n = threadIdx.x == 0 ? (tot & 2047) : threadIdx.x == 1 ? ((tot >> 11) & 2047) : tot;
+      const unsigned n = threadIdx.x == 0 ? (tot & 4095) : threadIdx.x == 1 ? ((tot >> 12) & 4095) : tot;
       unsigned long long *ctr = threadIdx.x == 0 ? nm2l : threadIdx.x == 1 ? np2p : nout;
       s_base[threadIdx.x] = n ? atomicAdd(ctr, (unsigned long long)n) : 0ull;
     }
@@ -131,26 +161,33 @@ __global__ void __launch_bounds__(TB) k_walk(CellView cv, const int2 *fin, const
       wpre += s_tot[w];
       wprek += s_totk[w];
     }
-    const int excl = wpre + incl - mine, exclk = wprek + inck - nk;
-    if (kind == 0) {
-      const unsigned long long sl = s_base[0] + (excl & 2047);
-      if (sl < mcap) {
-        m2l[sl] = make_int2(packed_i, j);
-        m2l_key[sl] = key;
-      } else {
-        *overflow = 1;
-      }
-    } else if (kind == 1) {
-      const unsigned long long sl = s_base[1] + ((excl >> 11) & 2047);
-      if (sl < pcap) p2p[sl] = make_int2(packed_i, j); else *overflow = 1;
-    } else if (nk > 0) {
-      const unsigned long long sl = s_base[2] + exclk;
-      for (int c = 0; c < nk; c++) {
-        if (sl + c < fcap) {
-          fout[sl + c] = kind == 2 ? make_int2((first + c) | (img << IMG_SHIFT), j) : make_int2(packed_i, first + c);
+    const int excl = wpre + incl - mine;
+    unsigned long long sm = s_base[0] + (excl & 4095), sp = s_base[1] + ((excl >> 12) & 4095),
+                       sf = s_base[2] + (wprek + inck - nf);
+#pragma unroll
+    for (int r = 0; r < WP; r++) {
+      if (kind[r] == 0) {
+        if (sm < mcap) {
+          m2l[sm] = pr[r];
+          m2l_key[sm] = key[r];
         } else {
           *overflow = 1;
         }
+        sm++;
+      } else if (kind[r] == 1) {
+        if (sp < pcap) p2p[sp] = pr[r]; else *overflow = 1;
+        sp++;
+      } else if (nk[r] > 0) {
+        const int img = (int)((u32)pr[r].x >> IMG_SHIFT);
+        for (int c = 0; c < nk[r]; c++) {
+          if (sf + c < fcap) {
+            fout[sf + c] = kind[r] == 2 ? make_int2((first[r] + c) | (img << IMG_SHIFT), pr[r].y)
+                                        : make_int2(pr[r].x, first[r] + c);
+          } else {
+            *overflow = 1;
+          }
+        }
+        sf += nk[r];
       }
     }
   }
@@ -299,6 +336,15 @@ __global__ void __launch_bounds__(SEG_WARPS * 32) k_order_segments32(const int *
   }
 }
 
+// Blocks of one wave of the walk: as many as are resident on the GPU at once.
+int walk_blocks(Handle &h, bool periodic) {
+  if (h.nsm == 0) FMM_CUDA(cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.prm.device));
+  int occ = 1;
+  FMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ, periodic ? k_walk<WALK_PAIRS, true> : k_walk<WALK_PAIRS, false>, TB, 0));
+  return h.nsm * std::max(occ, 1);
+}
+
 }  // namespace
 
 // CSR by target from the raw (target, source) pairs.  With `order` the
@@ -372,12 +418,14 @@ void build_lists(Handle &h) {
     h.launches++;
     CellView cv{h.c_xr.as<double4>(), h.c_child.as<int>(), h.c_nchild.as<int>()};
     const int steps = 2 * h.depth + 3;
+    const int walk_grid = walk_blocks(h, images != 0);
+    auto walk = images != 0 ? k_walk<WALK_PAIRS, true> : k_walk<WALK_PAIRS, false>;
     // frontier counters rotate over three words: step st reads word st % 3,
     // appends to (st + 1) % 3 (zeroed by step st - 1, or above) and zeroes
     // (st + 2) % 3
     for (int st = 0; st < steps; st++) {
       const int a = st & 1, b = a ^ 1;
-      k_walk<<<148 * WALK_BLOCKS_PER_SM, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[st % 3], h.frontier[b].as<int2>(),
+      walk<<<walk_grid, TB, 0, s>>>(cv, h.frontier[a].as<int2>(), &ctr->frontier[st % 3], h.frontier[b].as<int2>(),
                                     &ctr->frontier[(st + 1) % 3], &ctr->frontier[(st + 2) % 3], h.frontier_cap,
                                     h.m2l_raw.as<int2>(), &ctr->n_m2l, h.m2l_cap, h.p2p_raw.as<int2>(), &ctr->n_p2p,
                                     h.p2p_cap, h.prm.theta, images ? h.prm.cycle : 0.0, h.depth, &ctr->list_overflow,

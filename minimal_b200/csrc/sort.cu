@@ -221,6 +221,34 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const u64 *keys, long n,
   hist[(long)threadIdx.x * ntiles + blockIdx.x] = hs[threadIdx.x];
 }
 
+// Block d: exclusive scan of digit d's counts over the tiles, into
+// offs[d * ntiles + tile], and the digit's total into dtot[d].
+__global__ void __launch_bounds__(RS_THREADS) k_rs_digit_scan(const int *hist, int *offs, int *dtot, int ntiles) {
+  __shared__ int warp_sum[RS_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int *h = hist + (long)blockIdx.x * ntiles;
+  int *o = offs + (long)blockIdx.x * ntiles;
+  int carry = 0;
+  for (int base = 0; base < ntiles; base += RS_THREADS) {
+    const int i = base + threadIdx.x;
+    const int v = i < ntiles ? h[i] : 0;
+    const int incl = warp_incl_scan(v);
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    int wpre = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < RS_THREADS / 32; w++) {
+      const int ws = warp_sum[w];
+      wpre += w < warp ? ws : 0;
+      tot += ws;
+    }
+    if (i < ntiles) o[i] = carry + wpre + incl - v;
+    carry += tot;
+    __syncthreads();  // warp_sum is rewritten by the next chunk
+  }
+  if (threadIdx.x == 0) dtot[blockIdx.x] = carry;
+}
+
 // Stable scatter of one tile.  Warp w ranks its contiguous 256 items
 // (8 rounds of 32 lanes, per-warp digit counters bumped by the leader of
 // each group of equal digits), the counts of the 8 warps are combined into
@@ -229,14 +257,27 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const u64 *keys, long n,
 // contiguous in the output, so the stores coalesce.
 __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const u64 *kin, const u32 *vin, u64 *kout, u32 *vout,
                                                           long n, int shift, u64 mask, const int *offs,
-                                                          int ntiles) {
+                                                          const int *dtot, int ntiles) {
   constexpr int NW = RS_THREADS / 32, PER = RS_TILE / NW;  // 256 items per warp
+  static_assert(RS_BINS == RS_THREADS, "one thread per digit scans the digit totals");
   __shared__ int wcnt[NW][RS_BINS + 1];                     // per-warp digit counts, then offsets
   __shared__ int loff[RS_BINS + 1];                         // tile-local digit offsets
+  __shared__ int dbase[RS_BINS];                            // first output slot of each digit
+  __shared__ int dsum[NW];
   __shared__ u64 sk[RS_TILE];
   __shared__ u32 sv[RS_TILE];
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   for (int k = t; k < NW * (RS_BINS + 1); k += RS_THREADS) (&wcnt[0][0])[k] = 0;
+  {  // exclusive scan of the digit totals
+    const int c = dtot[t];
+    const int incl = warp_incl_scan(c);
+    if (lane == 31) dsum[warp] = incl;
+    __syncthreads();
+    int wpre = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) wpre += w < warp ? dsum[w] : 0;
+    dbase[t] = wpre + incl - c;
+  }
   __syncthreads();
   const long tile0 = (long)blockIdx.x * RS_TILE;
   const int valid = (int)(n - tile0 < RS_TILE ? n - tile0 : RS_TILE);
@@ -308,7 +349,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const u64 *kin, const
   for (int j = t; j < valid; j += RS_THREADS) {
     const u64 k = sk[j];
     const int d = (int)((k >> shift) & mask);
-    const long o = (long)offs[(long)d * ntiles + blockIdx.x] + (j - loff[d]);
+    const long o = (long)dbase[d] + offs[(long)d * ntiles + blockIdx.x] + (j - loff[d]);
     kout[o] = k;
     vout[o] = sv[j];
   }
@@ -349,17 +390,19 @@ void scan_exclusive_int(Handle &h, const int *in, int *out, long n, int *total_d
 void radix_sort_pairs(Handle &h, u64 *&k, u32 *&v, u64 *&k2, u32 *&v2, long n, int lo_bit, int hi_bit) {
   if (n <= 1 || hi_bit <= lo_bit) return;
   const int ntiles = (int)((n + RS_TILE - 1) / RS_TILE);
-  h.hist.need((size_t)2 * RS_BINS * ntiles * sizeof(int));
+  h.hist.need(((size_t)2 * RS_BINS * ntiles + RS_BINS) * sizeof(int));
   int *hist = h.hist.as<int>();
   int *offs = hist + (long)RS_BINS * ntiles;
+  int *dtot = offs + (long)RS_BINS * ntiles;
   for (int shift = lo_bit; shift < hi_bit; shift += 8) {
     const int bits = hi_bit - shift < 8 ? hi_bit - shift : 8;
     const u64 mask = (1ull << bits) - 1;
     k_rs_hist<<<ntiles, RS_THREADS, 0, h.stream>>>(k, n, shift, mask, hist, ntiles);
-    h.launches++;
+    // per digit over the tiles; the scatter adds the scanned digit totals
+    k_rs_digit_scan<<<RS_BINS, RS_THREADS, 0, h.stream>>>(hist, offs, dtot, ntiles);
+    h.launches += 2;
     FMM_LAUNCH();
-    scan_exclusive_int(h, hist, offs, (long)RS_BINS * ntiles, nullptr);
-    k_rs_scatter<<<ntiles, RS_THREADS, 0, h.stream>>>(k, v, k2, v2, n, shift, mask, offs, ntiles);
+    k_rs_scatter<<<ntiles, RS_THREADS, 0, h.stream>>>(k, v, k2, v2, n, shift, mask, offs, dtot, ntiles);
     h.launches++;
     FMM_LAUNCH();
     u64 *tk = k; k = k2; k2 = tk;
