@@ -190,9 +190,8 @@ void need_single(Handle &h, const char *what) {
 void do_tree(Handle &h) {
   if (h.n <= 0) throw Error{EXAFMM_ERR_STATE, "no bodies loaded"};
   Timer t(h, PH_TREE);
-  build_tree(h);
+  build_tree(h);  // sets srcf_ready: the mixed form's FP32 sources come with the gathered bodies
   h.have_tree = true;
-  h.srcf_ready = false;
   h.have_lists = h.have_up = h.have_horiz = h.have_down = false;
 }
 

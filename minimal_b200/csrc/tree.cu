@@ -365,23 +365,33 @@ __global__ void k_compact_leaves(const int *is_leaf, const int *pos, long c, int
 }
 
 // Bodies of one leaf back into input order (warp per leaf, rank sort).
-__global__ void k_leaf_order(const int *leaves, int nleaves, const int *begin, const int *count, u32 *vals,
-                             int *perm) {
+// Bodies of each leaf back to input order (a body's slot is the rank of its
+// input index among the leaf's), gathered into src.  With srcf (3D mixed
+// form) also the FP32 copy of each body as an offset from its leaf centre
+// (FP64 subtraction, one rounding) and the body's leaf, as k_make_srcf makes
+// them: one pass over the bodies instead of three.
+__global__ void k_leaf_order(const int *leaves, int nleaves, const int *begin, const int *count, const double4 *xr,
+                             const u32 *vals, const double4 *in, int *perm, double4 *src, float4 *srcf,
+                             int *body_leaf) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= nleaves) return;
   const int c = leaves[w], b0 = begin[c], nb = count[c];
+  const double4 C = xr[c];
   for (int a = lane; a < nb; a += 32) {
     const u32 v = vals[b0 + a];
     int r = 0;
     for (int k = 0; k < nb; k++) r += vals[b0 + k] < v;
-    perm[b0 + r] = (int)v;
+    const int b = b0 + r;
+    perm[b] = (int)v;
+    const double4 B = in[v];
+    src[b] = B;
+    if (srcf) {
+      srcf[b] = make_float4((float)(B.x - C.x), (float)(B.y - C.y), (float)(B.z - C.z), (float)B.w);
+      body_leaf[b] = w;
+    }
   }
 }
 
-__global__ void k_gather_bodies(const double4 *in, const int *perm, long n, double4 *src) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) src[i] = in[perm[i]];
-}
 
 __global__ void k_zero_counters(DevCounters *c) {
   const int t = threadIdx.x;
@@ -394,6 +404,7 @@ __global__ void k_zero_counters(DevCounters *c) {
 void build_tree(Handle &h) {
   const long n = h.n;
   cudaStream_t s = h.stream;
+  h.srcf_ready = false;  // set again once the new tree's FP32 sources are made
   const int nsys = h.nsys;
   h.geom.need((size_t)nsys * sizeof(RootGeom));
   h.counters.need(sizeof(DevCounters));
@@ -513,14 +524,21 @@ void build_tree(Handle &h) {
       h.level_base[l + 1] = h.level_base[l] + h.hc.level_count[l];
       if (h.hc.level_count[l]) h.depth = l;
     }
-    // 6. bodies of each leaf back to input order, then gather
+    // 6. bodies of each leaf back to input order and gathered (the mixed
+    // form's FP32 sources with them)
     h.perm.need(n * 4);
     h.src.need(n * sizeof(double4));
-    k_leaf_order<<<grid_for((long)h.nleaves * 32, TB), TB, 0, s>>>(h.leaves.as<int>(), h.nleaves, o.begin,
-                                                                  o.count, v, h.perm.as<int>());
-    k_gather_bodies<<<grid_for(n, TB), TB, 0, s>>>(h.in.as<double4>(), h.perm.as<int>(), n, h.src.as<double4>());
-    h.launches += 2;
+    const bool srcf = h.prm.precision == EXAFMM_MIXED && h.prm.dim == 3;
+    if (srcf) {
+      h.srcf.need((size_t)n * sizeof(float4));
+      h.body_leaf.need((size_t)n * sizeof(int));
+    }
+    k_leaf_order<<<grid_for((long)h.nleaves * 32, TB), TB, 0, s>>>(
+        h.leaves.as<int>(), h.nleaves, o.begin, o.count, o.xr, v, h.in.as<double4>(), h.perm.as<int>(),
+        h.src.as<double4>(), srcf ? h.srcf.as<float4>() : nullptr, srcf ? h.body_leaf.as<int>() : nullptr);
+    h.launches++;
     FMM_LAUNCH();
+    h.srcf_ready = srcf;
     break;
   }
   // 2D bodies lie at z = 0: the octree is the quadtree (the z digit is the
