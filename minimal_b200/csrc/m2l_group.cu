@@ -1401,10 +1401,16 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
     // at once (at 1M uniform bodies 7.82 -> 7.29 ms per evaluation at P = 8,
     // 9.03 -> 8.47 at P = 10); above, one CTA per tile (P = 12: 10.87
     // against 11.13 ms with the ranges)
-    const int nst = gemm64_smem(gp, 2) <= TC_SMEM_MAX ? 2 : 1;
+    auto kern = gp.maxp == GP_MAXP_SMALL ? k_gemm64<GP_MAXP_SMALL> : k_gemm64<GP_MAXP>;
+    int nst = gemm64_smem(gp, 2) <= TC_SMEM_MAX ? 2 : 1;
+    if (nst == 2) {  // one stage where that doubles the CTAs per SM (P = 12: 1 -> 2 CTAs)
+      int occ1 = 0, occ2 = 0;
+      FMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, kern, GP_WARPS * 32, gemm64_smem(gp, 1)));
+      FMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, kern, GP_WARPS * 32, gemm64_smem(gp, 2)));
+      if (occ1 >= 2 * occ2) nst = 1;
+    }
     const size_t smem = gemm64_smem(gp, nst);
     const bool bal = P <= 10;
-    auto kern = gp.maxp == GP_MAXP_SMALL ? k_gemm64<GP_MAXP_SMALL> : k_gemm64<GP_MAXP>;
     int G = ntiles;
     const int NT = tri(P);
     double2 *part = nullptr;
