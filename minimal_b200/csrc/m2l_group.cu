@@ -1397,10 +1397,11 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
     h.g_used_tc = true;
   } else {
     // two pipeline stages where they fit in shared memory (P <= 12), else
-    // one.  P <= 10: equal segment ranges over as many CTAs as fit on the GPU
+    // one.  P <= 11: equal segment ranges over as many CTAs as fit on the GPU
     // at once (at 1M uniform bodies 7.82 -> 7.29 ms per evaluation at P = 8,
-    // 9.03 -> 8.47 at P = 10); above, one CTA per tile (P = 12: 10.87
-    // against 11.13 ms with the ranges)
+    // 9.03 -> 8.47 at P = 10, 9.69 -> 9.35 at P = 11); above, one CTA per
+    // tile (P = 12, two one-stage CTAs per SM: 9.69 against 9.78 ms with the
+    // ranges)
     auto kern = gp.maxp == GP_MAXP_SMALL ? k_gemm64<GP_MAXP_SMALL> : k_gemm64<GP_MAXP>;
     int nst = gemm64_smem(gp, 2) <= TC_SMEM_MAX ? 2 : 1;
     if (nst == 2) {  // one stage where that doubles the CTAs per SM (P = 12: 1 -> 2 CTAs)
@@ -1410,7 +1411,7 @@ void contract(Handle &h, bool tcore, const TcPlan &tp, int KP16, const GroupPlan
       if (occ1 >= 2 * occ2) nst = 1;
     }
     const size_t smem = gemm64_smem(gp, nst);
-    const bool bal = P <= 10;
+    const bool bal = P <= 11;
     int G = ntiles;
     const int NT = tri(P);
     double2 *part = nullptr;
