@@ -213,12 +213,15 @@ def test_argument_and_state_errors():
     assert np.isfinite(fmm.bodies()).all()
 
 
-@pytest.mark.parametrize("P", [12, 13])
+@pytest.mark.parametrize("P", [11, 12, 13])
 def test_fp64_contraction_stage_counts_vs_oracle(port, P):
     """The FP64 grouped M2L stages each group's operator and gathered
-    multipoles with asynchronous copies, in two pipeline stages where they fit
-    in shared memory (P <= 12) and one above: both paths match the reference
-    restatement within the FP64 form's 1e-12."""
+    multipoles with asynchronous copies.  Its launch shapes by order: P = 11,
+    six pieces per warp, two pipeline stages, balanced segment ranges; P = 12,
+    four pieces per warp and one stage, so that two CTAs share an SM, one CTA
+    per tile; P = 13, six pieces, one stage (two do not fit).  (P <= 10, four
+    pieces, two stages and ranges, is covered by the random cases.)  Every
+    path matches the reference restatement within the FP64 form's 1e-12."""
     from minimal_b200 import FMM
     from minimal_b200.bodies import uniform_bodies
 
