@@ -337,7 +337,7 @@ template <bool F32>
 constexpr int ct_cap() { return F32 ? 1536 : 1024; }
 constexpr int CT_MAXTGT = 256;    // target-leaf bodies: two per thread
 constexpr int CT_TPT = 2;         // targets per thread (register blocking)
-constexpr int CT_BLOCK = 128;     // sources summed in FP32 before one compensated addition
+constexpr int CT_BLOCK = 256;     // sources summed in FP32 before one compensated addition
 // 32-body blocks a warp loads before storing them (register-bound)
 template <bool F32>
 constexpr int ct_unroll() { return F32 ? 2 : 1; }
